@@ -1,0 +1,306 @@
+/*
+ * kf_api.h -- C ABI of the B200 KinectFusion per-frame pipeline (libkfb200.so).
+ *
+ * A uint16 depth frame goes in; the camera pose, the TSDF volume and the per-level raycast
+ * vertex/normal maps come out.  Everything behind this header is hand-written sm_100a CUDA
+ * driven by C++ host code; nothing here carries a C++ or torch type.
+ *
+ * Conventions (all inherited from the reference so that its callers' data drops in):
+ *   - Depth maps are row-major float[h][w] in metres.
+ *   - Vertex / normal maps are row-major float[h][w][4] = (x, y, z, tag) with tag -1 for a valid
+ *     element and -2 for an invalid one (project/src/device_helper.cuh:9-10, :37-44).
+ *   - Matrices are column-major, the memory order of glm::mat3 / glm::mat4 (element (row r,
+ *     col c) at flat[c*dim + r]; test/example_test.cpp:36-50 pins this).
+ *   - A pose is camera->world (project/src/sensor.h:30-34).
+ *   - The TSDF is x-fastest, then y, then z.  Format KF_TSDF_F32F32 keeps distance and weight
+ *     in two float arrays; KF_TSDF_F16U16 keeps an fp16 distance array and a uint16 weight array
+ *     with KF_WEIGHT_SCALE fixed-point steps per unit of weight.  kf_get_tsdf /
+ *     kf_set_tsdf convert to and from the reference's interleaved float2 .bin layout
+ *     (project/src/voxel_grid.cpp:43-80).
+ *   - Every call returns a kf_status; nothing throws across this boundary.  Where the
+ *     reference throws std::runtime_error on a shape mismatch (e.g.
+ *     project/src/measurement.cu:144-147) this ABI returns KF_ERR_SHAPE.
+ *   - Stream arguments are cudaStream_t passed as void* (NULL = legacy default stream).
+ *     Stage calls are asynchronous unless elapsed_ms is non-NULL, in which case they record
+ *     events around the launch, synchronize and store the elapsed time, as every
+ *     reference kernel:: wrapper does (project/src/measurement.cuh:11).
+ */
+#ifndef KF_API_H
+#define KF_API_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define KF_API_VERSION 1
+#define KF_MAX_LEVELS 3
+/* fixed-point steps per unit of weight in the uint16 weight array of KF_TSDF_F16U16 */
+#define KF_WEIGHT_SCALE 128.0f
+
+typedef enum kf_status {
+    KF_OK = 0,
+    KF_ERR_ARG = 1,         /* null pointer, bad enum, unsupported size */
+    KF_ERR_SHAPE = 2,       /* map sizes disagree (reference: std::runtime_error) */
+    KF_ERR_CUDA = 3,        /* a CUDA runtime call failed */
+    KF_ERR_NONFINITE = 4,   /* ICP solution not finite: pose kept, frame not fused
+                               (reference: project/src/icp.cpp:67-73 throws) */
+    KF_ERR_OOM_BUDGET = 5,  /* admission refused: the session does not fit the HBM budget */
+    KF_ERR_TIMEOUT = 6,     /* a bounded device-side wait expired; the context stays usable */
+    KF_ERR_STATE = 7,       /* call not valid in the object's current state */
+    KF_ERR_CAPACITY = 8     /* no free slot */
+} kf_status;
+
+typedef enum kf_tsdf_format {
+    KF_TSDF_F32F32 = 0,     /* float distance + float weight, 8 B/voxel (reference layout) */
+    KF_TSDF_F16U16 = 1      /* fp16 distance + uint16 weight, 4 B/voxel */
+} kf_tsdf_format;
+
+/*
+ * Session configuration.  One struct replaces the reference's KinectFusionConfig
+ * (project/src/kinect_fusion.h:17-36), IcpConfig (project/src/icp.h:11-20) and the
+ * compile-time constants the reference hard-codes:
+ *   bilateral sigma_s / sigma_r / window  (project/src/measurement.cu:11-12, :38)
+ *   min / max sensor range 0.4 / 6.0 m     (project/src/tsdf.cuh:11-12)
+ *   raycast steps 1.99 mu / 0.1 mu          (project/src/raycast.cu:75-76)
+ *   principal point 319.5 / 239.5          (project/src/sensor.h:14)
+ *   frustum bounds 640 x 480                (project/src/tsdf.cu:40)
+ * kf_config_default() fills the reference's values (project/src/main.cpp:11-59, the
+ * dataset configuration) so that a default session behaves like the reference.
+ */
+typedef struct kf_config {
+    int width, height;           /* frame size; divisible by 2^(levels-1) */
+    float fx, fy, cx, cy;        /* level-0 intrinsics (reference: fx = fy = field_of_view) */
+    float depth_scale;           /* raw uint16 -> metres */
+    int unmirror;                /* flip columns on conversion (reference: use_kinect) */
+    int levels;                  /* pyramid levels, 1..3 (reference: iters_per_layer.size()) */
+    int iters[KF_MAX_LEVELS];    /* ICP iterations per level, index 0 = finest */
+    float dist_thresh;           /* correspondence distance rejection, metres */
+    float angle_thresh;          /* correspondence normal-angle rejection, radians */
+    float stop_angle;            /* early stop: rotation chord threshold */
+    float stop_dist;             /* early stop: translation threshold, metres */
+    float bilateral_sigma_s;     /* pixels */
+    float bilateral_sigma_r;     /* metres; the downsample gate is 3 * sigma_r */
+    int bilateral_radius;        /* window = 2 * radius + 1 */
+    int volume_n;                /* voxels per side */
+    float volume_width;          /* cube edge in metres, centred at the world origin */
+    float mu;                    /* truncation distance in metres */
+    float max_weight;            /* 0 = no clamp (reference behaviour) */
+    int tsdf_format;             /* kf_tsdf_format */
+    float min_depth, max_depth;  /* sensor range used by fusion and raycast */
+    float step_large, step_small;/* raycast steps in units of mu */
+    int compat_trunc8;           /* process only what the reference's dims/8 grids cover */
+    int keep_on_miss;            /* rays that miss the volume keep the previous map contents
+                                    (reference: project/src/raycast.cu:61-73 returns early) */
+    int export_icp_mask;         /* record per-pixel correspondence masks of the last iteration */
+    float initial_pose[16];      /* camera->world, column-major */
+} kf_config;
+
+/* A TSDF volume in device memory, for the per-stage calls. */
+typedef struct kf_volume {
+    void* f;                     /* distance array: float or __half, n^3, x fastest */
+    void* w;                     /* weight array: float or uint16, n^3 */
+    int n;
+    float width;                 /* metres */
+    float mu;                    /* metres */
+    int format;                  /* kf_tsdf_format */
+    float max_weight;            /* 0 = no clamp */
+} kf_volume;
+
+/* Per-frame results beyond the pose. */
+typedef struct kf_frame_stats {
+    int frame;                   /* index of the frame just processed (0 = first) */
+    int status;                  /* kf_status of that frame */
+    int icp_iters[KF_MAX_LEVELS];/* ICP iterations run per level (0 for frame 0) */
+} kf_frame_stats;
+
+/* ------------------------------------------------------------------------------------------ */
+/* library                                                                                    */
+/* ------------------------------------------------------------------------------------------ */
+int kf_api_version(void);
+const char* kf_status_string(int status);
+/* Fill the reference's defaults (project/src/main.cpp:11-59 dataset config, 640x480). */
+void kf_config_default(kf_config* cfg);
+/* Bytes of device memory a session with this configuration holds. */
+kf_status kf_session_footprint(const kf_config* cfg, size_t* bytes);
+
+/* ------------------------------------------------------------------------------------------ */
+/* session: the reference's KinectFusion class (project/src/kinect_fusion.h:38-48)          */
+/* ------------------------------------------------------------------------------------------ */
+typedef struct kf_session kf_session;
+
+/* Allocate buffers and the volume, initialise the grid to {f = 2, w = 0}
+ * (reference constructor, project/src/kinect_fusion.cpp:13-42). */
+kf_status kf_session_create(const kf_config* cfg, kf_session** out);
+kf_status kf_session_destroy(kf_session* s);
+/* Back to frame 0: grid re-initialised, pose = initial_pose. */
+kf_status kf_session_reset(kf_session* s);
+/* One frame.  Frame 0 converts and fuses only (initializeTracking,
+ * project/src/kinect_fusion.cpp:75-94); later frames run preprocessing, raycast at the
+ * previous pose, ICP and fusion (project/src/kinect_fusion.cpp:48-72).
+ * depth: w*h uint16 in host memory (is_device_ptr = 0) or device memory (1).
+ * pose_out (may be NULL): the new camera->world pose, column-major.
+ * The call synchronizes the stream before returning. */
+kf_status kf_process_frame(kf_session* s, const uint16_t* depth, int is_device_ptr,
+                           void* stream, float pose_out[16]);
+/* Enqueue one frame from device memory without synchronizing (for graph-replay drivers);
+ * results are valid once the stream reaches this point. */
+kf_status kf_process_frame_async(kf_session* s, const uint16_t* depth_device, void* stream);
+kf_status kf_get_pose(kf_session* s, float pose[16]);
+kf_status kf_set_pose(kf_session* s, const float pose[16]);
+kf_status kf_get_frame_stats(kf_session* s, kf_frame_stats* out);
+/* Map taps.  dst is host memory when to_host = 1, else device memory.  level in
+ * [0, levels); kf_get_depth with level = -1 returns the unfiltered metres map that fusion
+ * reads. */
+kf_status kf_get_depth(kf_session* s, int level, float* dst, int to_host);
+kf_status kf_get_vertex(kf_session* s, int level, float* dst, int to_host);
+kf_status kf_get_raycast(kf_session* s, int level, float* vertex, float* normal, int to_host);
+kf_status kf_get_icp_mask(kf_session* s, int level, uint8_t* dst, int to_host);
+/* TSDF readback / load.  layout 0: native arrays (f array then w array, each n^3);
+ * layout 1: reference interleaved float2 {f, w} (.bin layout). */
+kf_status kf_get_tsdf(kf_session* s, void* dst, size_t dst_bytes, int layout, int to_host);
+kf_status kf_set_tsdf(kf_session* s, const void* src, size_t src_bytes, int layout, int from_host);
+kf_status kf_get_volume(kf_session* s, kf_volume* out);
+
+/* ------------------------------------------------------------------------------------------ */
+/* stages: the reference's kernel:: wrappers, on device pointers                            */
+/* ------------------------------------------------------------------------------------------ */
+/* kernel::convertToDepthMeters, project/src/measurement.cuh:12 */
+kf_status kf_convert_to_depth_meters(const uint16_t* raw, int w, int h, float* out, int out_w,
+                                     int out_h, float scale, int unmirror, void* stream,
+                                     float* elapsed_ms);
+/* kernel::applyBilateralFilter, project/src/measurement.cuh:13 (sigma/window are the
+ * reference's compile-time constants, passed here) */
+kf_status kf_apply_bilateral_filter(const float* in, int w, int h, float* out, int out_w,
+                                    int out_h, float sigma_s, float sigma_r, int radius,
+                                    void* stream, float* elapsed_ms);
+/* kernel::downSample, project/src/measurement.cuh:14 */
+kf_status kf_down_sample(const float* in, int w, int h, float* out, int out_w, int out_h,
+                         float sigma_r, void* stream, float* elapsed_ms);
+/* kernel::createVertexMap, project/src/measurement.cuh:15 (inv_cam_k column-major 3x3) */
+kf_status kf_create_vertex_map(const float* depth, int w, int h, float* vertex, int out_w,
+                               int out_h, const float inv_cam_k[9], void* stream,
+                               float* elapsed_ms);
+/* kernel::createNormalMap, project/src/measurement.cuh:16 */
+kf_status kf_create_normal_map(const float* vertex, int w, int h, float* normal, int out_w,
+                               int out_h, void* stream, float* elapsed_ms);
+/* kernel::initializeGrid, project/src/tsdf.cuh:15 (value {f = 2, w = 0}) */
+kf_status kf_initialize_grid(const kf_volume* vol, void* stream, float* elapsed_ms);
+/* kernel::fuse, project/src/tsdf.cuh:16.  cam_k: level-0 intrinsics, column-major;
+ * w, h: the frustum bounds (the reference hard-codes 640 x 480). */
+kf_status kf_fuse(const float* depth_m, int w, int h, const float cam_k[9], const kf_volume* vol,
+                  const float pose[16], float min_depth, float max_depth, void* stream,
+                  float* elapsed_ms);
+/* kernel::raycast, project/src/raycast.cuh:11.  inv_cam_k: the level's inverse intrinsics. */
+kf_status kf_raycast(const kf_volume* vol, const float pose[16], const float inv_cam_k[9],
+                     float* vertex, int w, int h, float* normal, int nw, int nh,
+                     float min_depth, float max_depth, float step_large, float step_small,
+                     void* stream, float* elapsed_ms);
+/* kernel::constructIcpResiduals, project/src/icp.cuh:34-37.  Writes the reference's
+ * row-major A (w*h x 6) and b (w*h), zero rows for rejected pixels. */
+kf_status kf_construct_icp_residuals(const float* vertex, const float* target_vertex,
+                                     const float* target_normal, int w, int h,
+                                     const float prev_rot[9], const float prev_transl[3],
+                                     const float cur_rot[9], const float cur_transl[3],
+                                     const float cam_k[9], float distance_thresh,
+                                     float angle_thresh, float* mat_a, float* vec_b,
+                                     void* stream, float* elapsed_ms);
+/* LinearLeastSquares::solve, project/src/linear_least_squares.h:19: x = argmin |A x - b|
+ * over n rows (A row-major n x 6 and b on the device).  The normal equations are reduced
+ * in FP32 with compensated block sums and combined and solved (Cholesky) in FP64 on the
+ * device; only the 6 floats of x come back. */
+kf_status kf_solve_linear_least_squares(const float* mat_a, const float* vec_b, int n,
+                                        float x_out[6], void* stream);
+/* ICP::computePose, project/src/icp.h:35-36.  Coarse-to-fine point-to-plane ICP of the
+ * vertex pyramid against the predicted (world-frame) pyramid, starting at pose; each map
+ * pointer array holds `levels` device pointers.  One cooperative device launch runs every
+ * iteration, solve and early-stop test.  iters_out (may be NULL) gets iterations per level. */
+kf_status kf_compute_pose(const float* const* vertex, const float* const* target_vertex,
+                          const float* const* target_normal, int w, int h, int levels,
+                          const kf_config* cfg, const float pose[16], float pose_out[16],
+                          int iters_out[KF_MAX_LEVELS], void* stream);
+/* poseError, project/src/general_helper.h:9: out[0] = chord between the two rotations
+ * applied to normalize(1,1,1); out[1] = translation distance.  Host-side helper. */
+kf_status kf_pose_error(const float pose_1[16], const float pose_2[16], float out[2]);
+
+/* ------------------------------------------------------------------------------------------ */
+/* batch: many independent sessions of uneven sizes, one persistent launch per stage,        */
+/* replayed from a captured CUDA graph                                                        */
+/* ------------------------------------------------------------------------------------------ */
+typedef struct kf_batch kf_batch;
+
+kf_status kf_batch_create(const kf_config* cfgs, int n, kf_batch** out);
+kf_status kf_batch_destroy(kf_batch* b);
+/* One frame for every session whose entry in `depth` is non-NULL (host pointers when
+ * is_device_ptr = 0).  Sessions with a NULL entry sit this step out.  poses_out (may be
+ * NULL): n * 16 floats.  Synchronizes before returning. */
+kf_status kf_batch_step(kf_batch* b, const uint16_t* const* depth, int is_device_ptr,
+                        void* stream, float* poses_out);
+/* Enqueue a step whose frames are already in each session's device input buffer. */
+kf_status kf_batch_step_async(kf_batch* b, const int* active, void* stream);
+/* Device address of session i's uint16 input frame buffer (w*h elements). */
+kf_status kf_batch_input_buffer(kf_batch* b, int i, uint16_t** dev_ptr);
+kf_status kf_batch_session(kf_batch* b, int i, kf_session** out);
+/* Choose block shapes per stage by timing candidates on this batch's own data. */
+kf_status kf_batch_autotune(kf_batch* b, void* stream, char* report, size_t report_bytes);
+
+/* ------------------------------------------------------------------------------------------ */
+/* server: continuous batching of concurrent sessions with HBM-budget admission              */
+/* ------------------------------------------------------------------------------------------ */
+typedef struct kf_server kf_server;
+
+typedef struct kf_server_stats {
+    long long frames_done;
+    long long sessions_admitted;
+    long long sessions_refused;
+    long long steps;
+    int active_sessions;
+    int max_active_sessions;
+    size_t hbm_in_use;
+    size_t hbm_budget;
+    double p50_ms, p99_ms, max_ms;   /* submit -> result ready */
+} kf_server_stats;
+
+/* max_slots: most sessions resident at once; hbm_budget: bytes all sessions may hold. */
+kf_status kf_server_create(int max_slots, size_t hbm_budget, kf_server** out);
+kf_status kf_server_destroy(kf_server* srv);
+/* Admit a session: KF_ERR_OOM_BUDGET when it does not fit the budget, KF_ERR_CAPACITY when
+ * every slot is taken.  *id identifies it in later calls. */
+kf_status kf_server_open(kf_server* srv, const kf_config* cfg, int* id);
+kf_status kf_server_close(kf_server* srv, int id);
+/* Queue one frame (host memory, copied before return).  A session holds at most one
+ * queued frame; a second submit before the first is served returns KF_ERR_STATE. */
+kf_status kf_server_submit(kf_server* srv, int id, const uint16_t* depth, double t_submit_ms);
+/* Run one batched step over every session with a queued frame; returns how many frames it
+ * served in *served.  Frames that arrive while a step runs join the next one. */
+kf_status kf_server_step(kf_server* srv, int* served);
+/* Result of the session's last served frame. */
+kf_status kf_server_result(kf_server* srv, int id, float pose[16], kf_frame_stats* stats);
+kf_status kf_server_get_session(kf_server* srv, int id, kf_session** out);
+kf_status kf_server_stats_get(kf_server* srv, kf_server_stats* out);
+/* Clock used for latency accounting (milliseconds, monotonic). */
+double kf_now_ms(void);
+
+/* ------------------------------------------------------------------------------------------ */
+/* instrumentation (the reference times every kernel:: call with a blocking event pair,       */
+/* project/src/cuda_event.cpp:14-29; here events sit between the stage launches of a step,    */
+/* inside the captured graph, and nothing blocks)                                              */
+/* ------------------------------------------------------------------------------------------ */
+/* Record events between the stages of every step (re-captures the step graph). */
+kf_status kf_session_set_profiling(kf_session* s, int on);
+/* Device durations (ms) of the last completed step: preprocess, raycast, ICP, fusion. */
+kf_status kf_session_stage_times(kf_session* s, float ms[4]);
+kf_status kf_batch_set_profiling(kf_batch* b, int on);
+kf_status kf_batch_stage_times(kf_batch* b, float ms[4]);
+/* Self-test of the bounded device-side waits: a cooperative launch whose barrier is never
+ * completed must give up after timeout_ms and report KF_ERR_TIMEOUT, leaving the context
+ * usable.  waited_ms (may be NULL) gets the wall time the launch took. */
+kf_status kf_selftest_bounded_wait(int timeout_ms, int* waited_ms);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* KF_API_H */

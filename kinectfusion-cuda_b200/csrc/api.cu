@@ -1,0 +1,1631 @@
+// api.cu -- the C ABI (include/kf_api.h): sessions, per-stage calls, batches and the server.
+//
+// Host orchestration replaces KinectFusion (project/src/kinect_fusion.cpp), ICP
+// (project/src/icp.cpp) and LinearLeastSquares (project/src/linear_least_squares.cpp).
+// An Engine owns a set of session slots and the four per-step launches (preprocess,
+// raycast, ICP, fusion) over all of them; the launches plus the result copy are captured
+// once into a CUDA graph and replayed every step.  Work lists and per-session parameters
+// live in device memory, so sessions can join and leave without re-capturing.
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "kf_host.h"
+
+using namespace kf;
+
+namespace {
+
+thread_local cudaError_t g_last_cuda = cudaSuccess;
+
+#define KF_CK(expr)                                  \
+    do {                                             \
+        cudaError_t e_ = (expr);                     \
+        if (e_ != cudaSuccess) {                     \
+            g_last_cuda = e_;                        \
+            return KF_ERR_CUDA;                      \
+        }                                            \
+    } while (0)
+
+#define KF_TRY(expr)                                 \
+    do {                                             \
+        kf_status s_ = (expr);                       \
+        if (s_ != KF_OK) return s_;                  \
+    } while (0)
+
+inline cudaStream_t as_stream(void* s) { return static_cast<cudaStream_t>(s); }
+
+// ---- configuration ----
+
+kf_status validate(const kf_config& c) {
+    if (c.width <= 0 || c.height <= 0) return KF_ERR_ARG;
+    if (c.levels < 1 || c.levels > KF_MAX_LEVELS) return KF_ERR_ARG;
+    const int div = 1 << (c.levels - 1);
+    // GridMapPyramid::checkGridDimensions (project/src/grid_map_pyramid.h:63-72)
+    if (c.width % div || c.height % div) return KF_ERR_SHAPE;
+    if (c.compat_trunc8 && (c.width % 8 || c.height % 8)) return KF_ERR_SHAPE;
+    if (c.volume_n < 8 || c.volume_n % 8) return KF_ERR_ARG;
+    if (!(c.volume_width > 0.f) || !(c.mu > 0.f)) return KF_ERR_ARG;
+    if (c.tsdf_format != KF_TSDF_F32F32 && c.tsdf_format != KF_TSDF_F16U16) return KF_ERR_ARG;
+    if (c.bilateral_radius < 0 || c.bilateral_radius > kMaxBilateralRadius) return KF_ERR_ARG;
+    if (!(c.bilateral_sigma_s > 0.f) || !(c.bilateral_sigma_r > 0.f)) return KF_ERR_ARG;
+    if (!(c.step_large > 0.f) || !(c.step_small > 0.f)) return KF_ERR_ARG;
+    // a march step must still advance t in float at the far end of the range
+    if (!(c.min_depth >= 0.f) || !(c.max_depth > c.min_depth) || !(c.max_depth < 1000.f)) return KF_ERR_ARG;
+    if (!(c.mu * c.step_small > c.max_depth * 1e-6f)) return KF_ERR_ARG;
+    int total = 0;
+    for (int l = 0; l < c.levels; ++l) {
+        if (c.iters[l] < 0) return KF_ERR_ARG;
+        total += c.iters[l];
+    }
+    if (total > kIcpMaxPasses) return KF_ERR_ARG;
+    return KF_OK;
+}
+
+size_t level_px(const kf_config& c, int l) { return size_t(c.width >> l) * size_t(c.height >> l); }
+
+size_t footprint(const kf_config& c) {
+    const size_t n3 = size_t(c.volume_n) * c.volume_n * c.volume_n;
+    size_t b = n3 * (c.tsdf_format == KF_TSDF_F16U16 ? 4 : 8);
+    b += size_t(c.width) * c.height * (2 + 4);
+    for (int l = 0; l < c.levels; ++l) {
+        b += level_px(c, l) * (4 + 16 * 3);
+        if (c.export_icp_mask) b += level_px(c, l);
+    }
+    b += sizeof(float) * 2 * c.volume_n + sizeof(PoseDev);
+    return b;
+}
+
+int cover8(int dim, int trunc) { return trunc ? (dim / 8) * 8 : dim; }
+int cover_icp(int dim, int trunc) {
+    if (!trunc) return dim;
+    const int t = std::min(dim - 1, 8);
+    if (t <= 0) return dim;
+    return (dim / t) * t;
+}
+
+void pose16_to_double(const float* p, double* R, double* t) {
+    for (int c = 0; c < 3; ++c)
+        for (int r = 0; r < 3; ++r) R[c * 3 + r] = p[c * 4 + r];
+    for (int r = 0; r < 3; ++r) t[r] = p[12 + r];
+}
+
+// initial device pose state: estimate = previous = pose, float mirrors, inverse
+PoseDev make_pose_dev(const float* pose16) {
+    PoseDev P;
+    std::memset(&P, 0, sizeof(P));
+    pose16_to_double(pose16, P.Rp, P.tp);
+    std::memcpy(P.R, P.Rp, sizeof(P.R));
+    std::memcpy(P.t, P.tp, sizeof(P.t));
+    for (int q = 0; q < 9; ++q) { P.Rpf[q] = float(P.Rp[q]); P.Rf[q] = P.Rpf[q]; }
+    for (int q = 0; q < 3; ++q) { P.tpf[q] = float(P.tp[q]); P.tf[q] = P.tpf[q]; }
+    for (int c = 0; c < 3; ++c)
+        for (int r = 0; r < 3; ++r) P.iRf[c * 3 + r] = float(P.Rp[r * 3 + c]);
+    for (int r = 0; r < 3; ++r)
+        P.itf[r] = float(-(P.Rp[r * 3 + 0] * P.tp[0] + P.Rp[r * 3 + 1] * P.tp[1] + P.Rp[r * 3 + 2] * P.tp[2]));
+    P.level = -1;
+    P.fuse_ok = 1;
+    return P;
+}
+
+// ---- one session's device resources ----
+
+struct Slot {
+    bool used = false;
+    kf_config cfg{};
+    SessionDev d{};
+    std::vector<void*> allocs;
+    size_t bytes = 0;
+    int frames = 0;
+    kf_frame_stats stats{};
+    float pose[16]{};
+    bool external = false;   // maps supplied by the caller (kf_compute_pose)
+
+    void* alloc(size_t nbytes, cudaError_t& err) {
+        void* p = nullptr;
+        err = cudaMalloc(&p, nbytes);
+        if (err != cudaSuccess) return nullptr;
+        allocs.push_back(p);
+        bytes += nbytes;
+        err = cudaMemset(p, 0, nbytes);
+        return p;
+    }
+    void release() {
+        for (void* p : allocs) cudaFree(p);
+        allocs.clear();
+        bytes = 0;
+        used = false;
+        external = false;
+        frames = 0;
+    }
+};
+
+// level geometry (shared by full sessions and external-map ICP runs)
+void fill_levels(SessionDev& d, const kf_config& c) {
+    d.W = c.width;
+    d.H = c.height;
+    d.L = c.levels;
+    for (int l = 0; l < KF_MAX_LEVELS; ++l) {
+        LevelDev& Lv = d.lv[l];
+        std::memset(&Lv, 0, sizeof(Lv));
+        if (l >= c.levels) continue;
+        Lv.w = c.width >> l;
+        Lv.h = c.height >> l;
+        Lv.cw = cover8(Lv.w, c.compat_trunc8);
+        Lv.ch = cover8(Lv.h, c.compat_trunc8);
+        Lv.icw = cover_icp(Lv.w, c.compat_trunc8);
+        Lv.ich = cover_icp(Lv.h, c.compat_trunc8);
+        float k[9], ik[9];
+        level_intrinsics(c, l, k, ik);
+        Lv.fx = k[0]; Lv.fy = k[4]; Lv.cx = k[6]; Lv.cy = k[7];
+        std::memcpy(Lv.ik, ik, sizeof(ik));
+    }
+    d.iters[0] = d.iters[1] = d.iters[2] = 0;
+    for (int l = 0; l < c.levels; ++l) d.iters[l] = c.iters[l];
+    d.dist_th = c.dist_thresh;
+    d.angle_th = c.angle_thresh;
+    d.stop_a = c.stop_angle;
+    d.stop_d = c.stop_dist;
+}
+
+kf_status slot_create(Slot& s, const kf_config& c) {
+    KF_TRY(validate(c));
+    s.release();
+    s.cfg = c;
+    SessionDev& d = s.d;
+    std::memset(&d, 0, sizeof(d));
+    fill_levels(d, c);
+    d.depth_scale = c.depth_scale;
+    d.unmirror = c.unmirror;
+    d.trunc8 = c.compat_trunc8;
+    d.bil_inv_ss = 1.0f / (c.bilateral_sigma_s * c.bilateral_sigma_s);
+    d.bil_inv_sr = 1.0f / (c.bilateral_sigma_r * c.bilateral_sigma_r);
+    d.down_thr = 3.0f * c.bilateral_sigma_r;
+    d.bil_r = c.bilateral_radius;
+    cudaError_t err = cudaSuccess;
+#define KF_ALLOC(ptr, type, bytes)                                   \
+    do {                                                             \
+        ptr = static_cast<type>(s.alloc((bytes), err));              \
+        if (err != cudaSuccess) { g_last_cuda = err; s.release(); return KF_ERR_CUDA; } \
+    } while (0)
+    const size_t px = size_t(c.width) * c.height;
+    uint16_t* raw;
+    KF_ALLOC(raw, uint16_t*, px * 2);
+    d.raw = raw;
+    KF_ALLOC(d.depth_m, float*, px * 4);
+    for (int l = 0; l < c.levels; ++l) {
+        const size_t np = level_px(c, l);
+        KF_ALLOC(d.depth[l], float*, np * 4);
+        KF_ALLOC(d.vmap[l], float4*, np * 16);
+        KF_ALLOC(d.pv[l], float4*, np * 16);
+        KF_ALLOC(d.pn[l], float4*, np * 16);
+        if (c.export_icp_mask) KF_ALLOC(d.mask[l], uint8_t*, np);
+    }
+    d.n = c.volume_n;
+    d.fmt = c.tsdf_format;
+    d.vol_w = c.volume_width;
+    d.res = c.volume_width / float(c.volume_n - 1);
+    d.mu = c.mu;
+    d.max_w = c.max_weight;
+    const size_t n3 = size_t(c.volume_n) * c.volume_n * c.volume_n;
+    const size_t es = c.tsdf_format == KF_TSDF_F16U16 ? 2 : 4;
+    KF_ALLOC(d.tf, void*, n3 * es);
+    KF_ALLOC(d.tw, void*, n3 * es);
+    float* xs;
+    float* zs;
+    KF_ALLOC(xs, float*, sizeof(float) * c.volume_n);
+    KF_ALLOC(zs, float*, sizeof(float) * c.volume_n);
+    {
+        std::vector<float> hx(c.volume_n), hz(c.volume_n);
+        voxel_axes(c.volume_n, c.volume_width, hx.data(), hz.data());
+        err = cudaMemcpy(xs, hx.data(), sizeof(float) * c.volume_n, cudaMemcpyHostToDevice);
+        if (err == cudaSuccess) err = cudaMemcpy(zs, hz.data(), sizeof(float) * c.volume_n, cudaMemcpyHostToDevice);
+        if (err != cudaSuccess) { g_last_cuda = err; s.release(); return KF_ERR_CUDA; }
+    }
+    d.xs = xs;
+    d.zs = zs;
+    d.min_d = c.min_depth;
+    d.max_d = c.max_depth;
+    d.step_l = c.step_large;
+    d.step_s = c.step_small;
+    d.keep_on_miss = c.keep_on_miss;
+    KF_ALLOC(d.pose, PoseDev*, sizeof(PoseDev));
+#undef KF_ALLOC
+    // grid {f = 2, w = 0} and pose = initial_pose (project/src/kinect_fusion.cpp:33-36, :80)
+    err = launch_init_volume(d.tf, d.tw, (long long)n3, d.fmt, 0);
+    if (err == cudaSuccess) {
+        PoseDev P = make_pose_dev(c.initial_pose);
+        err = cudaMemcpy(d.pose, &P, sizeof(P), cudaMemcpyHostToDevice);
+    }
+    if (err == cudaSuccess) err = cudaDeviceSynchronize();
+    if (err != cudaSuccess) { g_last_cuda = err; s.release(); return KF_ERR_CUDA; }
+    s.used = true;
+    s.frames = 0;
+    std::memcpy(s.pose, c.initial_pose, sizeof(s.pose));
+    s.stats = kf_frame_stats{};
+    s.stats.frame = -1;
+    return KF_OK;
+}
+
+kf_status slot_reset(Slot& s) {
+    const kf_config& c = s.cfg;
+    const size_t n3 = size_t(c.volume_n) * c.volume_n * c.volume_n;
+    KF_CK(launch_init_volume(s.d.tf, s.d.tw, (long long)n3, s.d.fmt, 0));
+    PoseDev P = make_pose_dev(c.initial_pose);
+    KF_CK(cudaMemcpy(s.d.pose, &P, sizeof(P), cudaMemcpyHostToDevice));
+    KF_CK(cudaDeviceSynchronize());
+    s.frames = 0;
+    std::memcpy(s.pose, c.initial_pose, sizeof(s.pose));
+    s.stats = kf_frame_stats{};
+    s.stats.frame = -1;
+    return KF_OK;
+}
+
+// ---- engine: slots + launches ----
+
+template <class T>
+kf_status grow(T*& ptr, int& cap, int need) {
+    if (need <= cap && ptr) return KF_OK;
+    int nc = std::max(need, std::max(16, cap * 2));
+    if (ptr) cudaFree(ptr);
+    ptr = nullptr;
+    KF_CK(cudaMalloc(&ptr, sizeof(T) * size_t(nc)));
+    KF_CK(cudaMemset(ptr, 0, sizeof(T) * size_t(nc)));
+    cap = nc;
+    return KF_OK;
+}
+
+struct Engine {
+    int sms = 148;
+    int cap = 0;
+    std::vector<Slot> slots;
+    // device
+    SessionDev* d_sess = nullptr;
+    StepDev* d_step = nullptr;
+    OutDev* d_out = nullptr;
+    Tables* d_tb = nullptr;
+    PreTile* d_pre = nullptr;
+    RayTile* d_ray = nullptr;
+    IcpTile* d_itiles = nullptr;
+    IcpRange* d_iranges = nullptr;
+    long long* d_fprefix = nullptr;
+    float* d_partials = nullptr;
+    GridSync* d_sync = nullptr;
+    unsigned int* d_ctr = nullptr;
+    int cap_pre = 0, cap_ray = 0, cap_it = 0, cap_part = 0;
+    // pinned host
+    StepDev* h_step = nullptr;
+    OutDev* h_out = nullptr;
+    GridSync* h_sync = nullptr;
+    Tables tb{};
+    bool tables_dirty = true;
+    bool step_dirty = true;
+    int grid_pre = 1, grid_ray = 1, grid_icp = 1, grid_fuse = 1;
+    // graph
+    bool use_graph = true;
+    bool graph_dirty = true;
+    cudaGraphExec_t gexec = nullptr;
+    cudaStream_t cap_stream = nullptr;
+    bool stages[4] = {true, true, true, true};
+    // per-stage timing: events between the launches (also inside the captured graph)
+    bool profile = false;
+    cudaEvent_t ev[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
+
+    kf_status init(int capacity) {
+        if (capacity <= 0 || capacity > 1024) return KF_ERR_ARG;   // ICP kernel keeps 1024 slots in smem
+        cap = capacity;
+        slots.resize(capacity);
+        int dev = 0;
+        KF_CK(cudaGetDevice(&dev));
+        KF_CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+        KF_CK(cudaMalloc(&d_sess, sizeof(SessionDev) * capacity));
+        KF_CK(cudaMemset(d_sess, 0, sizeof(SessionDev) * capacity));
+        KF_CK(cudaMalloc(&d_step, sizeof(StepDev) * capacity));
+        KF_CK(cudaMemset(d_step, 0, sizeof(StepDev) * capacity));
+        KF_CK(cudaMalloc(&d_out, sizeof(OutDev) * capacity));
+        KF_CK(cudaMemset(d_out, 0, sizeof(OutDev) * capacity));
+        KF_CK(cudaMalloc(&d_tb, sizeof(Tables)));
+        KF_CK(cudaMalloc(&d_iranges, sizeof(IcpRange) * KF_MAX_LEVELS * capacity));
+        KF_CK(cudaMemset(d_iranges, 0, sizeof(IcpRange) * KF_MAX_LEVELS * capacity));
+        KF_CK(cudaMalloc(&d_fprefix, sizeof(long long) * (capacity + 1)));
+        KF_CK(cudaMalloc(&d_sync, sizeof(GridSync)));
+        KF_CK(cudaMalloc(&d_ctr, sizeof(unsigned int) * 4));
+        KF_CK(cudaMallocHost(&h_step, sizeof(StepDev) * capacity));
+        KF_CK(cudaMallocHost(&h_out, sizeof(OutDev) * capacity));
+        KF_CK(cudaMallocHost(&h_sync, sizeof(GridSync)));
+        std::memset(h_step, 0, sizeof(StepDev) * capacity);
+        std::memset(h_out, 0, sizeof(OutDev) * capacity);
+        std::memset(h_sync, 0, sizeof(GridSync));
+        KF_CK(cudaStreamCreateWithFlags(&cap_stream, cudaStreamNonBlocking));
+        // persistent grids (kf_batch_autotune may replace the first, second and fourth)
+        grid_pre = sms * 4;
+        grid_ray = sms * 6;
+        grid_fuse = sms * 8;
+        grid_icp = icp_max_grid(sms);
+        return KF_OK;
+    }
+
+    kf_status set_profile(bool on) {
+        if (on)
+            for (cudaEvent_t& e : ev)
+                if (!e) KF_CK(cudaEventCreate(&e));
+        if (profile != on) graph_dirty = true;
+        profile = on;
+        return KF_OK;
+    }
+
+    // durations of the four stages of the last completed step (ms)
+    kf_status stage_times(float* ms) {
+        if (!profile) return KF_ERR_STATE;
+        for (int i = 0; i < 4; ++i) KF_CK(cudaEventElapsedTime(&ms[i], ev[i], ev[i + 1]));
+        return KF_OK;
+    }
+
+    void destroy() {
+        if (gexec) cudaGraphExecDestroy(gexec);
+        gexec = nullptr;
+        for (Slot& s : slots) if (!s.external) s.release();
+        for (cudaEvent_t& e : ev)
+            if (e) cudaEventDestroy(e);
+        cudaFree(d_sess); cudaFree(d_step); cudaFree(d_out); cudaFree(d_tb); cudaFree(d_pre); cudaFree(d_ray);
+        cudaFree(d_itiles); cudaFree(d_iranges); cudaFree(d_fprefix); cudaFree(d_partials); cudaFree(d_sync);
+        cudaFree(d_ctr);
+        cudaFreeHost(h_step); cudaFreeHost(h_out); cudaFreeHost(h_sync);
+        if (cap_stream) cudaStreamDestroy(cap_stream);
+    }
+
+    EngineView view() const {
+        EngineView v;
+        v.sess = d_sess; v.step = d_step; v.out = d_out; v.tb = d_tb; v.pre = d_pre; v.ray = d_ray;
+        v.itiles = d_itiles; v.iranges = d_iranges; v.fuse_prefix = d_fprefix; v.partials = d_partials;
+        v.sync = d_sync; v.counters = d_ctr;
+        return v;
+    }
+
+    // rebuild and upload work lists (synchronous; callers hold the engine)
+    kf_status build_tables() {
+        std::vector<PreTile> pre;
+        std::vector<RayTile> ray;
+        std::vector<IcpTile> it[KF_MAX_LEVELS];
+        std::vector<IcpRange> ranges(size_t(KF_MAX_LEVELS) * cap, IcpRange{0, 0});
+        std::vector<long long> fprefix(cap + 1, 0);
+        std::vector<SessionDev> sess(cap);
+        int max_levels = 1;
+        for (int s = 0; s < cap; ++s) {
+            const Slot& sl = slots[s];
+            fprefix[s + 1] = fprefix[s];
+            if (!sl.used) { std::memset(&sess[s], 0, sizeof(SessionDev)); continue; }
+            sess[s] = sl.d;
+            const kf_config& c = sl.cfg;
+            max_levels = std::max(max_levels, c.levels);
+            if (!sl.external) {
+                for (int y = 0; y < c.height; y += kPreTileSize)
+                    for (int x = 0; x < c.width; x += kPreTileSize) pre.push_back(PreTile{s, x, y});
+                for (int l = 0; l < c.levels; ++l) {
+                    const LevelDev& Lv = sl.d.lv[l];
+                    for (int y = 0; y < Lv.ch; y += kRayTileH)
+                        for (int x = 0; x < Lv.cw; x += kRayTileW) ray.push_back(RayTile{s, l, x, y});
+                }
+                fprefix[s + 1] += (long long)c.volume_n * c.volume_n * fuse_segs_per_row(c.volume_n, c.tsdf_format);
+            }
+            for (int l = 0; l < c.levels; ++l) {
+                const LevelDev& Lv = sl.d.lv[l];
+                const int np = Lv.icw * Lv.ich;
+                IcpRange rg;
+                rg.begin = int(it[l].size());
+                for (int p0 = 0; p0 < np; p0 += kIcpTilePx) it[l].push_back(IcpTile{s, p0, std::min(kIcpTilePx, np - p0)});
+                rg.end = int(it[l].size());
+                ranges[size_t(l) * cap + s] = rg;
+            }
+        }
+        // concatenate ICP levels; ranges become absolute
+        std::vector<IcpTile> all;
+        int off[KF_MAX_LEVELS];
+        for (int l = 0; l < KF_MAX_LEVELS; ++l) {
+            off[l] = int(all.size());
+            all.insert(all.end(), it[l].begin(), it[l].end());
+            for (int s = 0; s < cap; ++s) {
+                IcpRange& rg = ranges[size_t(l) * cap + s];
+                rg.begin += off[l];
+                rg.end += off[l];
+            }
+        }
+        const int old_pre = cap_pre, old_ray = cap_ray, old_it = cap_it, old_part = cap_part;
+        KF_TRY(grow(d_pre, cap_pre, std::max<int>(1, int(pre.size()))));
+        KF_TRY(grow(d_ray, cap_ray, std::max<int>(1, int(ray.size()))));
+        KF_TRY(grow(d_itiles, cap_it, std::max<int>(1, int(all.size()))));
+        KF_TRY(grow(d_partials, cap_part, std::max<int>(1, int(all.size())) * 54));
+        if (old_pre != cap_pre || old_ray != cap_ray || old_it != cap_it || old_part != cap_part) graph_dirty = true;
+        if (!pre.empty()) KF_CK(cudaMemcpy(d_pre, pre.data(), sizeof(PreTile) * pre.size(), cudaMemcpyHostToDevice));
+        if (!ray.empty()) KF_CK(cudaMemcpy(d_ray, ray.data(), sizeof(RayTile) * ray.size(), cudaMemcpyHostToDevice));
+        if (!all.empty()) KF_CK(cudaMemcpy(d_itiles, all.data(), sizeof(IcpTile) * all.size(), cudaMemcpyHostToDevice));
+        KF_CK(cudaMemcpy(d_iranges, ranges.data(), sizeof(IcpRange) * ranges.size(), cudaMemcpyHostToDevice));
+        KF_CK(cudaMemcpy(d_fprefix, fprefix.data(), sizeof(long long) * fprefix.size(), cudaMemcpyHostToDevice));
+        KF_CK(cudaMemcpy(d_sess, sess.data(), sizeof(SessionDev) * cap, cudaMemcpyHostToDevice));
+        tb.S = cap;
+        tb.n_pre = int(pre.size());
+        tb.n_ray = int(ray.size());
+        for (int l = 0; l < KF_MAX_LEVELS; ++l) {
+            tb.n_itiles[l] = int(it[l].size());
+            tb.icp_off[l] = off[l];
+        }
+        tb.max_levels = max_levels;
+        tb.fuse_total = fprefix[cap];
+        KF_CK(cudaMemcpy(d_tb, &tb, sizeof(Tables), cudaMemcpyHostToDevice));
+        tables_dirty = false;
+        return KF_OK;
+    }
+
+    // the per-step sequence
+    kf_status record(cudaStream_t st) {
+        const EngineView v = view();
+        KF_CK(cudaMemsetAsync(d_ctr, 0, sizeof(unsigned int) * 4, st));
+        KF_CK(cudaMemsetAsync(d_sync, 0, sizeof(GridSync), st));
+        if (profile) KF_CK(cudaEventRecord(ev[0], st));
+        if (stages[0]) KF_CK(launch_preprocess(v, grid_pre, st));
+        if (profile) KF_CK(cudaEventRecord(ev[1], st));
+        if (stages[1]) KF_CK(launch_raycast(v, grid_ray, st));
+        if (profile) KF_CK(cudaEventRecord(ev[2], st));
+        if (stages[2]) KF_CK(launch_icp(v, grid_icp, st));
+        if (profile) KF_CK(cudaEventRecord(ev[3], st));
+        if (stages[3]) KF_CK(launch_fuse(v, grid_fuse, st));
+        if (profile) KF_CK(cudaEventRecord(ev[4], st));
+        KF_CK(cudaMemcpyAsync(h_out, d_out, sizeof(OutDev) * cap, cudaMemcpyDeviceToHost, st));
+        KF_CK(cudaMemcpyAsync(h_sync, d_sync, sizeof(GridSync), cudaMemcpyDeviceToHost, st));
+        return KF_OK;
+    }
+
+    kf_status capture() {
+        if (gexec) { cudaGraphExecDestroy(gexec); gexec = nullptr; }
+        cudaGraph_t g = nullptr;
+        KF_CK(cudaStreamBeginCapture(cap_stream, cudaStreamCaptureModeThreadLocal));
+        kf_status rs = record(cap_stream);
+        cudaError_t e = cudaStreamEndCapture(cap_stream, &g);
+        if (rs != KF_OK || e != cudaSuccess) {
+            if (g) cudaGraphDestroy(g);
+            cudaGetLastError();
+            use_graph = false;   // e.g. a cooperative launch that cannot be captured
+            return KF_OK;
+        }
+        e = cudaGraphInstantiate(&gexec, g, 0);
+        cudaGraphDestroy(g);
+        if (e != cudaSuccess) {
+            cudaGetLastError();
+            gexec = nullptr;
+            use_graph = false;
+            return KF_OK;
+        }
+        graph_dirty = false;
+        return KF_OK;
+    }
+
+    kf_status enqueue(cudaStream_t st) {
+        if (tables_dirty) {
+            KF_CK(cudaStreamSynchronize(st));
+            KF_TRY(build_tables());
+        }
+        if (step_dirty) {
+            KF_CK(cudaMemcpyAsync(d_step, h_step, sizeof(StepDev) * cap, cudaMemcpyHostToDevice, st));
+            step_dirty = false;
+        }
+        if (use_graph) {
+            if (graph_dirty || !gexec) KF_TRY(capture());
+            if (use_graph) {
+                KF_CK(cudaGraphLaunch(gexec, st));
+                return KF_OK;
+            }
+        }
+        return record(st);
+    }
+
+    // set h_step; waits for in-flight work before touching pinned memory the stream may read
+    kf_status set_step(const std::vector<StepDev>& want, cudaStream_t st) {
+        bool same = true;
+        for (int s = 0; s < cap; ++s)
+            if (h_step[s].active != want[s].active || h_step[s].first != want[s].first) same = false;
+        if (same && !step_dirty) return KF_OK;
+        KF_CK(cudaStreamSynchronize(st));
+        for (int s = 0; s < cap; ++s) h_step[s] = want[s];
+        step_dirty = true;
+        return KF_OK;
+    }
+
+    // after the stream finished: pull per-session results
+    kf_status collect(const std::vector<StepDev>& want) {
+        kf_status worst = KF_OK;
+        const bool timed_out = h_sync->abort != 0;
+        for (int s = 0; s < cap; ++s) {
+            if (!want[s].active) continue;
+            Slot& sl = slots[s];
+            const OutDev& o = h_out[s];
+            std::memcpy(sl.pose, o.pose, sizeof(sl.pose));
+            sl.stats.frame = sl.frames;
+            sl.stats.status = timed_out ? KF_ERR_TIMEOUT : o.status;
+            for (int l = 0; l < KF_MAX_LEVELS; ++l) sl.stats.icp_iters[l] = o.iters[l];
+            sl.frames += 1;
+            if (sl.stats.status != KF_OK && worst == KF_OK) worst = kf_status(sl.stats.status);
+        }
+        return worst;
+    }
+};
+
+kf_status record_ms(cudaStream_t st, cudaEvent_t a, cudaEvent_t b, float* ms) {
+    KF_CK(cudaEventRecord(b, st));
+    KF_CK(cudaEventSynchronize(b));
+    KF_CK(cudaEventElapsedTime(ms, a, b));
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    return KF_OK;
+}
+
+// event pair around a stage call when the caller asks for its time (the reference's
+// kernel:: wrappers all return elapsed milliseconds)
+struct StageTimer {
+    cudaEvent_t a = nullptr, b = nullptr;
+    float* ms;
+    cudaStream_t st;
+    StageTimer(float* m, cudaStream_t s) : ms(m), st(s) {
+        if (ms) {
+            cudaEventCreate(&a);
+            cudaEventCreate(&b);
+            cudaEventRecord(a, st);
+        }
+    }
+    kf_status finish(cudaError_t launch) {
+        if (launch != cudaSuccess) {
+            g_last_cuda = launch;
+            if (ms) { cudaEventDestroy(a); cudaEventDestroy(b); }
+            return KF_ERR_CUDA;
+        }
+        if (!ms) return KF_OK;
+        return record_ms(st, a, b, ms);
+    }
+};
+
+}  // namespace
+
+// ------------------------------------------------------------------------------------------
+// shared host math
+// ------------------------------------------------------------------------------------------
+namespace kf {
+
+void voxel_axes(int n, float width, float* xs, float* zs) {
+    // project/src/tsdf.cu:27-31: x = -w/2 + i * res; z accumulated "+= resolution" in float
+    const float res = width / float(n - 1);
+    const float base = -width * 0.5f;
+    for (int i = 0; i < n; ++i) xs[i] = base + float(i) * res;
+    float z = base + (-res);
+    for (int k = 0; k < n; ++k) {
+        z = z + res;
+        zs[k] = z;
+    }
+}
+
+void level_intrinsics(const kf_config& c, int level, float k[9], float ik[9]) {
+    // Sensor (project/src/sensor.h:14-19): f / 2^l, principal point (c + 0.5) / 2^l - 0.5
+    const float s = 1.0f / float(1 << level);
+    const float fx = c.fx * s, fy = c.fy * s;
+    const float cx = (c.cx + 0.5f) * s - 0.5f, cy = (c.cy + 0.5f) * s - 0.5f;
+    const float m[9] = {fx, 0.f, 0.f, 0.f, fy, 0.f, cx, cy, 1.f};
+    std::memcpy(k, m, sizeof(m));
+    // adjugate / determinant (glm::inverse of the 3x3)
+    const float a = m[0], b = m[3], cc = m[6], d = m[1], e = m[4], f = m[7], g = m[2], h = m[5], i = m[8];
+    const float det = a * (e * i - f * h) - b * (d * i - f * g) + cc * (d * h - e * g);
+    const float od = 1.0f / det;
+    ik[0] = (e * i - f * h) * od;  ik[3] = -(b * i - cc * h) * od; ik[6] = (b * f - cc * e) * od;
+    ik[1] = -(d * i - f * g) * od; ik[4] = (a * i - cc * g) * od;  ik[7] = -(a * f - cc * d) * od;
+    ik[2] = (d * h - e * g) * od;  ik[5] = -(a * h - b * g) * od;  ik[8] = (a * e - b * d) * od;
+}
+
+}  // namespace kf
+
+// ------------------------------------------------------------------------------------------
+// C ABI
+// ------------------------------------------------------------------------------------------
+// a session is a slot of an engine: its own (kf_session_create) or a batch's / server's
+struct kf_session {
+    Engine* eng = nullptr;
+    int slot = 0;
+    bool owns = false;
+    Slot& sl() { return eng->slots[slot]; }
+};
+
+struct kf_batch {
+    Engine eng;
+    int n = 0;
+    std::vector<kf_session*> views;
+};
+
+extern "C" {
+
+int kf_api_version(void) { return KF_API_VERSION; }
+
+const char* kf_status_string(int s) {
+    switch (s) {
+        case KF_OK: return "ok";
+        case KF_ERR_ARG: return "invalid argument";
+        case KF_ERR_SHAPE: return "map sizes do not match";
+        case KF_ERR_CUDA: return cudaGetErrorString(g_last_cuda);
+        case KF_ERR_NONFINITE: return "ICP solution not finite";
+        case KF_ERR_OOM_BUDGET: return "session does not fit the HBM budget";
+        case KF_ERR_TIMEOUT: return "device wait timed out";
+        case KF_ERR_STATE: return "call not valid in this state";
+        case KF_ERR_CAPACITY: return "no free slot";
+        default: return "unknown status";
+    }
+}
+
+void kf_config_default(kf_config* c) {
+    if (!c) return;
+    std::memset(c, 0, sizeof(*c));
+    const float pi = 3.14159265358979323846f;
+    // project/src/main.cpp:11-59 (dataset configuration)
+    c->width = 640;
+    c->height = 480;
+    c->fx = c->fy = 525.0f;
+    c->cx = 319.5f;                 // project/src/sensor.h:14
+    c->cy = 239.5f;
+    c->depth_scale = 1.0f / 5000.0f;
+    c->unmirror = 0;
+    c->levels = 3;
+    c->iters[0] = 10; c->iters[1] = 5; c->iters[2] = 3;
+    c->dist_thresh = 0.4f;
+    c->angle_thresh = 4.0f * pi / 18.0f;
+    c->stop_angle = 0.1f * pi / 180.0f;    // glm::radians(0.1f)
+    c->stop_dist = 0.01f;
+    c->bilateral_sigma_s = 4.0f;    // project/src/measurement.cu:11-12, :38
+    c->bilateral_sigma_r = 0.25f;
+    c->bilateral_radius = 3;
+    c->volume_n = 256;              // fusion volume: 8 m, 256^3, mu = 3 voxels
+    c->volume_width = 8.0f;
+    c->mu = 3.0f * (8.0f / 255.0f);
+    c->max_weight = 0.0f;
+    c->tsdf_format = KF_TSDF_F32F32;
+    c->min_depth = 0.4f;            // project/src/tsdf.cuh:11-12
+    c->max_depth = 6.0f;
+    c->step_large = 1.99f;          // project/src/raycast.cu:75-76
+    c->step_small = 0.1f;
+    c->compat_trunc8 = 0;
+    c->keep_on_miss = 1;
+    c->export_icp_mask = 0;
+    for (int i = 0; i < 16; ++i) c->initial_pose[i] = (i % 5 == 0) ? 1.0f : 0.0f;
+}
+
+kf_status kf_session_footprint(const kf_config* cfg, size_t* bytes) {
+    if (!cfg || !bytes) return KF_ERR_ARG;
+    KF_TRY(validate(*cfg));
+    *bytes = footprint(*cfg);
+    return KF_OK;
+}
+
+kf_status kf_session_create(const kf_config* cfg, kf_session** out) {
+    if (!cfg || !out) return KF_ERR_ARG;
+    KF_TRY(validate(*cfg));
+    kf_session* s = new (std::nothrow) kf_session;
+    if (!s) return KF_ERR_ARG;
+    s->eng = new (std::nothrow) Engine;
+    if (!s->eng) { delete s; return KF_ERR_ARG; }
+    s->owns = true;
+    kf_status st = s->eng->init(1);
+    if (st == KF_OK) st = slot_create(s->eng->slots[0], *cfg);
+    if (st != KF_OK) { s->eng->destroy(); delete s->eng; delete s; return st; }
+    s->eng->tables_dirty = true;
+    *out = s;
+    return KF_OK;
+}
+
+kf_status kf_session_destroy(kf_session* s) {
+    if (!s) return KF_ERR_ARG;
+    if (!s->owns) return KF_ERR_STATE;   // batch / server members go with their owner
+    cudaDeviceSynchronize();
+    s->eng->destroy();
+    delete s->eng;
+    delete s;
+    return KF_OK;
+}
+
+kf_status kf_session_reset(kf_session* s) {
+    if (!s) return KF_ERR_ARG;
+    KF_CK(cudaDeviceSynchronize());
+    return slot_reset(s->sl());
+}
+
+static kf_status session_enqueue(kf_session* s, const uint16_t* depth, int is_dev, cudaStream_t st) {
+    Slot& sl = s->sl();
+    const size_t bytes = size_t(sl.cfg.width) * sl.cfg.height * 2;
+    std::vector<StepDev> want(s->eng->cap, StepDev{0, 0});
+    want[s->slot] = StepDev{1, sl.frames == 0 ? 1 : 0};
+    KF_TRY(s->eng->set_step(want, st));
+    KF_CK(cudaMemcpyAsync(const_cast<uint16_t*>(sl.d.raw), depth, bytes,
+                          is_dev ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, st));
+    return s->eng->enqueue(st);
+}
+
+kf_status kf_process_frame(kf_session* s, const uint16_t* depth, int is_device_ptr, void* stream, float pose_out[16]) {
+    if (!s || !depth) return KF_ERR_ARG;
+    cudaStream_t st = as_stream(stream);
+    KF_TRY(session_enqueue(s, depth, is_device_ptr, st));
+    KF_CK(cudaStreamSynchronize(st));
+    std::vector<StepDev> want(s->eng->cap, StepDev{0, 0});
+    want[s->slot] = StepDev{1, 0};
+    kf_status r = s->eng->collect(want);
+    if (pose_out) std::memcpy(pose_out, s->sl().pose, sizeof(float) * 16);
+    return r;
+}
+
+kf_status kf_process_frame_async(kf_session* s, const uint16_t* depth_device, void* stream) {
+    if (!s || !depth_device) return KF_ERR_ARG;
+    cudaStream_t st = as_stream(stream);
+    KF_TRY(session_enqueue(s, depth_device, 1, st));
+    // results stay on the device; the frame counter advances here
+    s->sl().frames += 1;
+    return KF_OK;
+}
+
+kf_status kf_get_pose(kf_session* s, float pose[16]) {
+    if (!s || !pose) return KF_ERR_ARG;
+    // read the device state (also valid after async frames once the stream is idle)
+    PoseDev P;
+    KF_CK(cudaMemcpy(&P, s->sl().d.pose, sizeof(P), cudaMemcpyDeviceToHost));
+    for (int i = 0; i < 16; ++i) pose[i] = 0.f;
+    for (int c = 0; c < 3; ++c)
+        for (int r = 0; r < 3; ++r) pose[c * 4 + r] = float(P.Rp[c * 3 + r]);
+    for (int r = 0; r < 3; ++r) pose[12 + r] = float(P.tp[r]);
+    pose[15] = 1.f;
+    return KF_OK;
+}
+
+kf_status kf_set_pose(kf_session* s, const float pose[16]) {
+    if (!s || !pose) return KF_ERR_ARG;
+    KF_CK(cudaDeviceSynchronize());
+    PoseDev old;
+    KF_CK(cudaMemcpy(&old, s->sl().d.pose, sizeof(old), cudaMemcpyDeviceToHost));
+    PoseDev P = make_pose_dev(pose);
+    P.frame = old.frame;
+    KF_CK(cudaMemcpy(s->sl().d.pose, &P, sizeof(P), cudaMemcpyHostToDevice));
+    std::memcpy(s->sl().pose, pose, sizeof(float) * 16);
+    return KF_OK;
+}
+
+kf_status kf_get_frame_stats(kf_session* s, kf_frame_stats* out) {
+    if (!s || !out) return KF_ERR_ARG;
+    *out = s->sl().stats;
+    return KF_OK;
+}
+
+static kf_status copy_out(void* dst, const void* src, size_t bytes, int to_host) {
+    KF_CK(cudaDeviceSynchronize());
+    KF_CK(cudaMemcpy(dst, src, bytes, to_host ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice));
+    return KF_OK;
+}
+
+kf_status kf_get_depth(kf_session* s, int level, float* dst, int to_host) {
+    if (!s || !dst) return KF_ERR_ARG;
+    const Slot& sl = s->sl();
+    if (level == -1) return copy_out(dst, sl.d.depth_m, size_t(sl.cfg.width) * sl.cfg.height * 4, to_host);
+    if (level < 0 || level >= sl.cfg.levels) return KF_ERR_ARG;
+    return copy_out(dst, sl.d.depth[level], level_px(sl.cfg, level) * 4, to_host);
+}
+
+kf_status kf_get_vertex(kf_session* s, int level, float* dst, int to_host) {
+    if (!s || !dst) return KF_ERR_ARG;
+    const Slot& sl = s->sl();
+    if (level < 0 || level >= sl.cfg.levels) return KF_ERR_ARG;
+    return copy_out(dst, sl.d.vmap[level], level_px(sl.cfg, level) * 16, to_host);
+}
+
+kf_status kf_get_raycast(kf_session* s, int level, float* vertex, float* normal, int to_host) {
+    if (!s) return KF_ERR_ARG;
+    const Slot& sl = s->sl();
+    if (level < 0 || level >= sl.cfg.levels) return KF_ERR_ARG;
+    if (vertex) KF_TRY(copy_out(vertex, sl.d.pv[level], level_px(sl.cfg, level) * 16, to_host));
+    if (normal) KF_TRY(copy_out(normal, sl.d.pn[level], level_px(sl.cfg, level) * 16, to_host));
+    return KF_OK;
+}
+
+kf_status kf_get_icp_mask(kf_session* s, int level, uint8_t* dst, int to_host) {
+    if (!s || !dst) return KF_ERR_ARG;
+    const Slot& sl = s->sl();
+    if (level < 0 || level >= sl.cfg.levels || !sl.d.mask[level]) return KF_ERR_STATE;
+    return copy_out(dst, sl.d.mask[level], level_px(sl.cfg, level), to_host);
+}
+
+kf_status kf_get_tsdf(kf_session* s, void* dst, size_t dst_bytes, int layout, int to_host) {
+    if (!s || !dst) return KF_ERR_ARG;
+    const Slot& sl = s->sl();
+    const size_t n3 = size_t(sl.cfg.volume_n) * sl.cfg.volume_n * sl.cfg.volume_n;
+    const size_t es = sl.d.fmt == KF_TSDF_F16U16 ? 2 : 4;
+    KF_CK(cudaDeviceSynchronize());
+    const cudaMemcpyKind kind = to_host ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice;
+    if (layout == 0) {
+        if (dst_bytes < 2 * n3 * es) return KF_ERR_SHAPE;
+        KF_CK(cudaMemcpy(dst, sl.d.tf, n3 * es, kind));
+        KF_CK(cudaMemcpy(static_cast<char*>(dst) + n3 * es, sl.d.tw, n3 * es, kind));
+        return KF_OK;
+    }
+    if (layout != 1) return KF_ERR_ARG;
+    if (dst_bytes < n3 * 8) return KF_ERR_SHAPE;
+    float* tmp = nullptr;
+    if (to_host) KF_CK(cudaMalloc(&tmp, n3 * 8));
+    float* target = to_host ? tmp : static_cast<float*>(dst);
+    cudaError_t e = launch_export_interleaved(sl.d.tf, sl.d.tw, (long long)n3, sl.d.fmt, target, 0);
+    if (e == cudaSuccess) e = cudaDeviceSynchronize();
+    if (e == cudaSuccess && to_host) e = cudaMemcpy(dst, tmp, n3 * 8, cudaMemcpyDeviceToHost);
+    if (tmp) cudaFree(tmp);
+    KF_CK(e);
+    return KF_OK;
+}
+
+kf_status kf_set_tsdf(kf_session* s, const void* src, size_t src_bytes, int layout, int from_host) {
+    if (!s || !src) return KF_ERR_ARG;
+    Slot& sl = s->sl();
+    const size_t n3 = size_t(sl.cfg.volume_n) * sl.cfg.volume_n * sl.cfg.volume_n;
+    const size_t es = sl.d.fmt == KF_TSDF_F16U16 ? 2 : 4;
+    KF_CK(cudaDeviceSynchronize());
+    const cudaMemcpyKind kind = from_host ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice;
+    if (layout == 0) {
+        if (src_bytes < 2 * n3 * es) return KF_ERR_SHAPE;
+        KF_CK(cudaMemcpy(sl.d.tf, src, n3 * es, kind));
+        KF_CK(cudaMemcpy(sl.d.tw, static_cast<const char*>(src) + n3 * es, n3 * es, kind));
+        return KF_OK;
+    }
+    if (layout != 1) return KF_ERR_ARG;
+    if (src_bytes < n3 * 8) return KF_ERR_SHAPE;
+    float* tmp = nullptr;
+    const float* from = static_cast<const float*>(src);
+    if (from_host) {
+        KF_CK(cudaMalloc(&tmp, n3 * 8));
+        KF_CK(cudaMemcpy(tmp, src, n3 * 8, cudaMemcpyHostToDevice));
+        from = tmp;
+    }
+    cudaError_t e = launch_import_interleaved(from, sl.d.tf, sl.d.tw, (long long)n3, sl.d.fmt, 0);
+    if (e == cudaSuccess) e = cudaDeviceSynchronize();
+    if (tmp) cudaFree(tmp);
+    KF_CK(e);
+    return KF_OK;
+}
+
+kf_status kf_get_volume(kf_session* s, kf_volume* out) {
+    if (!s || !out) return KF_ERR_ARG;
+    const Slot& sl = s->sl();
+    out->f = sl.d.tf;
+    out->w = sl.d.tw;
+    out->n = sl.cfg.volume_n;
+    out->width = sl.cfg.volume_width;
+    out->mu = sl.cfg.mu;
+    out->format = sl.cfg.tsdf_format;
+    out->max_weight = sl.cfg.max_weight;
+    return KF_OK;
+}
+
+// ---- stages ----
+
+kf_status kf_convert_to_depth_meters(const uint16_t* raw, int w, int h, float* out, int out_w, int out_h, float scale,
+                                     int unmirror, void* stream, float* elapsed_ms) {
+    if (!raw || !out || w <= 0 || h <= 0) return KF_ERR_ARG;
+    if (w != out_w || h != out_h) return KF_ERR_SHAPE;
+    StageTimer t(elapsed_ms, as_stream(stream));
+    return t.finish(stage_convert(raw, out, w, h, scale, unmirror, as_stream(stream)));
+}
+
+kf_status kf_apply_bilateral_filter(const float* in, int w, int h, float* out, int out_w, int out_h, float sigma_s,
+                                    float sigma_r, int radius, void* stream, float* elapsed_ms) {
+    if (!in || !out || w <= 0 || h <= 0 || radius < 0 || radius > kMaxBilateralRadius) return KF_ERR_ARG;
+    if (w != out_w || h != out_h) return KF_ERR_SHAPE;
+    StageTimer t(elapsed_ms, as_stream(stream));
+    return t.finish(stage_bilateral(in, out, w, h, sigma_s, sigma_r, radius, as_stream(stream)));
+}
+
+kf_status kf_down_sample(const float* in, int w, int h, float* out, int out_w, int out_h, float sigma_r, void* stream,
+                         float* elapsed_ms) {
+    if (!in || !out || out_w <= 0 || out_h <= 0) return KF_ERR_ARG;
+    // project/src/measurement.cu:186-189
+    if (w / out_w != 2 || h / out_h != 2) return KF_ERR_SHAPE;
+    StageTimer t(elapsed_ms, as_stream(stream));
+    return t.finish(stage_down_sample(in, out, out_w, out_h, sigma_r, as_stream(stream)));
+}
+
+kf_status kf_create_vertex_map(const float* depth, int w, int h, float* vertex, int out_w, int out_h,
+                               const float inv_cam_k[9], void* stream, float* elapsed_ms) {
+    if (!depth || !vertex || !inv_cam_k || w <= 0 || h <= 0) return KF_ERR_ARG;
+    if (w != out_w || h != out_h) return KF_ERR_SHAPE;
+    StageTimer t(elapsed_ms, as_stream(stream));
+    return t.finish(stage_vertex(depth, reinterpret_cast<float4*>(vertex), w, h, inv_cam_k, as_stream(stream)));
+}
+
+kf_status kf_create_normal_map(const float* vertex, int w, int h, float* normal, int out_w, int out_h, void* stream,
+                               float* elapsed_ms) {
+    if (!vertex || !normal || w <= 0 || h <= 0) return KF_ERR_ARG;
+    if (w != out_w || h != out_h) return KF_ERR_SHAPE;
+    StageTimer t(elapsed_ms, as_stream(stream));
+    return t.finish(stage_normal(reinterpret_cast<const float4*>(vertex), reinterpret_cast<float4*>(normal), w, h,
+                                 as_stream(stream)));
+}
+
+static kf_status check_volume(const kf_volume* v) {
+    if (!v || !v->f || !v->w || v->n < 8 || v->n % 8) return KF_ERR_ARG;
+    if (v->format != KF_TSDF_F32F32 && v->format != KF_TSDF_F16U16) return KF_ERR_ARG;
+    if (!(v->width > 0.f) || !(v->mu > 0.f)) return KF_ERR_ARG;
+    return KF_OK;
+}
+
+kf_status kf_initialize_grid(const kf_volume* vol, void* stream, float* elapsed_ms) {
+    KF_TRY(check_volume(vol));
+    const long long n3 = (long long)vol->n * vol->n * vol->n;
+    StageTimer t(elapsed_ms, as_stream(stream));
+    return t.finish(launch_init_volume(vol->f, vol->w, n3, vol->format, as_stream(stream)));
+}
+
+kf_status kf_fuse(const float* depth_m, int w, int h, const float cam_k[9], const kf_volume* vol, const float pose[16],
+                  float min_depth, float max_depth, void* stream, float* elapsed_ms) {
+    if (!depth_m || !cam_k || !pose || w <= 0 || h <= 0) return KF_ERR_ARG;
+    KF_TRY(check_volume(vol));
+    std::vector<float> xs(vol->n), zs(vol->n);
+    voxel_axes(vol->n, vol->width, xs.data(), zs.data());
+    float* d_ax = nullptr;
+    KF_CK(cudaMalloc(&d_ax, sizeof(float) * 2 * vol->n));
+    cudaStream_t st = as_stream(stream);
+    cudaError_t e = cudaMemcpyAsync(d_ax, xs.data(), sizeof(float) * vol->n, cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(d_ax + vol->n, zs.data(), sizeof(float) * vol->n, cudaMemcpyHostToDevice, st);
+    StageTimer t(elapsed_ms, st);
+    if (e == cudaSuccess) e = stage_fuse(depth_m, w, h, cam_k, vol, pose, min_depth, max_depth, d_ax, d_ax + vol->n, st);
+    kf_status r = t.finish(e);
+    cudaStreamSynchronize(st);
+    cudaFree(d_ax);
+    return r;
+}
+
+kf_status kf_raycast(const kf_volume* vol, const float pose[16], const float inv_cam_k[9], float* vertex, int w, int h,
+                     float* normal, int nw, int nh, float min_depth, float max_depth, float step_large,
+                     float step_small, void* stream, float* elapsed_ms) {
+    if (!pose || !inv_cam_k || !vertex || !normal || w <= 0 || h <= 0) return KF_ERR_ARG;
+    KF_TRY(check_volume(vol));
+    if (w != nw || h != nh) return KF_ERR_SHAPE;   // project/src/raycast.cu:155-158
+    if (!(step_large > 0.f) || !(max_depth > min_depth) || !(max_depth < 1000.f) ||
+        !(vol->mu * step_small > max_depth * 1e-6f))
+        return KF_ERR_ARG;
+    StageTimer t(elapsed_ms, as_stream(stream));
+    return t.finish(stage_raycast(vol, pose, inv_cam_k, reinterpret_cast<float4*>(vertex),
+                                  reinterpret_cast<float4*>(normal), w, h, min_depth, max_depth, step_large,
+                                  step_small, as_stream(stream)));
+}
+
+kf_status kf_construct_icp_residuals(const float* vertex, const float* target_vertex, const float* target_normal, int w,
+                                     int h, const float prev_rot[9], const float prev_transl[3], const float cur_rot[9],
+                                     const float cur_transl[3], const float cam_k[9], float distance_thresh,
+                                     float angle_thresh, float* mat_a, float* vec_b, void* stream, float* elapsed_ms) {
+    if (!vertex || !target_vertex || !target_normal || !prev_rot || !prev_transl || !cur_rot || !cur_transl ||
+        !cam_k || !mat_a || !vec_b || w <= 0 || h <= 0)
+        return KF_ERR_ARG;
+    StageTimer t(elapsed_ms, as_stream(stream));
+    return t.finish(stage_icp_residuals(reinterpret_cast<const float4*>(vertex),
+                                        reinterpret_cast<const float4*>(target_vertex),
+                                        reinterpret_cast<const float4*>(target_normal), w, h, prev_rot, prev_transl,
+                                        cur_rot, cur_transl, cam_k, distance_thresh, angle_thresh, mat_a, vec_b,
+                                        as_stream(stream)));
+}
+
+// scratch of kf_solve_linear_least_squares: block partials + the FP64 solution, kept per
+// process and grown on demand
+static std::mutex g_lls_mu;
+static float* g_lls_partials = nullptr;
+static int g_lls_cap = 0;
+static double* g_lls_x = nullptr;
+
+kf_status kf_solve_linear_least_squares(const float* mat_a, const float* vec_b, int n, float x_out[6], void* stream) {
+    if (!mat_a || !vec_b || !x_out || n <= 0) return KF_ERR_ARG;
+    std::lock_guard<std::mutex> lk(g_lls_mu);
+    const int nb = lls_num_blocks(n);
+    if (nb > g_lls_cap || !g_lls_partials) {
+        if (g_lls_partials) cudaFree(g_lls_partials);
+        g_lls_partials = nullptr;
+        KF_CK(cudaMalloc(&g_lls_partials, sizeof(float) * 54 * size_t(nb)));
+        g_lls_cap = nb;
+    }
+    if (!g_lls_x) KF_CK(cudaMalloc(&g_lls_x, sizeof(double) * 6));
+    cudaStream_t st = as_stream(stream);
+    KF_CK(stage_lls(mat_a, vec_b, n, g_lls_partials, g_lls_x, nb, st));
+    double x[6];
+    KF_CK(cudaMemcpyAsync(x, g_lls_x, sizeof(x), cudaMemcpyDeviceToHost, st));
+    KF_CK(cudaStreamSynchronize(st));
+    for (int q = 0; q < 6; ++q) x_out[q] = float(x[q]);
+    for (int q = 0; q < 6; ++q)
+        if (!std::isfinite(x[q])) return KF_ERR_NONFINITE;
+    return KF_OK;
+}
+
+kf_status kf_compute_pose(const float* const* vertex, const float* const* target_vertex,
+                          const float* const* target_normal, int w, int h, int levels, const kf_config* cfg,
+                          const float pose[16], float pose_out[16], int iters_out[KF_MAX_LEVELS], void* stream) {
+    if (!vertex || !target_vertex || !target_normal || !cfg || !pose || !pose_out) return KF_ERR_ARG;
+    if (levels < 1 || levels > KF_MAX_LEVELS) return KF_ERR_ARG;
+    kf_config c = *cfg;
+    c.width = w;
+    c.height = h;
+    c.levels = levels;
+    c.export_icp_mask = 0;
+    const int div = 1 << (levels - 1);
+    if (w % div || h % div) return KF_ERR_SHAPE;
+    int total = 0;
+    for (int l = 0; l < levels; ++l) total += std::max(0, c.iters[l]);
+    if (total > kIcpMaxPasses) return KF_ERR_ARG;
+    for (int l = 0; l < levels; ++l)
+        if (!vertex[l] || !target_vertex[l] || !target_normal[l]) return KF_ERR_ARG;
+    Engine eng;
+    kf_status st = eng.init(1);
+    if (st != KF_OK) { eng.destroy(); return st; }
+    Slot& sl = eng.slots[0];
+    sl.cfg = c;
+    sl.used = true;
+    sl.external = true;
+    std::memset(&sl.d, 0, sizeof(sl.d));
+    fill_levels(sl.d, c);
+    for (int l = 0; l < levels; ++l) {
+        sl.d.vmap[l] = reinterpret_cast<float4*>(const_cast<float*>(vertex[l]));
+        sl.d.pv[l] = reinterpret_cast<float4*>(const_cast<float*>(target_vertex[l]));
+        sl.d.pn[l] = reinterpret_cast<float4*>(const_cast<float*>(target_normal[l]));
+    }
+    PoseDev* d_pose = nullptr;
+    cudaStream_t s = as_stream(stream);
+    auto fail = [&](cudaError_t e) {
+        g_last_cuda = e;
+        if (d_pose) cudaFree(d_pose);
+        eng.destroy();
+        return KF_ERR_CUDA;
+    };
+    cudaError_t e = cudaMalloc(&d_pose, sizeof(PoseDev));
+    if (e != cudaSuccess) return fail(e);
+    PoseDev P = make_pose_dev(pose);
+    e = cudaMemcpy(d_pose, &P, sizeof(P), cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) return fail(e);
+    sl.d.pose = d_pose;
+    st = eng.build_tables();
+    if (st != KF_OK) { cudaFree(d_pose); eng.destroy(); return st; }
+    StepDev step{1, 0};
+    e = cudaMemcpy(eng.d_step, &step, sizeof(step), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemsetAsync(eng.d_sync, 0, sizeof(GridSync), s);
+    if (e == cudaSuccess) e = launch_icp(eng.view(), eng.grid_icp, s);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(eng.h_out, eng.d_out, sizeof(OutDev), cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(eng.h_sync, eng.d_sync, sizeof(GridSync), cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) return fail(e);
+    std::memcpy(pose_out, eng.h_out[0].pose, sizeof(float) * 16);
+    if (iters_out)
+        for (int l = 0; l < KF_MAX_LEVELS; ++l) iters_out[l] = eng.h_out[0].iters[l];
+    kf_status r = eng.h_sync->abort ? KF_ERR_TIMEOUT : kf_status(eng.h_out[0].status);
+    cudaFree(d_pose);
+    eng.destroy();
+    return r;
+}
+
+kf_status kf_pose_error(const float p1[16], const float p2[16], float out[2]) {
+    if (!p1 || !p2 || !out) return KF_ERR_ARG;
+    // project/src/general_helper.cpp:11-21 in float
+    const float inv = 1.0f / std::sqrt(3.0f);
+    const float v[3] = {inv, inv, inv};
+    float a[3], b[3];
+    for (int r = 0; r < 3; ++r) {
+        a[r] = p1[r] * v[0] + p1[4 + r] * v[1] + p1[8 + r] * v[2];
+        b[r] = p2[r] * v[0] + p2[4 + r] * v[1] + p2[8 + r] * v[2];
+    }
+    out[0] = std::sqrt((a[0] - b[0]) * (a[0] - b[0]) + (a[1] - b[1]) * (a[1] - b[1]) + (a[2] - b[2]) * (a[2] - b[2]));
+    out[1] = std::sqrt((p1[12] - p2[12]) * (p1[12] - p2[12]) + (p1[13] - p2[13]) * (p1[13] - p2[13]) +
+                       (p1[14] - p2[14]) * (p1[14] - p2[14]));
+    return KF_OK;
+}
+
+// ---- batch ----
+
+kf_status kf_batch_create(const kf_config* cfgs, int n, kf_batch** out) {
+    if (!cfgs || n <= 0 || !out) return KF_ERR_ARG;
+    for (int i = 0; i < n; ++i) KF_TRY(validate(cfgs[i]));
+    kf_batch* b = new (std::nothrow) kf_batch;
+    if (!b) return KF_ERR_ARG;
+    b->n = n;
+    kf_status st = b->eng.init(n);
+    for (int i = 0; i < n && st == KF_OK; ++i) st = slot_create(b->eng.slots[i], cfgs[i]);
+    if (st != KF_OK) { b->eng.destroy(); delete b; return st; }
+    b->eng.tables_dirty = true;
+    *out = b;
+    return KF_OK;
+}
+
+kf_status kf_batch_destroy(kf_batch* b) {
+    if (!b) return KF_ERR_ARG;
+    cudaDeviceSynchronize();
+    for (kf_session* v : b->views) delete v;
+    b->eng.destroy();
+    delete b;
+    return KF_OK;
+}
+
+kf_status kf_batch_step(kf_batch* b, const uint16_t* const* depth, int is_device_ptr, void* stream, float* poses_out) {
+    if (!b || !depth) return KF_ERR_ARG;
+    cudaStream_t st = as_stream(stream);
+    std::vector<StepDev> want(b->n);
+    for (int i = 0; i < b->n; ++i) {
+        Slot& sl = b->eng.slots[i];
+        want[i] = StepDev{depth[i] ? 1 : 0, sl.frames == 0 ? 1 : 0};
+    }
+    KF_TRY(b->eng.set_step(want, st));
+    for (int i = 0; i < b->n; ++i) {
+        if (!depth[i]) continue;
+        Slot& sl = b->eng.slots[i];
+        KF_CK(cudaMemcpyAsync(const_cast<uint16_t*>(sl.d.raw), depth[i], size_t(sl.cfg.width) * sl.cfg.height * 2,
+                              is_device_ptr ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, st));
+    }
+    KF_TRY(b->eng.enqueue(st));
+    KF_CK(cudaStreamSynchronize(st));
+    kf_status r = b->eng.collect(want);
+    if (poses_out)
+        for (int i = 0; i < b->n; ++i) std::memcpy(poses_out + 16 * size_t(i), b->eng.slots[i].pose, sizeof(float) * 16);
+    return r;
+}
+
+kf_status kf_batch_step_async(kf_batch* b, const int* active, void* stream) {
+    if (!b || !active) return KF_ERR_ARG;
+    cudaStream_t st = as_stream(stream);
+    std::vector<StepDev> want(b->n);
+    for (int i = 0; i < b->n; ++i) want[i] = StepDev{active[i] ? 1 : 0, b->eng.slots[i].frames == 0 ? 1 : 0};
+    KF_TRY(b->eng.set_step(want, st));
+    KF_TRY(b->eng.enqueue(st));
+    for (int i = 0; i < b->n; ++i)
+        if (active[i]) b->eng.slots[i].frames += 1;
+    return KF_OK;
+}
+
+kf_status kf_batch_input_buffer(kf_batch* b, int i, uint16_t** dev_ptr) {
+    if (!b || !dev_ptr || i < 0 || i >= b->n) return KF_ERR_ARG;
+    *dev_ptr = const_cast<uint16_t*>(b->eng.slots[i].d.raw);
+    return KF_OK;
+}
+
+}  // extern "C"
+
+// ------------------------------------------------------------------------------------------
+// batch views and autotuning
+// ------------------------------------------------------------------------------------------
+namespace {
+
+// time one stage of a step (ms, device events) with the given grid
+kf_status time_stage(Engine& e, int stage, int grid, cudaStream_t st, int reps, float* ms) {
+    const int saved[4] = {e.grid_pre, e.grid_ray, e.grid_icp, e.grid_fuse};
+    int* target = stage == 0 ? &e.grid_pre : stage == 1 ? &e.grid_ray : stage == 2 ? &e.grid_icp : &e.grid_fuse;
+    *target = grid;
+    bool keep[4];
+    for (int q = 0; q < 4; ++q) { keep[q] = e.stages[q]; e.stages[q] = (q == stage); }
+    const bool ug = e.use_graph;
+    e.use_graph = false;
+    cudaEvent_t a, b;
+    cudaEventCreate(&a);
+    cudaEventCreate(&b);
+    kf_status r = e.record(st);   // warm-up
+    cudaEventRecord(a, st);
+    for (int i = 0; i < reps && r == KF_OK; ++i) r = e.record(st);
+    cudaEventRecord(b, st);
+    cudaEventSynchronize(b);
+    float t = 0.f;
+    cudaEventElapsedTime(&t, a, b);
+    *ms = t / float(reps);
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    for (int q = 0; q < 4; ++q) e.stages[q] = keep[q];
+    e.use_graph = ug;
+    e.grid_pre = saved[0]; e.grid_ray = saved[1]; e.grid_icp = saved[2]; e.grid_fuse = saved[3];
+    return r;
+}
+
+}  // namespace
+
+extern "C" {
+
+kf_status kf_batch_session(kf_batch* b, int i, kf_session** out) {
+    if (!b || !out || i < 0 || i >= b->n) return KF_ERR_ARG;
+    if (b->views.empty()) {
+        b->views.resize(b->n, nullptr);
+    }
+    if (!b->views[i]) {
+        kf_session* v = new (std::nothrow) kf_session;
+        if (!v) return KF_ERR_ARG;
+        v->eng = &b->eng;
+        v->slot = i;
+        v->owns = false;
+        b->views[i] = v;
+    }
+    *out = b->views[i];
+    return KF_OK;
+}
+
+// Pick the persistent grid of each stage by timing candidates on this batch's own frames.
+// Volumes and poses are saved first and restored afterwards, so tuning leaves the sessions
+// exactly as they were.  Every session must have processed at least one frame.
+kf_status kf_batch_autotune(kf_batch* b, void* stream, char* report, size_t report_bytes) {
+    if (!b) return KF_ERR_ARG;
+    Engine& e = b->eng;
+    cudaStream_t st = as_stream(stream);
+    for (int i = 0; i < b->n; ++i)
+        if (e.slots[i].frames == 0) return KF_ERR_STATE;
+    KF_CK(cudaStreamSynchronize(st));
+    if (e.tables_dirty) KF_TRY(e.build_tables());
+    // all sessions take part, none on its first frame
+    std::vector<StepDev> want(b->n, StepDev{1, 0});
+    for (int s = 0; s < b->n; ++s) e.h_step[s] = want[s];
+    KF_CK(cudaMemcpy(e.d_step, e.h_step, sizeof(StepDev) * b->n, cudaMemcpyHostToDevice));
+    e.step_dirty = false;
+    // snapshot volumes and pose state
+    std::vector<void*> saved;
+    std::vector<size_t> sizes;
+    for (int i = 0; i < b->n; ++i) {
+        const Slot& sl = e.slots[i];
+        const size_t n3 = size_t(sl.cfg.volume_n) * sl.cfg.volume_n * sl.cfg.volume_n;
+        const size_t es = sl.d.fmt == KF_TSDF_F16U16 ? 2 : 4;
+        void* p = nullptr;
+        KF_CK(cudaMalloc(&p, 2 * n3 * es + sizeof(PoseDev)));
+        KF_CK(cudaMemcpy(p, sl.d.tf, n3 * es, cudaMemcpyDeviceToDevice));
+        KF_CK(cudaMemcpy(static_cast<char*>(p) + n3 * es, sl.d.tw, n3 * es, cudaMemcpyDeviceToDevice));
+        KF_CK(cudaMemcpy(static_cast<char*>(p) + 2 * n3 * es, sl.d.pose, sizeof(PoseDev), cudaMemcpyDeviceToDevice));
+        saved.push_back(p);
+        sizes.push_back(n3 * es);
+    }
+    std::string rep = "{";
+    const int sms = e.sms;
+    const int cand_pre[] = {1, 2, 4, 8};
+    const int cand_ray[] = {2, 4, 6, 8, 12, 16};
+    const int cand_fuse[] = {4, 8, 12, 16, 24};
+    const char* names[4] = {"preprocess", "raycast", "icp", "fuse"};
+    kf_status r = KF_OK;
+    for (int stage = 0; stage < 4 && r == KF_OK; ++stage) {
+        if (stage == 2) continue;   // the cooperative ICP grid is one block per SM
+        const int* cand = stage == 0 ? cand_pre : stage == 1 ? cand_ray : cand_fuse;
+        const int nc = stage == 0 ? 4 : stage == 1 ? 6 : 5;
+        float best = 1e30f;
+        int best_g = 0;
+        char buf[160];
+        for (int c = 0; c < nc && r == KF_OK; ++c) {
+            float ms = 0.f;
+            r = time_stage(e, stage, sms * cand[c], st, 5, &ms);
+            if (ms < best) { best = ms; best_g = sms * cand[c]; }
+        }
+        if (r != KF_OK) break;
+        if (stage == 0) e.grid_pre = best_g;
+        if (stage == 1) e.grid_ray = best_g;
+        if (stage == 3) e.grid_fuse = best_g;
+        snprintf(buf, sizeof(buf), "%s\"%s\": {\"grid\": %d, \"ms\": %.5f}", rep.size() > 1 ? ", " : "", names[stage],
+                 best_g, best);
+        rep += buf;
+    }
+    rep += "}";
+    // restore
+    for (int i = 0; i < b->n; ++i) {
+        const Slot& sl = e.slots[i];
+        cudaMemcpy(sl.d.tf, saved[i], sizes[i], cudaMemcpyDeviceToDevice);
+        cudaMemcpy(sl.d.tw, static_cast<char*>(saved[i]) + sizes[i], sizes[i], cudaMemcpyDeviceToDevice);
+        cudaMemcpy(sl.d.pose, static_cast<char*>(saved[i]) + 2 * sizes[i], sizeof(PoseDev), cudaMemcpyDeviceToDevice);
+        cudaFree(saved[i]);
+    }
+    KF_CK(cudaDeviceSynchronize());
+    e.graph_dirty = true;
+    if (report && report_bytes) {
+        std::strncpy(report, rep.c_str(), report_bytes - 1);
+        report[report_bytes - 1] = 0;
+    }
+    return r;
+}
+
+}  // extern "C"
+
+// ------------------------------------------------------------------------------------------
+// server: continuous batching with HBM-budget admission
+// ------------------------------------------------------------------------------------------
+namespace {
+
+struct ServerSlot {
+    int id = -1;                  // session id, -1 = free
+    uint16_t* stage[2] = {nullptr, nullptr};   // pinned staging buffers
+    size_t stage_bytes = 0;
+    int pending = -1;             // staged buffer waiting for a step
+    int inflight = -1;            // staged buffer a running step reads
+    double t_submit[2] = {0, 0};
+    bool has_result = false;
+};
+
+double now_ms() {
+    using namespace std::chrono;
+    return duration<double, std::milli>(steady_clock::now().time_since_epoch()).count();
+}
+
+}  // namespace
+
+struct kf_server {
+    Engine eng;
+    int max_slots = 0;
+    size_t budget = 0, in_use = 0;
+    std::vector<ServerSlot> hs;
+    std::vector<kf_session*> views;
+    std::mutex q_mu;     // queue state (submit / step bookkeeping)
+    std::mutex gpu_mu;   // engine: steps, open, close
+    cudaStream_t stream = nullptr;
+    int next_id = 1;
+    std::vector<double> lat;
+    long long frames_done = 0, admitted = 0, refused = 0, steps = 0;
+    int max_active = 0;
+
+    int find(int id) const {
+        for (int i = 0; i < max_slots; ++i)
+            if (hs[i].id == id) return i;
+        return -1;
+    }
+};
+
+extern "C" {
+
+double kf_now_ms(void) { return now_ms(); }
+
+kf_status kf_server_create(int max_slots, size_t hbm_budget, kf_server** out) {
+    if (max_slots <= 0 || !out) return KF_ERR_ARG;
+    kf_server* s = new (std::nothrow) kf_server;
+    if (!s) return KF_ERR_ARG;
+    s->max_slots = max_slots;
+    s->budget = hbm_budget;
+    s->hs.resize(max_slots);
+    s->views.resize(max_slots, nullptr);
+    kf_status st = s->eng.init(max_slots);
+    if (st == KF_OK && cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking) != cudaSuccess) st = KF_ERR_CUDA;
+    if (st != KF_OK) { s->eng.destroy(); delete s; return st; }
+    *out = s;
+    return KF_OK;
+}
+
+kf_status kf_server_destroy(kf_server* s) {
+    if (!s) return KF_ERR_ARG;
+    std::lock_guard<std::mutex> g(s->gpu_mu);
+    cudaDeviceSynchronize();
+    for (ServerSlot& h : s->hs)
+        for (int b = 0; b < 2; ++b)
+            if (h.stage[b]) cudaFreeHost(h.stage[b]);
+    for (kf_session* v : s->views) delete v;
+    s->eng.destroy();
+    if (s->stream) cudaStreamDestroy(s->stream);
+    delete s;
+    return KF_OK;
+}
+
+kf_status kf_server_open(kf_server* s, const kf_config* cfg, int* id) {
+    if (!s || !cfg || !id) return KF_ERR_ARG;
+    KF_TRY(validate(*cfg));
+    std::lock_guard<std::mutex> g(s->gpu_mu);
+    const size_t need = footprint(*cfg) + size_t(cfg->width) * cfg->height * 2 * 2;
+    if (s->in_use + need > s->budget) {
+        s->refused++;
+        return KF_ERR_OOM_BUDGET;
+    }
+    int slot = -1;
+    for (int i = 0; i < s->max_slots; ++i)
+        if (s->hs[i].id < 0) { slot = i; break; }
+    if (slot < 0) {
+        s->refused++;
+        return KF_ERR_CAPACITY;
+    }
+    KF_CK(cudaStreamSynchronize(s->stream));
+    KF_TRY(slot_create(s->eng.slots[slot], *cfg));
+    ServerSlot& h = s->hs[slot];
+    h.stage_bytes = size_t(cfg->width) * cfg->height * 2;
+    for (int b = 0; b < 2; ++b) {
+        if (cudaMallocHost(&h.stage[b], h.stage_bytes) != cudaSuccess) {
+            s->eng.slots[slot].release();
+            return KF_ERR_CUDA;
+        }
+    }
+    h.pending = h.inflight = -1;
+    h.has_result = false;
+    {
+        std::lock_guard<std::mutex> q(s->q_mu);
+        h.id = s->next_id++;
+    }
+    s->in_use += s->eng.slots[slot].bytes + 2 * h.stage_bytes;
+    s->eng.tables_dirty = true;
+    s->admitted++;
+    *id = h.id;
+    return KF_OK;
+}
+
+kf_status kf_server_close(kf_server* s, int id) {
+    if (!s) return KF_ERR_ARG;
+    std::lock_guard<std::mutex> g(s->gpu_mu);
+    int slot;
+    {
+        std::lock_guard<std::mutex> q(s->q_mu);
+        slot = s->find(id);
+        if (slot < 0) return KF_ERR_ARG;
+        s->hs[slot].id = -1;
+        s->hs[slot].pending = -1;
+    }
+    KF_CK(cudaStreamSynchronize(s->stream));
+    ServerSlot& h = s->hs[slot];
+    s->in_use -= s->eng.slots[slot].bytes + 2 * h.stage_bytes;
+    s->eng.slots[slot].release();
+    for (int b = 0; b < 2; ++b) {
+        if (h.stage[b]) cudaFreeHost(h.stage[b]);
+        h.stage[b] = nullptr;
+    }
+    s->eng.tables_dirty = true;
+    return KF_OK;
+}
+
+kf_status kf_server_submit(kf_server* s, int id, const uint16_t* depth, double t_submit_ms) {
+    if (!s || !depth) return KF_ERR_ARG;
+    std::lock_guard<std::mutex> q(s->q_mu);
+    const int slot = s->find(id);
+    if (slot < 0) return KF_ERR_ARG;
+    ServerSlot& h = s->hs[slot];
+    if (h.pending >= 0) return KF_ERR_STATE;
+    const int b = h.inflight == 0 ? 1 : 0;
+    std::memcpy(h.stage[b], depth, h.stage_bytes);
+    h.t_submit[b] = t_submit_ms;
+    h.pending = b;
+    return KF_OK;
+}
+
+kf_status kf_server_step(kf_server* s, int* served) {
+    if (!s) return KF_ERR_ARG;
+    std::lock_guard<std::mutex> g(s->gpu_mu);
+    const int cap = s->max_slots;
+    std::vector<StepDev> want(cap, StepDev{0, 0});
+    int n = 0;
+    {
+        std::lock_guard<std::mutex> q(s->q_mu);
+        for (int i = 0; i < cap; ++i) {
+            ServerSlot& h = s->hs[i];
+            if (h.id < 0 || h.pending < 0) continue;
+            h.inflight = h.pending;
+            h.pending = -1;
+            want[i] = StepDev{1, s->eng.slots[i].frames == 0 ? 1 : 0};
+            ++n;
+        }
+    }
+    if (served) *served = n;
+    if (n == 0) return KF_OK;
+    cudaStream_t st = s->stream;
+    KF_TRY(s->eng.set_step(want, st));
+    for (int i = 0; i < cap; ++i) {
+        if (!want[i].active) continue;
+        const ServerSlot& h = s->hs[i];
+        KF_CK(cudaMemcpyAsync(const_cast<uint16_t*>(s->eng.slots[i].d.raw), h.stage[h.inflight], h.stage_bytes,
+                              cudaMemcpyHostToDevice, st));
+    }
+    KF_TRY(s->eng.enqueue(st));
+    KF_CK(cudaStreamSynchronize(st));
+    kf_status r = s->eng.collect(want);
+    const double t = now_ms();
+    {
+        std::lock_guard<std::mutex> q(s->q_mu);
+        for (int i = 0; i < cap; ++i) {
+            if (!want[i].active) continue;
+            ServerSlot& h = s->hs[i];
+            s->lat.push_back(t - h.t_submit[h.inflight]);
+            h.inflight = -1;
+            h.has_result = true;
+        }
+        s->frames_done += n;
+        s->steps++;
+        s->max_active = std::max(s->max_active, n);
+    }
+    return r;
+}
+
+kf_status kf_server_result(kf_server* s, int id, float pose[16], kf_frame_stats* stats) {
+    if (!s) return KF_ERR_ARG;
+    std::lock_guard<std::mutex> g(s->gpu_mu);
+    const int slot = s->find(id);
+    if (slot < 0) return KF_ERR_ARG;
+    if (!s->hs[slot].has_result) return KF_ERR_STATE;
+    if (pose) std::memcpy(pose, s->eng.slots[slot].pose, sizeof(float) * 16);
+    if (stats) *stats = s->eng.slots[slot].stats;
+    return KF_OK;
+}
+
+kf_status kf_server_get_session(kf_server* s, int id, kf_session** out) {
+    if (!s || !out) return KF_ERR_ARG;
+    std::lock_guard<std::mutex> g(s->gpu_mu);
+    const int slot = s->find(id);
+    if (slot < 0) return KF_ERR_ARG;
+    if (!s->views[slot]) {
+        kf_session* v = new (std::nothrow) kf_session;
+        if (!v) return KF_ERR_ARG;
+        v->eng = &s->eng;
+        v->slot = slot;
+        v->owns = false;
+        s->views[slot] = v;
+    }
+    *out = s->views[slot];
+    return KF_OK;
+}
+
+kf_status kf_server_stats_get(kf_server* s, kf_server_stats* out) {
+    if (!s || !out) return KF_ERR_ARG;
+    std::lock_guard<std::mutex> q(s->q_mu);
+    std::memset(out, 0, sizeof(*out));
+    out->frames_done = s->frames_done;
+    out->sessions_admitted = s->admitted;
+    out->sessions_refused = s->refused;
+    out->steps = s->steps;
+    int active = 0;
+    for (const ServerSlot& h : s->hs)
+        if (h.id >= 0) ++active;
+    out->active_sessions = active;
+    out->max_active_sessions = s->max_active;
+    out->hbm_in_use = s->in_use;
+    out->hbm_budget = s->budget;
+    if (!s->lat.empty()) {
+        std::vector<double> v = s->lat;
+        std::sort(v.begin(), v.end());
+        auto pct = [&v](double p) {
+            const size_t i = std::min(v.size() - 1, size_t(p * double(v.size() - 1) + 0.5));
+            return v[i];
+        };
+        out->p50_ms = pct(0.50);
+        out->p99_ms = pct(0.99);
+        out->max_ms = v.back();
+    }
+    return KF_OK;
+}
+
+}  // extern "C"
+
+// ------------------------------------------------------------------------------------------
+// instrumentation
+// ------------------------------------------------------------------------------------------
+extern "C" {
+
+kf_status kf_session_set_profiling(kf_session* s, int on) {
+    if (!s) return KF_ERR_ARG;
+    return s->eng->set_profile(on != 0);
+}
+
+kf_status kf_session_stage_times(kf_session* s, float ms[4]) {
+    if (!s || !ms) return KF_ERR_ARG;
+    return s->eng->stage_times(ms);
+}
+
+kf_status kf_batch_set_profiling(kf_batch* b, int on) {
+    if (!b) return KF_ERR_ARG;
+    return b->eng.set_profile(on != 0);
+}
+
+kf_status kf_batch_stage_times(kf_batch* b, float ms[4]) {
+    if (!b || !ms) return KF_ERR_ARG;
+    return b->eng.stage_times(ms);
+}
+
+kf_status kf_selftest_bounded_wait(int timeout_ms, int* waited_ms) {
+    if (timeout_ms <= 0 || timeout_ms > 5000) return KF_ERR_ARG;
+    GridSync* g = nullptr;
+    int* res = nullptr;
+    KF_CK(cudaMalloc(&g, sizeof(GridSync)));
+    cudaError_t e = cudaMalloc(&res, sizeof(int));
+    if (e == cudaSuccess) e = cudaMemset(g, 0, sizeof(GridSync));
+    if (e == cudaSuccess) e = cudaMemset(res, 0xff, sizeof(int));
+    const double t0 = now_ms();
+    if (e == cudaSuccess) e = launch_barrier_selftest(g, (unsigned long long)timeout_ms * 1000000ull, res, 0);
+    if (e == cudaSuccess) e = cudaDeviceSynchronize();
+    const double t1 = now_ms();
+    int h_res = -1;
+    GridSync h_g{};
+    if (e == cudaSuccess) e = cudaMemcpy(&h_res, res, sizeof(int), cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess) e = cudaMemcpy(&h_g, g, sizeof(GridSync), cudaMemcpyDeviceToHost);
+    cudaFree(g);
+    cudaFree(res);
+    KF_CK(e);
+    if (waited_ms) *waited_ms = int(t1 - t0 + 0.5);
+    if (h_res == 0 && h_g.abort && h_g.timeouts == 1) return KF_ERR_TIMEOUT;
+    return h_res == 1 ? KF_OK : KF_ERR_STATE;
+}
+
+}  // extern "C"

@@ -1,0 +1,537 @@
+// k_icp.cu -- projective point-to-plane ICP on the device.
+//
+// Reference: constructIcpResidualsKernel (project/src/icp.cu:7-82) writes an N x 6 matrix A
+// and a vector b to HBM, cuBLAS forms A^T A and A^T b, two copies bring them to the host,
+// Eigen solves a float LLT and the host updates the pose, per iteration
+// (project/src/icp.cpp:25-87, project/src/linear_least_squares.cpp:23-44).
+//
+// Here one cooperative launch runs the whole coarse-to-fine loop for every session of a
+// batch.  Each pass:
+//   A. every block takes pixel tiles of sessions still iterating, associates and rejects
+//      pixels as the reference does, and accumulates the 27 distinct entries of A^T A / A^T b
+//      (21 + 6) in FP32; a warp-shuffle reduce-scatter with two-sum compensation and a
+//      compensated combine across warps give one (sum, compensation) pair per entry per tile;
+//   B. one block per session adds its tiles' pairs in FP64, solves the 6x6 system by FP64
+//      Cholesky, updates the FP64 pose and applies the reference's early-stop test;
+// separated by bounded grid barriers.  Nothing returns to the host until the frame is done.
+#include "kf_host.h"
+
+namespace kf {
+
+// ---- loads of data other blocks of the same launch wrote (bypass L1) ----
+__device__ __forceinline__ float ldcg(const float* p) { return __ldcg(p); }
+__device__ __forceinline__ double ldcg(const double* p) { return __ldcg(p); }
+__device__ __forceinline__ int ldcg(const int* p) { return __ldcg(p); }
+
+// ---- per-pixel residual: constructIcpResidualsKernel body with computeCorrespondence,
+// areVerticesTooFarAway, areNormalsTooDifferent and computeAndFillA/B
+// (project/src/icp.cu:20-81, project/src/icp.cuh:40-95) ----
+__device__ __forceinline__ bool icp_pixel(const float4* __restrict__ vm, const float4* __restrict__ tv,
+                                          const float4* __restrict__ tn, int w, int h, int u, int v, const float* R,
+                                          const float* t, const float* M, const float* tp, float dist_th,
+                                          float ang_th, float a[6], float& b) {
+    const float4 vc = __ldg(vm + size_t(v) * w + u);
+    if (vc.w != kValid) return false;
+    const F3 s = mv3(R, f3(vc)) + F3{t[0], t[1], t[2]};
+    // (K * R_prev^T) * (s - t_prev), then floor(x / z), floor(y / z)
+    const F3 pt = mv3(M, s - F3{tp[0], tp[1], tp[2]});
+    const int uc = int(floorf(pt.x / pt.z));   // cvt.rzi: NaN -> 0, as in the reference
+    const int vcor = int(floorf(pt.y / pt.z));
+    if (uc < 0 || vcor < 0 || uc >= w || vcor >= h) return false;
+    const float4 d4 = __ldg(tv + size_t(vcor) * w + uc);
+    const float4 n4 = __ldg(tn + size_t(vcor) * w + uc);
+    if (d4.w != kValid || n4.w != kValid) return false;
+    const F3 d = f3(d4);
+    const F3 e = s - d;
+    if (sqrtf(dot3(e, e)) > dist_th) return false;
+    const float4 ns = compute_normal(vm, w, h, u, v);
+    if (ns.w == kInvalid) return false;
+    F3 nr = mv3(R, f3(ns));
+    nr = nr * rsqrtf(dot3(nr, nr));
+    const F3 n = f3(n4);
+    if (acosf(dot3(nr, n)) > ang_th) return false;   // NaN passes, as in the reference
+    a[0] = n.y * s.z - n.z * s.y;
+    a[1] = n.z * s.x - n.x * s.z;
+    a[2] = n.x * s.y - n.y * s.x;
+    a[3] = n.x;
+    a[4] = n.y;
+    a[5] = n.z;
+    b = n.x * d.x + n.y * d.y + n.z * d.z - n.x * s.x - n.y * s.y - n.z * s.z;
+    return true;
+}
+
+// the 27 distinct products: upper triangle of A^T A row by row, then A^T b
+__device__ __forceinline__ void accumulate_products(float acc[32], const float a[6], float b) {
+    int k = 0;
+#pragma unroll
+    for (int r = 0; r < 6; ++r)
+#pragma unroll
+        for (int c = r; c < 6; ++c) acc[k++] += a[r] * a[c];
+#pragma unroll
+    for (int r = 0; r < 6; ++r) acc[21 + r] += a[r] * b;
+}
+
+__device__ __forceinline__ void two_sum(float a, float b, float& s, float& e) {
+    s = a + b;
+    const float bb = s - a;
+    e = (a - (s - bb)) + (b - bb);
+}
+
+// Reduce 32 slots across the warp.  Each step halves the slots a lane keeps and exchanges the
+// other half with its partner, adding with two-sum; lane l ends with the warp total of slot l
+// as (sum, compensation).
+__device__ __forceinline__ void warp_reduce_scatter(float (&v)[32], float (&c)[32], int lane) {
+#pragma unroll
+    for (int off = 16; off >= 1; off >>= 1) {
+        const bool up = (lane & off) != 0;
+#pragma unroll
+        for (int i = 0; i < off; ++i) {
+            const float sv = up ? v[i] : v[i + off];
+            const float sc = up ? c[i] : c[i + off];
+            const float kv = up ? v[i + off] : v[i];
+            const float kc = up ? c[i + off] : c[i];
+            const float rv = __shfl_xor_sync(0xffffffffu, sv, off);
+            const float rc = __shfl_xor_sync(0xffffffffu, sc, off);
+            float s, e;
+            two_sum(kv, rv, s, e);
+            v[i] = s;
+            c[i] = kc + rc + e;
+        }
+    }
+}
+
+// Block reduction of each thread's 27 partial sums to 27 compensated pairs stored at out
+// (54 floats).  red: shared scratch of 8 * 32 * 2 floats.  Must be called by all threads.
+__device__ __forceinline__ void block_reduce_store(float (&acc)[32], float* red, float* out) {
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    float c[32];
+#pragma unroll
+    for (int i = 0; i < 32; ++i) c[i] = 0.f;
+    warp_reduce_scatter(acc, c, lane);
+    red[(warp * 32 + lane) * 2 + 0] = acc[0];
+    red[(warp * 32 + lane) * 2 + 1] = c[0];
+    __syncthreads();
+    if (tid < 27) {
+        float s = red[tid * 2 + 0], cc = red[tid * 2 + 1];
+        const int nw = blockDim.x >> 5;
+        for (int w = 1; w < nw; ++w) {
+            float t, e;
+            two_sum(s, red[(w * 32 + tid) * 2 + 0], t, e);
+            cc += red[(w * 32 + tid) * 2 + 1] + e;
+            s = t;
+        }
+        __stcg(out + 2 * tid + 0, s);
+        __stcg(out + 2 * tid + 1, cc);
+    }
+    __syncthreads();
+}
+
+// ---- FP64 solve and pose algebra (thread-level) ----
+
+// Cholesky (LLT) solve of the 6x6 normal equations (the reference: Eigen LLT<float>,
+// project/src/linear_least_squares.cpp:41).  Returns false for a non-positive pivot.
+__device__ bool cholesky6(const double* ata, const double* atb, double* x) {
+    double L[6][6];
+    for (int j = 0; j < 6; ++j) {
+        double d = ata[j * 6 + j];
+        for (int k = 0; k < j; ++k) d -= L[j][k] * L[j][k];
+        if (!(d > 0.0)) return false;
+        const double ljj = sqrt(d);
+        L[j][j] = ljj;
+        for (int i = j + 1; i < 6; ++i) {
+            double s = ata[i * 6 + j];
+            for (int k = 0; k < j; ++k) s -= L[i][k] * L[j][k];
+            L[i][j] = s / ljj;
+        }
+    }
+    double y[6];
+    for (int i = 0; i < 6; ++i) {
+        double s = atb[i];
+        for (int k = 0; k < i; ++k) s -= L[i][k] * y[k];
+        y[i] = s / L[i][i];
+    }
+    for (int i = 5; i >= 0; --i) {
+        double s = y[i];
+        for (int k = i + 1; k < 6; ++k) s -= L[k][i] * x[k];
+        x[i] = s / L[i][i];
+    }
+    for (int i = 0; i < 6; ++i)
+        if (!isfinite(x[i])) return false;
+    return true;
+}
+
+// glm::orientate3(vec3(beta, alpha, gamma)) of project/src/icp.cpp:82: the Euler composition
+// Y * X * Z, i.e. R_y(gamma) R_x(beta) R_z(alpha); column-major out
+__device__ void euler_yxz(double beta, double gamma, double alpha, double* m) {
+    double sx, cx, sy, cy, sz, cz;
+    sincos(beta, &sx, &cx);
+    sincos(gamma, &sy, &cy);
+    sincos(alpha, &sz, &cz);
+    m[0] = cy * cz + sy * sx * sz;  m[1] = cx * sz;  m[2] = -sy * cz + cy * sx * sz;
+    m[3] = -cy * sz + sy * sx * cz; m[4] = cx * cz;  m[5] = sy * sz + cy * sx * cz;
+    m[6] = sy * cx;                 m[7] = -sx;      m[8] = cy * cx;
+}
+
+__device__ __forceinline__ void m3d_vec(const double* m, const double* v, double* o) {
+    for (int r = 0; r < 3; ++r) o[r] = m[r] * v[0] + m[3 + r] * v[1] + m[6 + r] * v[2];
+}
+
+// the float data phase A of the next pass reads: estimate and K_l * R_prev^T
+__device__ void publish_pass(PoseDev* P, const LevelDev& Lv) {
+    for (int q = 0; q < 9; ++q) P->Rf[q] = float(P->R[q]);
+    for (int q = 0; q < 3; ++q) P->tf[q] = float(P->t[q]);
+    // K = [fx 0 cx; 0 fy cy; 0 0 1];  M = K * Rp^T;  (Rp^T)(r, c) = Rp(c, r) = Rp[r * 3 + c]
+    for (int col = 0; col < 3; ++col) {
+        // column col of Rp^T = row col of Rp = (Rp[col], Rp[3 + col], Rp[6 + col])
+        const double a0 = P->Rp[col], a1 = P->Rp[3 + col], a2 = P->Rp[6 + col];
+        P->M[col * 3 + 0] = float(double(Lv.fx) * a0 + double(Lv.cx) * a2);
+        P->M[col * 3 + 1] = float(double(Lv.fy) * a1 + double(Lv.cy) * a2);
+        P->M[col * 3 + 2] = float(a2);
+    }
+    __threadfence();
+}
+
+// first ICP level with iterations at or below `from`
+__device__ __forceinline__ int next_level(const SessionDev* S, int from) {
+    int l = from;
+    while (l >= 0 && S->iters[l] <= 0) --l;
+    return l;
+}
+
+// phase 0 for one session (one thread)
+__device__ void icp_begin(const SessionDev* S, const StepDev st) {
+    if (!st.active) return;   // empty or idle slot: its state is not touched
+    PoseDev* P = S->pose;
+    P->status = KF_OK;
+    for (int l = 0; l < kMaxLevels; ++l) P->iters[l] = 0;
+    P->it = 0;
+    if (st.first) { P->level = -1; P->cont = 0; __threadfence(); return; }
+    for (int q = 0; q < 9; ++q) P->R[q] = P->Rp[q];
+    for (int q = 0; q < 3; ++q) P->t[q] = P->tp[q];
+    P->level = next_level(S, S->L - 1);
+    if (P->level >= 0) publish_pass(P, S->lv[P->level]);
+    P->cont = P->level >= 0 ? 1 : 0;
+    __threadfence();
+}
+
+// phase B for one session: FP64 combine of the tile pairs, solve, update, stop test
+// (ICP::computePose loop body, project/src/icp.cpp:36-54).  All threads of the block call it.
+__device__ void icp_solve(const EngineView& v, int s, double* sm) {
+    const SessionDev* S = &v.sess[s];
+    PoseDev* P = S->pose;
+    const int tid = threadIdx.x;
+    const int level = ldcg(&P->level);
+    const IcpRange rg = v.iranges[level * v.tb->S + s];
+    // 8 groups x 27 entries: each group adds every 8th tile in FP64
+    if (tid < 8 * 27) {
+        const int k = tid % 27, g = tid / 27;
+        double acc = 0.0;
+        for (int t = rg.begin + g; t < rg.end; t += 8) {
+            const float* p = v.partials + size_t(t) * 54;
+            acc += double(ldcg(p + 2 * k)) + double(ldcg(p + 2 * k + 1));
+        }
+        sm[g * 27 + k] = acc;
+    }
+    __syncthreads();
+    if (tid == 0) {
+        double tot[27];
+        for (int k = 0; k < 27; ++k) {
+            double a = 0.0;
+            for (int g = 0; g < 8; ++g) a += sm[g * 27 + k];
+            tot[k] = a;
+        }
+        double ata[36], atb[6];
+        int k = 0;
+        for (int r = 0; r < 6; ++r)
+            for (int c = r; c < 6; ++c) { ata[r * 6 + c] = tot[k]; ata[c * 6 + r] = tot[k]; ++k; }
+        for (int r = 0; r < 6; ++r) atb[r] = tot[21 + r];
+        double x[6];
+        if (!cholesky6(ata, atb, x)) {
+            // the reference throws (project/src/icp.cpp:67-73): keep the previous pose, no fusion
+            P->status = KF_ERR_NONFINITE;
+            P->level = -1;
+            P->cont = 0;
+            __threadfence();
+        } else {
+            double dR[9], R0[9], t0[3];
+            for (int q = 0; q < 9; ++q) R0[q] = P->R[q];
+            for (int q = 0; q < 3; ++q) t0[q] = P->t[q];
+            euler_yxz(x[0], x[1], x[2], dR);
+            // R <- dR^T R, t <- dR^T t + dt (ICP::updatePose, project/src/icp.cpp:85-86)
+            double dRt[9];
+            for (int c = 0; c < 3; ++c)
+                for (int r = 0; r < 3; ++r) dRt[c * 3 + r] = dR[r * 3 + c];
+            for (int c = 0; c < 3; ++c) m3d_vec(dRt, R0 + 3 * c, P->R + 3 * c);
+            double nt[3];
+            m3d_vec(dRt, t0, nt);
+            for (int q = 0; q < 3; ++q) P->t[q] = nt[q] + x[3 + q];
+            P->iters[level] += 1;
+            // poseError(previous estimate, new estimate) (project/src/general_helper.cpp:11-21)
+            const double iv = 0.57735026918962576451;
+            double a0[3], a1[3], vv[3] = {iv, iv, iv};
+            m3d_vec(R0, vv, a0);
+            m3d_vec(P->R, vv, a1);
+            const double ang = sqrt((a0[0] - a1[0]) * (a0[0] - a1[0]) + (a0[1] - a1[1]) * (a0[1] - a1[1]) +
+                                    (a0[2] - a1[2]) * (a0[2] - a1[2]));
+            const double dist = sqrt((t0[0] - P->t[0]) * (t0[0] - P->t[0]) + (t0[1] - P->t[1]) * (t0[1] - P->t[1]) +
+                                     (t0[2] - P->t[2]) * (t0[2] - P->t[2]));
+            int it = P->it + 1;
+            int lvl = level;
+            if ((ang < double(S->stop_a) && dist < double(S->stop_d)) || it >= S->iters[level]) {
+                lvl = next_level(S, level - 1);
+                it = 0;
+            }
+            P->it = it;
+            P->level = lvl;
+            if (lvl >= 0) publish_pass(P, S->lv[lvl]);
+            P->cont = lvl >= 0 ? 1 : 0;
+            __threadfence();
+        }
+    }
+    __syncthreads();
+}
+
+// phase C for one session (one thread): the frame's pose becomes the previous pose; the
+// inverse feeds fusion; the result block goes to the host.
+__device__ void icp_finish(const SessionDev* S, const StepDev st, OutDev* out) {
+    if (!st.active) return;
+    PoseDev* P = S->pose;
+    const bool ok = P->status == KF_OK;
+    if (ok && !st.first) {
+        for (int q = 0; q < 9; ++q) P->Rp[q] = P->R[q];
+        for (int q = 0; q < 3; ++q) P->tp[q] = P->t[q];
+    }
+    for (int q = 0; q < 9; ++q) P->Rpf[q] = float(P->Rp[q]);
+    for (int q = 0; q < 3; ++q) P->tpf[q] = float(P->tp[q]);
+    // inverse: R^T, -R^T t
+    for (int c = 0; c < 3; ++c)
+        for (int r = 0; r < 3; ++r) P->iRf[c * 3 + r] = float(P->Rp[r * 3 + c]);
+    for (int r = 0; r < 3; ++r)
+        P->itf[r] = float(-(P->Rp[r * 3 + 0] * P->tp[0] + P->Rp[r * 3 + 1] * P->tp[1] + P->Rp[r * 3 + 2] * P->tp[2]));
+    P->fuse_ok = ok ? 1 : 0;
+    P->frame += 1;
+    for (int q = 0; q < 16; ++q) out->pose[q] = 0.f;
+    for (int c = 0; c < 3; ++c)
+        for (int r = 0; r < 3; ++r) out->pose[c * 4 + r] = P->Rpf[c * 3 + r];
+    for (int r = 0; r < 3; ++r) out->pose[12 + r] = P->tpf[r];
+    out->pose[15] = 1.f;
+    for (int l = 0; l < kMaxLevels; ++l) out->iters[l] = P->iters[l];
+    out->status = P->status;
+    out->frame = P->frame;
+    __threadfence();
+}
+
+// ---- the persistent cooperative kernel ----
+
+constexpr int kIcpMaxSessionsSmem = 1024;
+
+__global__ void __launch_bounds__(kIcpThreads) icp_kernel(EngineView v) {
+    __shared__ float red[8 * 32 * 2];
+    __shared__ double dsm[8 * 27];
+    __shared__ float mats[24];
+    __shared__ int s_pre[kIcpMaxSessionsSmem + 1];
+    __shared__ int s_lvl[kIcpMaxSessionsSmem];
+    __shared__ int s_any;
+    const int tid = threadIdx.x;
+    const unsigned int nb = gridDim.x;
+    unsigned int epoch = 0;
+    const int S_cap = v.tb->S;
+
+    for (int s = blockIdx.x; s < S_cap; s += gridDim.x)
+        if (tid == 0) icp_begin(&v.sess[s], v.step[s]);
+    if (!grid_barrier(v.sync, nb, epoch)) return;
+
+    for (int pass = 0; pass < kIcpMaxPasses; ++pass) {
+        // which sessions iterate in this pass, at which level; virtual tile prefix
+        if (tid == 0) s_any = 0;
+        __syncthreads();
+        for (int s = tid; s < S_cap; s += blockDim.x) {
+            int cnt = 0, lvl = -1;
+            const StepDev st = v.step[s];
+            if (st.active && !st.first && ldcg(&v.sess[s].pose->cont)) {
+                lvl = ldcg(&v.sess[s].pose->level);
+                const IcpRange rg = v.iranges[lvl * S_cap + s];
+                cnt = rg.end - rg.begin;
+                s_any = 1;
+            }
+            s_lvl[s] = lvl;
+            s_pre[s + 1] = cnt;
+        }
+        __syncthreads();
+        if (!s_any) break;   // block-uniform: every block sees the same flags
+        if (tid == 0) {
+            s_pre[0] = 0;
+            for (int s = 0; s < S_cap; ++s) s_pre[s + 1] += s_pre[s];
+        }
+        __syncthreads();
+        const int total = s_pre[S_cap];
+
+        // phase A
+        for (int vt = blockIdx.x; vt < total; vt += gridDim.x) {
+            int lo = 0, hi = S_cap;
+            while (hi - lo > 1) {
+                const int mid = (lo + hi) >> 1;
+                if (s_pre[mid] <= vt) lo = mid; else hi = mid;
+            }
+            const int s = lo, lvl = s_lvl[s];
+            const int abs_t = v.iranges[lvl * S_cap + s].begin + (vt - s_pre[s]);
+            const IcpTile T = v.itiles[abs_t];
+            const SessionDev* S = &v.sess[s];
+            const PoseDev* P = S->pose;
+            if (tid < 9) mats[tid] = ldcg(&P->Rf[tid]);
+            else if (tid < 12) mats[tid] = ldcg(&P->tf[tid - 9]);
+            else if (tid < 21) mats[tid] = ldcg(&P->M[tid - 12]);
+            else if (tid < 24) mats[tid] = ldcg(&P->tpf[tid - 21]);
+            __syncthreads();
+            const LevelDev& Lv = S->lv[lvl];
+            const float4* vm = S->vmap[lvl];
+            const float4* tv = S->pv[lvl];
+            const float4* tn = S->pn[lvl];
+            uint8_t* mask = S->mask[lvl];
+            float acc[32];
+#pragma unroll
+            for (int q = 0; q < 32; ++q) acc[q] = 0.f;
+            const float dist = S->dist_th, ang = S->angle_th;
+#pragma unroll 1
+            for (int k = 0; k < kIcpPxPerThread; ++k) {
+                const int p = T.p0 + tid + k * kIcpThreads;
+                if (p >= T.p0 + T.np) break;
+                const int u = p % Lv.icw, vv = p / Lv.icw;
+                float a[6], b;
+                const bool ok = icp_pixel(vm, tv, tn, Lv.w, Lv.h, u, vv, mats, mats + 9, mats + 12, mats + 21, dist,
+                                          ang, a, b);
+                if (mask) mask[size_t(vv) * Lv.w + u] = ok ? 1 : 0;
+                if (ok) accumulate_products(acc, a, b);
+            }
+            block_reduce_store(acc, red, v.partials + size_t(abs_t) * 54);
+        }
+        if (!grid_barrier(v.sync, nb, epoch)) return;
+
+        // phase B
+        for (int s = blockIdx.x; s < S_cap; s += gridDim.x)
+            if (s_lvl[s] >= 0) icp_solve(v, s, dsm);
+        if (!grid_barrier(v.sync, nb, epoch)) return;
+    }
+
+    for (int s = blockIdx.x; s < S_cap; s += gridDim.x)
+        if (tid == 0) icp_finish(&v.sess[s], v.step[s], v.out + s);
+}
+
+int icp_max_grid(int num_sms) { return num_sms; }
+
+// Bounded-wait self test: a two-block cooperative launch in which block 1 never arrives at
+// the barrier block 0 waits on.  The wait gives up after timeout_ns, sets the abort flag and
+// records the outcome; nothing spins past the limit.
+__global__ void barrier_selftest_kernel(GridSync* g, unsigned long long timeout_ns, int* result) {
+    unsigned int epoch = 0;
+    if (blockIdx.x == 0) {
+        const bool ok = grid_barrier(g, gridDim.x, epoch, timeout_ns);
+        if (threadIdx.x == 0) *result = ok ? 1 : 0;
+    }
+}
+
+cudaError_t launch_barrier_selftest(GridSync* g, unsigned long long timeout_ns, int* result, cudaStream_t st) {
+    void* args[] = {&g, &timeout_ns, &result};
+    return cudaLaunchCooperativeKernel((const void*)barrier_selftest_kernel, dim3(2), dim3(32), args, 0, st);
+}
+
+cudaError_t launch_icp(const EngineView& v, int grid, cudaStream_t st) {
+    void* args[] = {const_cast<EngineView*>(&v)};
+    return cudaLaunchCooperativeKernel((const void*)icp_kernel, dim3(grid), dim3(kIcpThreads), args, 0, st);
+}
+
+// ---- stage: kernel::constructIcpResiduals (A rows and b to HBM, as the reference) ----
+
+struct IcpStageMats { float R[9], t[3], M[9], tp[3]; };
+
+__global__ void icp_rows_kernel(const float4* vm, const float4* tv, const float4* tn, int w, int h, IcpStageMats m,
+                                float dist, float angle, float* A, float* b) {
+    const int u = blockIdx.x * blockDim.x + threadIdx.x, vv = blockIdx.y * blockDim.y + threadIdx.y;
+    if (u >= w || vv >= h) return;
+    float a[6], bb;
+    const bool ok = icp_pixel(vm, tv, tn, w, h, u, vv, m.R, m.t, m.M, m.tp, dist, angle, a, bb);
+    const size_t idx = size_t(vv) * w + u;
+    for (int q = 0; q < 6; ++q) A[idx * 6 + q] = ok ? a[q] : 0.f;
+    b[idx] = ok ? bb : 0.f;
+}
+
+cudaError_t stage_icp_residuals(const float4* vmap, const float4* tv, const float4* tn, int w, int h,
+                                const float* Rp, const float* tp, const float* Rc, const float* tc, const float* k,
+                                float dist, float angle, float* A, float* b, cudaStream_t st) {
+    IcpStageMats m;
+    for (int q = 0; q < 9; ++q) m.R[q] = Rc[q];
+    for (int q = 0; q < 3; ++q) { m.t[q] = tc[q]; m.tp[q] = tp[q]; }
+    // M = K * Rp^T with K the caller's full 3x3 (column-major)
+    for (int col = 0; col < 3; ++col)
+        for (int row = 0; row < 3; ++row) {
+            float acc = 0.f;
+            for (int q = 0; q < 3; ++q) acc += k[q * 3 + row] * Rp[q * 3 + col];   // K(row,q) * Rp^T(q,col) = K(row,q) * Rp(col,q)
+            m.M[col * 3 + row] = acc;
+        }
+    dim3 blk(16, 16), grd((w + 15) / 16, (h + 15) / 16);
+    icp_rows_kernel<<<grd, blk, 0, st>>>(vmap, tv, tn, w, h, m, dist, angle, A, b);
+    return cudaGetLastError();
+}
+
+// ---- stage: LinearLeastSquares::solve on A (n x 6, row-major) and b in device memory ----
+
+int lls_num_blocks(int n) {
+    const int per = kIcpTilePx;
+    int nb = (n + per - 1) / per;
+    if (nb < 1) nb = 1;
+    if (nb > 148 * 4) nb = 148 * 4;
+    return nb;
+}
+
+__global__ void __launch_bounds__(kIcpThreads) lls_partials_kernel(const float* A, const float* b, int n,
+                                                                   float* partials) {
+    __shared__ float red[8 * 32 * 2];
+    float acc[32];
+#pragma unroll
+    for (int q = 0; q < 32; ++q) acc[q] = 0.f;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        float a[6];
+        for (int q = 0; q < 6; ++q) a[q] = A[size_t(i) * 6 + q];
+        accumulate_products(acc, a, b[i]);
+    }
+    block_reduce_store(acc, red, partials + size_t(blockIdx.x) * 54);
+}
+
+__global__ void lls_solve_kernel(const float* partials, int nblocks, double* x_out) {
+    __shared__ double sm[8 * 27];
+    const int tid = threadIdx.x;
+    if (tid < 8 * 27) {
+        const int k = tid % 27, g = tid / 27;
+        double acc = 0.0;
+        for (int t = g; t < nblocks; t += 8) acc += double(partials[size_t(t) * 54 + 2 * k]) + double(partials[size_t(t) * 54 + 2 * k + 1]);
+        sm[g * 27 + k] = acc;
+    }
+    __syncthreads();
+    if (tid == 0) {
+        double tot[27];
+        for (int k = 0; k < 27; ++k) {
+            double a = 0.0;
+            for (int g = 0; g < 8; ++g) a += sm[g * 27 + k];
+            tot[k] = a;
+        }
+        double ata[36], atb[6], x[6];
+        int k = 0;
+        for (int r = 0; r < 6; ++r)
+            for (int c = r; c < 6; ++c) { ata[r * 6 + c] = tot[k]; ata[c * 6 + r] = tot[k]; ++k; }
+        for (int r = 0; r < 6; ++r) atb[r] = tot[21 + r];
+        if (!cholesky6(ata, atb, x))
+            for (int q = 0; q < 6; ++q) x[q] = __longlong_as_double(0x7ff8000000000000ll);
+        for (int q = 0; q < 6; ++q) x_out[q] = x[q];
+    }
+}
+
+cudaError_t stage_lls(const float* A, const float* b, int n, float* partials, double* x_dev, int nblocks,
+                      cudaStream_t st) {
+    lls_partials_kernel<<<nblocks, kIcpThreads, 0, st>>>(A, b, n, partials);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    lls_solve_kernel<<<1, 256, 0, st>>>(partials, nblocks, x_dev);
+    return cudaGetLastError();
+}
+
+}  // namespace kf

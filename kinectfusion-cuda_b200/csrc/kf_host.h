@@ -1,0 +1,83 @@
+// kf_host.h -- host-side interface between the C ABI layer and the kernel files.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "kf_device.cuh"
+
+namespace kf {
+
+// Table sizes the kernels read from device memory, so that a captured graph stays valid
+// when the work lists change (sessions opening and closing).
+struct Tables {
+    int S;                   // slot capacity (length of the session / step / range arrays)
+    int n_pre;               // preprocessing tiles
+    int n_ray;               // raycast tiles
+    int n_itiles[kMaxLevels];// ICP tiles per level
+    int icp_off[kMaxLevels]; // offset of each level's tiles in the ICP tile array
+    int max_levels;
+    int pad;
+    long long fuse_total;    // fusion segments over all slots
+};
+
+// raw pointers the kernels take
+struct EngineView {
+    const SessionDev* sess;
+    const StepDev* step;
+    OutDev* out;
+    const Tables* tb;
+    const PreTile* pre;
+    const RayTile* ray;
+    const IcpTile* itiles;
+    const IcpRange* iranges;     // [level * S + s]
+    const long long* fuse_prefix;// S + 1 entries, in segments
+    float* partials;             // ICP block partials, 54 floats per tile
+    GridSync* sync;
+    unsigned int* counters;      // [0] raycast tiles, [1..] fusion segments (64-bit at [2])
+};
+
+constexpr int kPreTileSize = 32;
+constexpr int kRayTileW = 16, kRayTileH = 16;
+constexpr int kIcpThreads = 256;
+constexpr int kIcpPxPerThread = 8;
+constexpr int kIcpTilePx = kIcpThreads * kIcpPxPerThread;
+constexpr int kIcpMaxPasses = 64;     // hard cap on ICP passes per frame
+
+// launch helpers (each returns the CUDA error of its launch)
+cudaError_t launch_preprocess(const EngineView& v, int grid, cudaStream_t st);
+cudaError_t launch_raycast(const EngineView& v, int grid, cudaStream_t st);
+cudaError_t launch_icp(const EngineView& v, int grid, cudaStream_t st);
+cudaError_t launch_fuse(const EngineView& v, int grid, cudaStream_t st);
+int icp_max_grid(int num_sms);
+cudaError_t launch_barrier_selftest(GridSync* g, unsigned long long timeout_ns, int* result, cudaStream_t st);
+int fuse_segs_per_row(int n, int fmt);
+int fuse_vec(int fmt);
+
+cudaError_t launch_init_volume(void* f, void* w, long long nvox, int fmt, cudaStream_t st);
+cudaError_t launch_export_interleaved(const void* f, const void* w, long long nvox, int fmt, float* dst, cudaStream_t st);
+cudaError_t launch_import_interleaved(const float* src, void* f, void* w, long long nvox, int fmt, cudaStream_t st);
+
+// stage kernels (per-stage C ABI)
+cudaError_t stage_convert(const uint16_t* raw, float* out, int w, int h, float scale, int unmirror, cudaStream_t st);
+cudaError_t stage_bilateral(const float* in, float* out, int w, int h, float ss, float sr, int r, cudaStream_t st);
+cudaError_t stage_down_sample(const float* in, float* out, int wo, int ho, float sr, cudaStream_t st);
+cudaError_t stage_vertex(const float* d, float4* v, int w, int h, const float* ik, cudaStream_t st);
+cudaError_t stage_normal(const float4* v, float4* n, int w, int h, cudaStream_t st);
+cudaError_t stage_raycast(const kf_volume* vol, const float* pose, const float* ik, float4* vtx, float4* nrm, int w,
+                          int h, float min_d, float max_d, float step_l, float step_s, cudaStream_t st);
+cudaError_t stage_fuse(const float* depth, int w, int h, const float* k, const kf_volume* vol, const float* pose,
+                       float min_d, float max_d, const float* xs, const float* zs, cudaStream_t st);
+cudaError_t stage_icp_residuals(const float4* vmap, const float4* tv, const float4* tn, int w, int h,
+                                const float* Rp, const float* tp, const float* Rc, const float* tc, const float* k,
+                                float dist, float angle, float* A, float* b, cudaStream_t st);
+// LinearLeastSquares::solve: partials of the normal equations then an FP64 combine + solve
+int lls_num_blocks(int n);
+cudaError_t stage_lls(const float* A, const float* b, int n, float* partials, double* x_dev, int nblocks,
+                      cudaStream_t st);
+
+// host math shared by the API layer
+void voxel_axes(int n, float width, float* xs, float* zs);
+void level_intrinsics(const kf_config& c, int level, float k[9], float ik[9]);
+
+}  // namespace kf

@@ -1,0 +1,572 @@
+"""kfb200 -- Python host mirror of the reference's KinectFusion interface over libkfb200.so.
+
+The names follow the reference (isikmustafa/kinectfusion-cuda, project/src):
+
+    KinectFusion            project/src/kinect_fusion.h:38-48  (per-frame pipeline)
+    kernel.*                project/src/measurement.cuh, raycast.cuh, tsdf.cuh, icp.cuh
+    ICP.computePose         project/src/icp.h:35-36
+    LinearLeastSquares      project/src/linear_least_squares.h:19
+    poseError               project/src/general_helper.h:9
+
+Host arrays are numpy; device arrays for the per-stage ``kernel`` calls are torch CUDA
+tensors (torch is only the allocator here).  4x4 poses and 3x3 matrices are numpy arrays
+indexed [row, col]; they are converted to the column-major layout of the C ABI at the
+boundary.  Every call goes through the CUDA library; there is no CPU path.
+"""
+import ctypes
+
+import numpy as np
+
+from . import _lib
+from ._lib import (KF_ERR_ARG, KF_ERR_CAPACITY, KF_ERR_CUDA, KF_ERR_NONFINITE, KF_ERR_OOM_BUDGET, KF_ERR_SHAPE,
+                   KF_ERR_STATE, KF_ERR_TIMEOUT, KF_MAX_LEVELS, KF_OK, KF_TSDF_F16U16, KF_TSDF_F32F32, KF_WEIGHT_SCALE,
+                   KfConfig, KfError, KfFrameStats, KfServerStats, KfVolume, check, lib)
+
+__all__ = [
+    "KfConfig", "KfError", "default_config", "config_small", "config_full", "KinectFusion", "kernel", "ICP",
+    "LinearLeastSquares", "poseError", "Batch", "Server", "lib", "to_colmajor", "from_colmajor",
+]
+
+
+# ------------------------------------------------------------------------------------------
+# conversions
+# ------------------------------------------------------------------------------------------
+def to_colmajor(m):
+    """numpy [row, col] matrix -> ctypes float array in column-major (glm) order."""
+    m = np.asarray(m, dtype=np.float32)
+    flat = np.ascontiguousarray(m.T).reshape(-1)
+    return (ctypes.c_float * flat.size)(*flat.tolist())
+
+
+def from_colmajor(arr, dim):
+    a = np.array(arr[: dim * dim], dtype=np.float32)
+    return a.reshape(dim, dim).T.copy()
+
+
+def _fptr(a):
+    return ctypes.cast(a, ctypes.POINTER(ctypes.c_float))
+
+
+def _np_ptr(a):
+    # data_as keeps a reference to the array, so temporaries live through the call
+    return a.ctypes.data_as(ctypes.c_void_p)
+
+
+def _dev_ptr(t):
+    """Device address of a torch CUDA tensor (the only accepted device buffer type)."""
+    if not hasattr(t, "data_ptr") or not getattr(t, "is_cuda", False):
+        raise TypeError("device buffers must be torch CUDA tensors")
+    if not t.is_contiguous():
+        raise ValueError("device buffers must be contiguous")
+    return ctypes.c_void_p(t.data_ptr())
+
+
+def _stream(stream):
+    if stream is None:
+        return None
+    return ctypes.c_void_p(int(getattr(stream, "cuda_stream", stream)))
+
+
+# ------------------------------------------------------------------------------------------
+# configuration
+# ------------------------------------------------------------------------------------------
+def default_config(**overrides):
+    """The reference's configuration (project/src/main.cpp:11-59, dataset mode), with
+    keyword overrides for any field of kf_config."""
+    c = KfConfig()
+    lib.kf_config_default(ctypes.byref(c))
+    for k, v in overrides.items():
+        if k == "iters":
+            for i in range(KF_MAX_LEVELS):
+                c.iters[i] = int(v[i]) if i < len(v) else 0
+        elif k == "initial_pose":
+            flat = np.asarray(v, dtype=np.float32).T.reshape(-1)
+            for i in range(16):
+                c.initial_pose[i] = float(flat[i])
+        else:
+            if not hasattr(c, k):
+                raise AttributeError("kf_config has no field %r" % k)
+            setattr(c, k, v)
+    return c
+
+
+def start_pose(cube_width):
+    """Camera at (0, 0, -cube_width) looking along +z: the synthetic scenes' start pose."""
+    p = np.eye(4, dtype=np.float32)
+    p[2, 3] = -cube_width
+    return p
+
+
+def config_small(**overrides):
+    """Plain pipeline, small size: 320x240, fx = fy = 262.5, 128^3 float/float TSDF over a
+    2 m cube, truncation 0.03 m, bilateral sigma_s 4.5 px / sigma_r 30 mm / 5x5, ICP 4/5/10
+    coarse to fine, 0.1 m / 20 degrees, depth in millimetres."""
+    kw = dict(width=320, height=240, fx=262.5, fy=262.5, cx=159.5, cy=119.5, depth_scale=1e-3,
+              iters=(10, 5, 4), dist_thresh=0.1, angle_thresh=float(np.deg2rad(20.0)),
+              bilateral_sigma_s=4.5, bilateral_sigma_r=0.03, bilateral_radius=2,
+              volume_n=128, volume_width=2.0, mu=0.03, initial_pose=start_pose(2.0))
+    kw.update(overrides)
+    return default_config(**kw)
+
+
+def config_full(**overrides):
+    """Plain pipeline at full size: 640x480, fx = fy = 525, 512^3 float/float TSDF over a
+    3 m cube, truncation 0.02 m, ICP 4/5/10 coarse to fine."""
+    kw = dict(width=640, height=480, fx=525.0, fy=525.0, cx=319.5, cy=239.5, depth_scale=1e-3,
+              iters=(10, 5, 4), dist_thresh=0.1, angle_thresh=float(np.deg2rad(20.0)),
+              bilateral_sigma_s=4.5, bilateral_sigma_r=0.03, bilateral_radius=2,
+              volume_n=512, volume_width=3.0, mu=0.02, initial_pose=start_pose(3.0))
+    kw.update(overrides)
+    return default_config(**kw)
+
+
+def level_intrinsics(cfg, level):
+    """K_l of the reference's Sensor (project/src/sensor.h:14-19) as a numpy 3x3."""
+    s = np.float32(1.0) / np.float32(1 << level)
+    k = np.zeros((3, 3), dtype=np.float32)
+    k[0, 0] = np.float32(cfg.fx) * s
+    k[1, 1] = np.float32(cfg.fy) * s
+    k[0, 2] = (np.float32(cfg.cx) + np.float32(0.5)) * s - np.float32(0.5)
+    k[1, 2] = (np.float32(cfg.cy) + np.float32(0.5)) * s - np.float32(0.5)
+    k[2, 2] = 1.0
+    return k
+
+
+# ------------------------------------------------------------------------------------------
+# the per-frame pipeline
+# ------------------------------------------------------------------------------------------
+class KinectFusion:
+    """One reconstruction session (the reference's KinectFusion class).
+
+    process_frame(depth) runs one frame: frame 0 fuses only, later frames preprocess,
+    raycast at the previous pose, run ICP and fuse (project/src/kinect_fusion.cpp:44-94).
+    """
+
+    def __init__(self, config, _handle=None, _owner=None):
+        self.config = config
+        self._owner = _owner
+        if _handle is not None:
+            self._s = _handle
+            self._owns = False
+        else:
+            h = ctypes.c_void_p()
+            check(lib.kf_session_create(ctypes.byref(config), ctypes.byref(h)), "kf_session_create")
+            self._s = h
+            self._owns = True
+        self.w, self.h = config.width, config.height
+
+    def close(self):
+        if getattr(self, "_owns", False) and self._s:
+            lib.kf_session_destroy(self._s)
+        self._s = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def reset(self):
+        check(lib.kf_session_reset(self._s), "kf_session_reset")
+
+    def process_frame(self, depth, stream=None):
+        """depth: (h, w) uint16 numpy array (host) or torch CUDA tensor.  Returns
+        (status, pose 4x4); a non-finite ICP solution returns KF_ERR_NONFINITE with the
+        previous pose kept (the reference throws, project/src/icp.cpp:67-73)."""
+        pose = (ctypes.c_float * 16)()
+        if hasattr(depth, "is_cuda") and depth.is_cuda:
+            st = lib.kf_process_frame(self._s, _dev_ptr(depth), 1, _stream(stream), pose)
+        else:
+            d = np.ascontiguousarray(depth, dtype=np.uint16)
+            if d.shape != (self.h, self.w):
+                raise ValueError("depth frame must be %dx%d" % (self.h, self.w))
+            st = lib.kf_process_frame(self._s, _np_ptr(d), 0, _stream(stream), pose)
+        if st not in (KF_OK, KF_ERR_NONFINITE):
+            raise KfError(st, "kf_process_frame")
+        return st, from_colmajor(pose, 4)
+
+    def startTracking(self, frames):
+        """Run every frame of an iterable (the reference reads them from a dataset,
+        project/src/kinect_fusion.cpp:44-73); returns the list of poses."""
+        return [self.process_frame(f)[1] for f in frames]
+
+    # taps
+    def pose(self):
+        p = (ctypes.c_float * 16)()
+        check(lib.kf_get_pose(self._s, p))
+        return from_colmajor(p, 4)
+
+    def set_pose(self, pose):
+        check(lib.kf_set_pose(self._s, to_colmajor(pose)))
+
+    def frame_stats(self):
+        st = KfFrameStats()
+        check(lib.kf_get_frame_stats(self._s, ctypes.byref(st)))
+        return {"frame": st.frame, "status": st.status, "icp_iters": list(st.icp_iters)}
+
+    def _lw(self, level):
+        return self.w >> level, self.h >> level
+
+    def depth(self, level=0):
+        w, h = (self.w, self.h) if level < 0 else self._lw(level)
+        out = np.empty((h, w), np.float32)
+        check(lib.kf_get_depth(self._s, level, _np_ptr(out), 1))
+        return out
+
+    def vertex_map(self, level=0):
+        w, h = self._lw(level)
+        out = np.empty((h, w, 4), np.float32)
+        check(lib.kf_get_vertex(self._s, level, _np_ptr(out), 1))
+        return out
+
+    def raycast_maps(self, level=0):
+        w, h = self._lw(level)
+        v = np.empty((h, w, 4), np.float32)
+        n = np.empty((h, w, 4), np.float32)
+        check(lib.kf_get_raycast(self._s, level, _np_ptr(v), _np_ptr(n), 1))
+        return v, n
+
+    def icp_mask(self, level=0):
+        w, h = self._lw(level)
+        m = np.empty((h, w), np.uint8)
+        check(lib.kf_get_icp_mask(self._s, level, _np_ptr(m), 1))
+        return m
+
+    def tsdf(self):
+        """(f, w) float32 arrays of shape (n, n, n) indexed [z, y, x]."""
+        n = self.config.volume_n
+        inter = np.empty((n, n, n, 2), np.float32)
+        check(lib.kf_get_tsdf(self._s, _np_ptr(inter), inter.nbytes, 1, 1))
+        return inter[..., 0].copy(), inter[..., 1].copy()
+
+    def set_tsdf(self, f, w):
+        n = self.config.volume_n
+        inter = np.empty((n, n, n, 2), np.float32)
+        inter[..., 0] = f
+        inter[..., 1] = w
+        check(lib.kf_set_tsdf(self._s, _np_ptr(inter), inter.nbytes, 1, 1))
+
+    def saveTSDF(self, path):
+        """Reference .bin layout: n^3 float2 {f, w}, x fastest (project/src/voxel_grid.cpp:43-62)."""
+        n = self.config.volume_n
+        inter = np.empty((n, n, n, 2), np.float32)
+        check(lib.kf_get_tsdf(self._s, _np_ptr(inter), inter.nbytes, 1, 1))
+        inter.tofile(path)
+
+    def loadTSDF(self, path):
+        n = self.config.volume_n
+        inter = np.fromfile(path, dtype=np.float32, count=n * n * n * 2)
+        if inter.size != n * n * n * 2:
+            raise ValueError("TSDF file is too short")
+        check(lib.kf_set_tsdf(self._s, _np_ptr(inter), inter.nbytes, 1, 1))
+
+    def volume(self):
+        v = KfVolume()
+        check(lib.kf_get_volume(self._s, ctypes.byref(v)))
+        return v
+
+    def process_frame_async(self, depth_dev, stream=None):
+        """Enqueue a frame already in device memory (torch CUDA uint16 tensor); no sync."""
+        check(lib.kf_process_frame_async(self._s, _dev_ptr(depth_dev), _stream(stream)), "kf_process_frame_async")
+
+    def set_profiling(self, on=True):
+        check(lib.kf_session_set_profiling(self._s, int(bool(on))))
+
+    def stage_times(self):
+        """Device ms of preprocess, raycast, ICP and fusion in the last completed step."""
+        ms = (ctypes.c_float * 4)()
+        check(lib.kf_session_stage_times(self._s, ms))
+        return list(ms)
+
+
+# ------------------------------------------------------------------------------------------
+# per-stage calls (the reference's kernel:: namespace), on torch CUDA tensors
+# ------------------------------------------------------------------------------------------
+class kernel:  # noqa: N801 -- mirrors the reference's C++ namespace
+    """Each call returns the elapsed milliseconds, like the reference's wrappers
+    (project/src/measurement.cuh:11), and raises KfError(KF_ERR_SHAPE) where the reference
+    throws std::runtime_error."""
+
+    @staticmethod
+    def _ms(fn, *args):
+        ms = ctypes.c_float(0.0)
+        check(fn(*args, ctypes.byref(ms)), fn.__name__)
+        return ms.value
+
+    @staticmethod
+    def convertToDepthMeters(raw, out, scale, unmirror=False, stream=None):
+        h, w = raw.shape
+        oh, ow = out.shape
+        return kernel._ms(lib.kf_convert_to_depth_meters, _dev_ptr(raw), w, h, _dev_ptr(out), ow, oh, scale,
+                          int(unmirror), _stream(stream))
+
+    @staticmethod
+    def applyBilateralFilter(inp, out, sigma_s=4.0, sigma_r=0.25, radius=3, stream=None):
+        h, w = inp.shape
+        oh, ow = out.shape
+        return kernel._ms(lib.kf_apply_bilateral_filter, _dev_ptr(inp), w, h, _dev_ptr(out), ow, oh, sigma_s,
+                          sigma_r, radius, _stream(stream))
+
+    @staticmethod
+    def downSample(inp, out, sigma_r=0.25, stream=None):
+        h, w = inp.shape
+        oh, ow = out.shape
+        return kernel._ms(lib.kf_down_sample, _dev_ptr(inp), w, h, _dev_ptr(out), ow, oh, sigma_r, _stream(stream))
+
+    @staticmethod
+    def createVertexMap(depth, vertex, inv_cam_k, stream=None):
+        h, w = depth.shape
+        oh, ow = vertex.shape[:2]
+        return kernel._ms(lib.kf_create_vertex_map, _dev_ptr(depth), w, h, _dev_ptr(vertex), ow, oh,
+                          to_colmajor(inv_cam_k), _stream(stream))
+
+    @staticmethod
+    def createNormalMap(vertex, normal, stream=None):
+        h, w = vertex.shape[:2]
+        oh, ow = normal.shape[:2]
+        return kernel._ms(lib.kf_create_normal_map, _dev_ptr(vertex), w, h, _dev_ptr(normal), ow, oh,
+                          _stream(stream))
+
+    @staticmethod
+    def volume(f, w, width, mu, fmt=KF_TSDF_F32F32, max_weight=0.0):
+        """A kf_volume over torch tensors f, w of shape (n, n, n)."""
+        v = KfVolume()
+        v.f = _dev_ptr(f).value
+        v.w = _dev_ptr(w).value
+        v.n = int(f.shape[0])
+        v.width = float(width)
+        v.mu = float(mu)
+        v.format = int(fmt)
+        v.max_weight = float(max_weight)
+        return v
+
+    @staticmethod
+    def initializeGrid(vol, stream=None):
+        return kernel._ms(lib.kf_initialize_grid, ctypes.byref(vol), _stream(stream))
+
+    @staticmethod
+    def fuse(depth_m, vol, pose, cam_k, min_depth=0.4, max_depth=6.0, stream=None):
+        h, w = depth_m.shape
+        return kernel._ms(lib.kf_fuse, _dev_ptr(depth_m), w, h, to_colmajor(cam_k), ctypes.byref(vol),
+                          to_colmajor(pose), min_depth, max_depth, _stream(stream))
+
+    @staticmethod
+    def raycast(vol, pose, inv_cam_k, vertex, normal, min_depth=0.4, max_depth=6.0, step_large=1.99,
+                step_small=0.1, stream=None):
+        h, w = vertex.shape[:2]
+        nh, nw = normal.shape[:2]
+        return kernel._ms(lib.kf_raycast, ctypes.byref(vol), to_colmajor(pose), to_colmajor(inv_cam_k),
+                          _dev_ptr(vertex), w, h, _dev_ptr(normal), nw, nh, min_depth, max_depth, step_large,
+                          step_small, _stream(stream))
+
+    @staticmethod
+    def constructIcpResiduals(vertex, target_vertex, target_normal, prev_rot, prev_transl, cur_rot, cur_transl,
+                              cam_k, distance_thresh, angle_thresh, mat_a, vec_b, stream=None):
+        h, w = vertex.shape[:2]
+        pt = (ctypes.c_float * 3)(*[float(x) for x in prev_transl])
+        ct = (ctypes.c_float * 3)(*[float(x) for x in cur_transl])
+        return kernel._ms(lib.kf_construct_icp_residuals, _dev_ptr(vertex), _dev_ptr(target_vertex),
+                          _dev_ptr(target_normal), w, h, to_colmajor(prev_rot), pt, to_colmajor(cur_rot), ct,
+                          to_colmajor(cam_k), distance_thresh, angle_thresh, _dev_ptr(mat_a), _dev_ptr(vec_b),
+                          _stream(stream))
+
+
+class LinearLeastSquares:
+    """LinearLeastSquares::solve (project/src/linear_least_squares.cpp:23-44) on device A, b."""
+
+    def solve(self, mat_a, vec_b, n_equations, stream=None):
+        x = (ctypes.c_float * 6)()
+        st = lib.kf_solve_linear_least_squares(_dev_ptr(mat_a), _dev_ptr(vec_b), int(n_equations), x,
+                                               _stream(stream))
+        if st not in (KF_OK, KF_ERR_NONFINITE):
+            raise KfError(st, "kf_solve_linear_least_squares")
+        return np.array(x[:], dtype=np.float32)
+
+
+class ICP:
+    """ICP::computePose (project/src/icp.cpp:25-58) over device pyramids."""
+
+    def __init__(self, config):
+        self.config = config
+
+    def computePose(self, vertex_pyramid, target_vertex_pyramid, target_normal_pyramid, pose, stream=None):
+        levels = len(vertex_pyramid)
+        h, w = vertex_pyramid[0].shape[:2]
+        arr = ctypes.c_void_p * levels
+        v = arr(*[_dev_ptr(t) for t in vertex_pyramid])
+        tv = arr(*[_dev_ptr(t) for t in target_vertex_pyramid])
+        tn = arr(*[_dev_ptr(t) for t in target_normal_pyramid])
+        out = (ctypes.c_float * 16)()
+        iters = (ctypes.c_int * KF_MAX_LEVELS)()
+        st = lib.kf_compute_pose(v, tv, tn, w, h, levels, ctypes.byref(self.config), to_colmajor(pose), out, iters,
+                                 _stream(stream))
+        if st not in (KF_OK, KF_ERR_NONFINITE):
+            raise KfError(st, "kf_compute_pose")
+        return st, from_colmajor(out, 4), list(iters)
+
+
+def poseError(pose_1, pose_2):
+    """poseError (project/src/general_helper.cpp:11-21): (rotation chord, translation distance)."""
+    out = (ctypes.c_float * 2)()
+    check(lib.kf_pose_error(to_colmajor(pose_1), to_colmajor(pose_2), out))
+    return float(out[0]), float(out[1])
+
+
+# ------------------------------------------------------------------------------------------
+# batched and served forms
+# ------------------------------------------------------------------------------------------
+class Batch:
+    """Many independent sessions stepped together: one persistent launch per stage over all
+    of them, replayed from a captured CUDA graph."""
+
+    def __init__(self, configs):
+        self.configs = list(configs)
+        arr = (KfConfig * len(self.configs))(*self.configs)
+        h = ctypes.c_void_p()
+        check(lib.kf_batch_create(arr, len(self.configs), ctypes.byref(h)), "kf_batch_create")
+        self._b = h
+        self._sessions = {}
+
+    def close(self):
+        if self._b:
+            lib.kf_batch_destroy(self._b)
+        self._b = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __len__(self):
+        return len(self.configs)
+
+    def step(self, frames, stream=None):
+        """frames: list (one per session) of (h, w) uint16 numpy arrays or None to skip.
+        Returns (status, poses (n, 4, 4))."""
+        n = len(self.configs)
+        keep = []
+        ptrs = (ctypes.c_void_p * n)()
+        for i, f in enumerate(frames):
+            if f is None:
+                ptrs[i] = None
+                continue
+            a = np.ascontiguousarray(f, dtype=np.uint16)
+            keep.append(a)
+            ptrs[i] = a.ctypes.data
+        poses = (ctypes.c_float * (16 * n))()
+        st = lib.kf_batch_step(self._b, ptrs, 0, _stream(stream), poses)
+        if st not in (KF_OK, KF_ERR_NONFINITE):
+            raise KfError(st, "kf_batch_step")
+        p = np.array(poses[:], dtype=np.float32).reshape(n, 4, 4).transpose(0, 2, 1).copy()
+        return st, p
+
+    def session(self, i):
+        h = ctypes.c_void_p()
+        check(lib.kf_batch_session(self._b, i, ctypes.byref(h)))
+        return KinectFusion(self.configs[i], _handle=h, _owner=self)
+
+    def input_buffer(self, i):
+        p = ctypes.c_void_p()
+        check(lib.kf_batch_input_buffer(self._b, i, ctypes.byref(p)))
+        return p.value
+
+    def step_async(self, active, stream=None):
+        arr = (ctypes.c_int * len(self.configs))(*[int(bool(a)) for a in active])
+        check(lib.kf_batch_step_async(self._b, arr, _stream(stream)), "kf_batch_step_async")
+
+    def autotune(self, stream=None):
+        buf = ctypes.create_string_buffer(1024)
+        check(lib.kf_batch_autotune(self._b, _stream(stream), buf, 1024), "kf_batch_autotune")
+        return buf.value.decode()
+
+    def set_profiling(self, on=True):
+        check(lib.kf_batch_set_profiling(self._b, int(bool(on))))
+
+    def stage_times(self):
+        ms = (ctypes.c_float * 4)()
+        check(lib.kf_batch_stage_times(self._b, ms))
+        return list(ms)
+
+
+def selftest_bounded_wait(timeout_ms=50):
+    """Runs a device wait nothing releases; returns (status, wall ms).  The expected status
+    is KF_ERR_TIMEOUT: the wait gave up on its own and the context is still usable."""
+    waited = ctypes.c_int(0)
+    st = lib.kf_selftest_bounded_wait(int(timeout_ms), ctypes.byref(waited))
+    return st, waited.value
+
+
+class Server:
+    """Continuous batching: sessions open and close at any time, frames are submitted as
+    they arrive and every step serves all queued frames together."""
+
+    def __init__(self, max_slots, hbm_budget_bytes):
+        h = ctypes.c_void_p()
+        check(lib.kf_server_create(int(max_slots), int(hbm_budget_bytes), ctypes.byref(h)), "kf_server_create")
+        self._s = h
+        self._cfg = {}
+
+    def close(self):
+        if self._s:
+            lib.kf_server_destroy(self._s)
+        self._s = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def open(self, config):
+        """Returns the session id, or raises KfError(KF_ERR_OOM_BUDGET / KF_ERR_CAPACITY)."""
+        sid = ctypes.c_int()
+        check(lib.kf_server_open(self._s, ctypes.byref(config), ctypes.byref(sid)), "kf_server_open")
+        self._cfg[sid.value] = config
+        return sid.value
+
+    def try_open(self, config):
+        sid = ctypes.c_int()
+        st = lib.kf_server_open(self._s, ctypes.byref(config), ctypes.byref(sid))
+        if st == KF_OK:
+            self._cfg[sid.value] = config
+            return sid.value
+        if st in (KF_ERR_OOM_BUDGET, KF_ERR_CAPACITY):
+            return None
+        raise KfError(st, "kf_server_open")
+
+    def close_session(self, sid):
+        check(lib.kf_server_close(self._s, sid), "kf_server_close")
+        self._cfg.pop(sid, None)
+
+    def submit(self, sid, depth, t_ms=None):
+        d = np.ascontiguousarray(depth, dtype=np.uint16)
+        t = lib.kf_now_ms() if t_ms is None else float(t_ms)
+        return lib.kf_server_submit(self._s, sid, _np_ptr(d), t)
+
+    def step(self):
+        n = ctypes.c_int()
+        st = lib.kf_server_step(self._s, ctypes.byref(n))
+        if st not in (KF_OK, KF_ERR_NONFINITE):
+            raise KfError(st, "kf_server_step")
+        return n.value
+
+    def result(self, sid):
+        p = (ctypes.c_float * 16)()
+        fs = KfFrameStats()
+        check(lib.kf_server_result(self._s, sid, p, ctypes.byref(fs)), "kf_server_result")
+        return from_colmajor(p, 4), {"frame": fs.frame, "status": fs.status, "icp_iters": list(fs.icp_iters)}
+
+    def session(self, sid):
+        h = ctypes.c_void_p()
+        check(lib.kf_server_get_session(self._s, sid, ctypes.byref(h)))
+        return KinectFusion(self._cfg[sid], _handle=h, _owner=self)
+
+    def stats(self):
+        s = KfServerStats()
+        check(lib.kf_server_stats_get(self._s, ctypes.byref(s)))
+        return {f: getattr(s, f) for f, _ in KfServerStats._fields_}
+
+    @staticmethod
+    def now_ms():
+        return lib.kf_now_ms()

@@ -1,0 +1,185 @@
+"""End-to-end parity of the per-frame pipeline (kf_session, graph-replayed) against the CPU
+oracle's restatement of KinectFusion::startTracking on the same seeded synthetic frames.
+
+Bounds: per-frame pose within 1e-4 rad (rotation chord) / 1e-4 m of the FP64 oracle; depth
+pyramid and valid-pixel masks equal, values within 2e-6 relative; ICP correspondence masks
+agreeing on >= 99.9% of pixels; TSDF within 1e-3 of the truncation distance on >= 99.9% of
+voxels; raycast depth within 1 mm on >= 99.9% of pixels where both hit."""
+import os
+import tempfile
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+NFRAMES = 10
+
+
+@pytest.fixture(scope="module")
+def run_small(kf, orc, cuda):
+    from kfb200 import synth
+    cfg = kf.config_small(export_icp_mask=1)
+    imgs, gt = synth.sequence(cfg, NFRAMES, seed=33)
+    s = kf.KinectFusion(cfg)
+    P = orc.Pipeline(cfg, prec=1)
+    rows = []
+    for i, img in enumerate(imgs):
+        st_g, pose_g = s.process_frame(img)
+        st_o, pose_o = P.process_frame(img)
+        rows.append((st_g, st_o, pose_g, pose_o, s.frame_stats()["icp_iters"], P.iters()))
+    return cfg, imgs, s, P, rows
+
+
+def test_pose_per_frame(kf, run_small):
+    cfg, imgs, s, P, rows = run_small
+    for i, (st_g, st_o, pg, po, ig, io) in enumerate(rows):
+        assert st_g == st_o == kf.KF_OK, i
+        a, d = kf.poseError(po, pg)
+        assert a <= 1e-4 and d <= 1e-4, (i, a, d, ig, io)
+
+
+def test_first_frame_fuses_only(kf, run_small):
+    cfg, imgs, s, P, rows = run_small
+    assert rows[0][4] == [0, 0, 0]
+    np.testing.assert_array_equal(rows[0][2], kf.start_pose(cfg.volume_width))
+
+
+def test_pyramid_and_masks(kf, orc, run_small):
+    cfg, imgs, s, P, rows = run_small
+    np.testing.assert_array_equal(s.depth(-1), P.depth(-1))     # uint16 -> fp16 -> metres, bit exact
+    for level in range(3):
+        gd, od = s.depth(level), P.depth(level)
+        np.testing.assert_array_equal(gd > 0.01, od > 0.01)
+        v = od > 0.01
+        np.testing.assert_allclose(gd[v], od[v], rtol=2e-6)
+        gv, ov = s.vertex_map(level), P.vertex_map(level)
+        np.testing.assert_array_equal(gv[..., 3], ov[..., 3])
+
+
+def test_icp_masks(kf, run_small):
+    cfg, imgs, s, P, rows = run_small
+    for level in range(3):
+        agree = np.mean(s.icp_mask(level) == P.icp_mask(level))
+        assert agree >= 0.999, (level, agree)
+
+
+def test_raycast_maps(kf, run_small):
+    cfg, imgs, s, P, rows = run_small
+    cam = rows[-2][3][:3, 3]   # the raycast of the last frame ran at the previous pose
+    for level in range(3):
+        gv, gn = s.raycast_maps(level)
+        ov, on = P.raycast_maps(level)
+        gh, oh = gv[..., 3] == -1, ov[..., 3] == -1
+        assert np.mean(gh == oh) >= 0.999
+        both = gh & oh
+        dz = np.abs(np.linalg.norm(gv[both][:, :3] - cam, axis=1) - np.linalg.norm(ov[both][:, :3] - cam, axis=1))
+        assert np.mean(dz <= 1e-3) >= 0.999
+
+
+def test_tsdf(kf, run_small):
+    cfg, imgs, s, P, rows = run_small
+    gf, gw = s.tsdf()
+    of, ow = P.tsdf()
+    assert np.mean(np.abs(gf - of) <= 1e-3) >= 0.999
+    assert np.mean((gw > 0) == (ow > 0)) >= 0.9999
+
+
+def test_tsdf_save_load_roundtrip(kf, run_small):
+    cfg, imgs, s, P, rows = run_small
+    f, w = s.tsdf()
+    with tempfile.TemporaryDirectory() as d:
+        path = os.path.join(d, "tsdf.bin")
+        s.saveTSDF(path)
+        raw = np.fromfile(path, np.float32).reshape(cfg.volume_n, cfg.volume_n, cfg.volume_n, 2)
+        np.testing.assert_array_equal(raw[..., 0], f)     # reference .bin layout: {f, w}, x fastest
+        other = kf.KinectFusion(cfg)
+        other.loadTSDF(path)
+        f2, w2 = other.tsdf()
+        np.testing.assert_array_equal(f2, f)
+        np.testing.assert_array_equal(w2, w)
+        other.close()
+
+
+def test_nonfinite_keeps_pose_and_skips_fusion(kf, run_small):
+    cfg, imgs, s, P, rows = run_small
+    pose0 = s.pose()
+    f0, w0 = s.tsdf()
+    st, pose = s.process_frame(np.zeros((cfg.height, cfg.width), np.uint16))   # no correspondences
+    assert st == kf.KF_ERR_NONFINITE
+    np.testing.assert_array_equal(pose, pose0)
+    f1, w1 = s.tsdf()
+    np.testing.assert_array_equal(f1, f0)
+    assert s.frame_stats()["status"] == kf.KF_ERR_NONFINITE
+
+
+def test_reset_replays_identically(kf, run_small):
+    cfg, imgs, s, P, rows = run_small
+    s.reset()
+    for i in range(3):
+        st, pose = s.process_frame(imgs[i])
+        np.testing.assert_array_equal(pose, rows[i][2])
+
+
+def test_device_input_path(kf, cuda, run_small):
+    cfg, imgs, s, P, rows = run_small
+    s2 = kf.KinectFusion(cfg)
+    for i in range(3):
+        d = cuda.from_numpy(imgs[i].view(np.int16)).cuda()
+        st, pose = s2.process_frame(d)
+        np.testing.assert_array_equal(pose, rows[i][2])
+    s2.close()
+
+
+def test_trunc8_compat_mode(kf, orc):
+    from kfb200 import synth
+    cfg = kf.config_small(compat_trunc8=1)
+    imgs, _ = synth.sequence(cfg, 4, seed=35)
+    s = kf.KinectFusion(cfg)
+    P = orc.Pipeline(cfg, prec=1)
+    for img in imgs:
+        _, pg = s.process_frame(img)
+        _, po = P.process_frame(img)
+        a, d = kf.poseError(po, pg)
+        assert a <= 1e-4 and d <= 1e-4
+    # level 2 of 320x240 is 80x60: the reference's 8x8 grid never writes rows 56-59
+    assert np.all(s.depth(2)[56:] == 0) and np.all(s.vertex_map(2)[56:, :, 3] == 0)
+    s.close()
+
+
+def test_f16u16_precision_form_vs_fp64(kf, orc):
+    """FP16 distance + uint16 weight volume against the FP64 oracle (float volume): reported
+    error bounds for pose, TSDF (in truncation units) and raycast depth."""
+    from kfb200 import synth
+    cfg16 = kf.config_small(tsdf_format=kf.KF_TSDF_F16U16)
+    cfg = kf.config_small()
+    imgs, _ = synth.sequence(cfg, 8, seed=37)
+    s = kf.KinectFusion(cfg16)
+    P = orc.Pipeline(cfg, prec=1)
+    worst = 0.0
+    for img in imgs:
+        _, pg = s.process_frame(img)
+        _, po = P.process_frame(img)
+        worst = max(worst, *kf.poseError(po, pg))
+    assert worst <= 5e-4
+    gf, gw = s.tsdf()
+    of, ow = P.tsdf()
+    obs = (ow > 0) & (gw > 0)
+    rms = np.sqrt(np.mean((gf[obs] - of[obs]) ** 2))
+    assert rms < 5e-3
+    s.close()
+
+
+def test_bilateral_radius_zero_and_single_level(kf, orc):
+    from kfb200 import synth
+    cfg = kf.config_small(levels=1, iters=(6, 0, 0), bilateral_radius=0)
+    imgs, _ = synth.sequence(cfg, 3, seed=39)
+    s = kf.KinectFusion(cfg)
+    P = orc.Pipeline(cfg, prec=1)
+    for img in imgs:
+        _, pg = s.process_frame(img)
+        _, po = P.process_frame(img)
+        a, d = kf.poseError(po, pg)
+        assert a <= 1e-4 and d <= 1e-4
+    np.testing.assert_allclose(s.depth(0), s.depth(-1), rtol=0)   # a 1x1 window is the identity
+    s.close()
