@@ -37,8 +37,9 @@ extern "C" {
 
 #define KF_API_VERSION 1
 #define KF_MAX_LEVELS 3
-/* fixed-point steps per unit of weight in the uint16 weight array of KF_TSDF_F16U16 */
-#define KF_WEIGHT_SCALE 128.0f
+/* fixed-point steps per unit of weight in the uint16 weight array of KF_TSDF_F16U16; the
+ * weight saturates at 65535 / 1024 (just under 64, the configurations' max weight) */
+#define KF_WEIGHT_SCALE 1024.0f
 
 typedef enum kf_status {
     KF_OK = 0,

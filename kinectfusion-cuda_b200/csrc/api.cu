@@ -199,6 +199,9 @@ kf_status slot_create(Slot& s, const kf_config& c) {
     KF_ALLOC(raw, uint16_t*, px * 2);
     d.raw = raw;
     KF_ALLOC(d.depth_m, float*, px * 4);
+    d.t16w = (c.width + 15) / 16;
+    d.t16h = (c.height + 15) / 16;
+    KF_ALLOC(d.dmax16, float*, sizeof(float) * size_t(d.t16w) * d.t16h);
     for (int l = 0; l < c.levels; ++l) {
         const size_t np = level_px(c, l);
         KF_ALLOC(d.depth[l], float*, np * 4);
@@ -236,9 +239,14 @@ kf_status slot_create(Slot& s, const kf_config& c) {
     d.step_s = c.step_small;
     d.keep_on_miss = c.keep_on_miss;
     KF_ALLOC(d.pose, PoseDev*, sizeof(PoseDev));
+    d.nb = c.volume_n / 8;
+    const long long nbricks = (long long)d.nb * d.nb * d.nb;
+    KF_ALLOC(d.bmin, float*, sizeof(float) * size_t(nbricks));
+    KF_ALLOC(d.dirty, uint8_t*, size_t(nbricks));
 #undef KF_ALLOC
     // grid {f = 2, w = 0} and pose = initial_pose (project/src/kinect_fusion.cpp:33-36, :80)
     err = launch_init_volume(d.tf, d.tw, (long long)n3, d.fmt, 0);
+    if (err == cudaSuccess) err = launch_init_bricks(d.bmin, d.dirty, nbricks, 0);
     if (err == cudaSuccess) {
         PoseDev P = make_pose_dev(c.initial_pose);
         err = cudaMemcpy(d.pose, &P, sizeof(P), cudaMemcpyHostToDevice);
@@ -257,6 +265,7 @@ kf_status slot_reset(Slot& s) {
     const kf_config& c = s.cfg;
     const size_t n3 = size_t(c.volume_n) * c.volume_n * c.volume_n;
     KF_CK(launch_init_volume(s.d.tf, s.d.tw, (long long)n3, s.d.fmt, 0));
+    KF_CK(launch_init_bricks(s.d.bmin, s.d.dirty, (long long)s.d.nb * s.d.nb * s.d.nb, 0));
     PoseDev P = make_pose_dev(c.initial_pose);
     KF_CK(cudaMemcpy(s.d.pose, &P, sizeof(P), cudaMemcpyHostToDevice));
     KF_CK(cudaDeviceSynchronize());
@@ -295,9 +304,11 @@ struct Engine {
     IcpTile* d_itiles = nullptr;
     IcpRange* d_iranges = nullptr;
     long long* d_fprefix = nullptr;
+    long long* d_bprefix = nullptr;
     float* d_partials = nullptr;
     GridSync* d_sync = nullptr;
     unsigned int* d_ctr = nullptr;
+    static constexpr int kCounters = 8;
     int cap_pre = 0, cap_ray = 0, cap_it = 0, cap_part = 0;
     // pinned host
     StepDev* h_step = nullptr;
@@ -306,7 +317,7 @@ struct Engine {
     Tables tb{};
     bool tables_dirty = true;
     bool step_dirty = true;
-    int grid_pre = 1, grid_ray = 1, grid_icp = 1, grid_fuse = 1;
+    int grid_pre = 1, grid_ray = 1, grid_icp = 1, grid_fuse = 1, grid_brick = 1;
     // graph
     bool use_graph = true;
     bool graph_dirty = true;
@@ -334,8 +345,9 @@ struct Engine {
         KF_CK(cudaMalloc(&d_iranges, sizeof(IcpRange) * KF_MAX_LEVELS * capacity));
         KF_CK(cudaMemset(d_iranges, 0, sizeof(IcpRange) * KF_MAX_LEVELS * capacity));
         KF_CK(cudaMalloc(&d_fprefix, sizeof(long long) * (capacity + 1)));
+        KF_CK(cudaMalloc(&d_bprefix, sizeof(long long) * (capacity + 1)));
         KF_CK(cudaMalloc(&d_sync, sizeof(GridSync)));
-        KF_CK(cudaMalloc(&d_ctr, sizeof(unsigned int) * 4));
+        KF_CK(cudaMalloc(&d_ctr, sizeof(unsigned int) * kCounters));
         KF_CK(cudaMallocHost(&h_step, sizeof(StepDev) * capacity));
         KF_CK(cudaMallocHost(&h_out, sizeof(OutDev) * capacity));
         KF_CK(cudaMallocHost(&h_sync, sizeof(GridSync)));
@@ -346,7 +358,8 @@ struct Engine {
         // persistent grids (kf_batch_autotune may replace the first, second and fourth)
         grid_pre = sms * 4;
         grid_ray = sms * 6;
-        grid_fuse = sms * 8;
+        grid_fuse = sms * 4;
+        grid_brick = sms * 4;
         grid_icp = icp_max_grid(sms);
         return KF_OK;
     }
@@ -374,7 +387,8 @@ struct Engine {
         for (cudaEvent_t& e : ev)
             if (e) cudaEventDestroy(e);
         cudaFree(d_sess); cudaFree(d_step); cudaFree(d_out); cudaFree(d_tb); cudaFree(d_pre); cudaFree(d_ray);
-        cudaFree(d_itiles); cudaFree(d_iranges); cudaFree(d_fprefix); cudaFree(d_partials); cudaFree(d_sync);
+        cudaFree(d_itiles); cudaFree(d_iranges); cudaFree(d_fprefix); cudaFree(d_bprefix); cudaFree(d_partials);
+        cudaFree(d_sync);
         cudaFree(d_ctr);
         cudaFreeHost(h_step); cudaFreeHost(h_out); cudaFreeHost(h_sync);
         if (cap_stream) cudaStreamDestroy(cap_stream);
@@ -383,7 +397,8 @@ struct Engine {
     EngineView view() const {
         EngineView v;
         v.sess = d_sess; v.step = d_step; v.out = d_out; v.tb = d_tb; v.pre = d_pre; v.ray = d_ray;
-        v.itiles = d_itiles; v.iranges = d_iranges; v.fuse_prefix = d_fprefix; v.partials = d_partials;
+        v.itiles = d_itiles; v.iranges = d_iranges; v.fuse_prefix = d_fprefix; v.brick_prefix = d_bprefix;
+        v.partials = d_partials;
         v.sync = d_sync; v.counters = d_ctr;
         return v;
     }
@@ -394,12 +409,13 @@ struct Engine {
         std::vector<RayTile> ray;
         std::vector<IcpTile> it[KF_MAX_LEVELS];
         std::vector<IcpRange> ranges(size_t(KF_MAX_LEVELS) * cap, IcpRange{0, 0});
-        std::vector<long long> fprefix(cap + 1, 0);
+        std::vector<long long> fprefix(cap + 1, 0), bprefix(cap + 1, 0);
         std::vector<SessionDev> sess(cap);
         int max_levels = 1;
         for (int s = 0; s < cap; ++s) {
             const Slot& sl = slots[s];
             fprefix[s + 1] = fprefix[s];
+            bprefix[s + 1] = bprefix[s];
             if (!sl.used) { std::memset(&sess[s], 0, sizeof(SessionDev)); continue; }
             sess[s] = sl.d;
             const kf_config& c = sl.cfg;
@@ -413,13 +429,17 @@ struct Engine {
                         for (int x = 0; x < Lv.cw; x += kRayTileW) ray.push_back(RayTile{s, l, x, y});
                 }
                 fprefix[s + 1] += (long long)c.volume_n * c.volume_n * fuse_segs_per_row(c.volume_n, c.tsdf_format);
+                bprefix[s + 1] += (long long)sl.d.nb * sl.d.nb * sl.d.nb;
             }
             for (int l = 0; l < c.levels; ++l) {
                 const LevelDev& Lv = sl.d.lv[l];
                 const int np = Lv.icw * Lv.ich;
+                // about one tile per ICP block per session-level, at least a block's worth
+                int tile = (np + grid_icp - 1) / grid_icp;
+                tile = std::max(kIcpThreads, (tile + 31) / 32 * 32);
                 IcpRange rg;
                 rg.begin = int(it[l].size());
-                for (int p0 = 0; p0 < np; p0 += kIcpTilePx) it[l].push_back(IcpTile{s, p0, std::min(kIcpTilePx, np - p0)});
+                for (int p0 = 0; p0 < np; p0 += tile) it[l].push_back(IcpTile{s, p0, std::min(tile, np - p0)});
                 rg.end = int(it[l].size());
                 ranges[size_t(l) * cap + s] = rg;
             }
@@ -447,6 +467,7 @@ struct Engine {
         if (!all.empty()) KF_CK(cudaMemcpy(d_itiles, all.data(), sizeof(IcpTile) * all.size(), cudaMemcpyHostToDevice));
         KF_CK(cudaMemcpy(d_iranges, ranges.data(), sizeof(IcpRange) * ranges.size(), cudaMemcpyHostToDevice));
         KF_CK(cudaMemcpy(d_fprefix, fprefix.data(), sizeof(long long) * fprefix.size(), cudaMemcpyHostToDevice));
+        KF_CK(cudaMemcpy(d_bprefix, bprefix.data(), sizeof(long long) * bprefix.size(), cudaMemcpyHostToDevice));
         KF_CK(cudaMemcpy(d_sess, sess.data(), sizeof(SessionDev) * cap, cudaMemcpyHostToDevice));
         tb.S = cap;
         tb.n_pre = int(pre.size());
@@ -457,6 +478,7 @@ struct Engine {
         }
         tb.max_levels = max_levels;
         tb.fuse_total = fprefix[cap];
+        tb.brick_total = bprefix[cap];
         KF_CK(cudaMemcpy(d_tb, &tb, sizeof(Tables), cudaMemcpyHostToDevice));
         tables_dirty = false;
         return KF_OK;
@@ -465,17 +487,18 @@ struct Engine {
     // the per-step sequence
     kf_status record(cudaStream_t st) {
         const EngineView v = view();
-        KF_CK(cudaMemsetAsync(d_ctr, 0, sizeof(unsigned int) * 4, st));
+        KF_CK(cudaMemsetAsync(d_ctr, 0, sizeof(unsigned int) * kCounters, st));
         KF_CK(cudaMemsetAsync(d_sync, 0, sizeof(GridSync), st));
-        if (profile) KF_CK(cudaEventRecord(ev[0], st));
+        if (profile) KF_CK(cudaEventRecordWithFlags(ev[0], st, cudaEventRecordExternal));
         if (stages[0]) KF_CK(launch_preprocess(v, grid_pre, st));
-        if (profile) KF_CK(cudaEventRecord(ev[1], st));
+        if (profile) KF_CK(cudaEventRecordWithFlags(ev[1], st, cudaEventRecordExternal));
         if (stages[1]) KF_CK(launch_raycast(v, grid_ray, st));
-        if (profile) KF_CK(cudaEventRecord(ev[2], st));
+        if (profile) KF_CK(cudaEventRecordWithFlags(ev[2], st, cudaEventRecordExternal));
         if (stages[2]) KF_CK(launch_icp(v, grid_icp, st));
-        if (profile) KF_CK(cudaEventRecord(ev[3], st));
+        if (profile) KF_CK(cudaEventRecordWithFlags(ev[3], st, cudaEventRecordExternal));
         if (stages[3]) KF_CK(launch_fuse(v, grid_fuse, st));
-        if (profile) KF_CK(cudaEventRecord(ev[4], st));
+        if (stages[3]) KF_CK(launch_bricks(v, grid_brick, st));
+        if (profile) KF_CK(cudaEventRecordWithFlags(ev[4], st, cudaEventRecordExternal));
         KF_CK(cudaMemcpyAsync(h_out, d_out, sizeof(OutDev) * cap, cudaMemcpyDeviceToHost, st));
         KF_CK(cudaMemcpyAsync(h_sync, d_sync, sizeof(GridSync), cudaMemcpyDeviceToHost, st));
         return KF_OK;
@@ -873,21 +896,25 @@ kf_status kf_set_tsdf(kf_session* s, const void* src, size_t src_bytes, int layo
         if (src_bytes < 2 * n3 * es) return KF_ERR_SHAPE;
         KF_CK(cudaMemcpy(sl.d.tf, src, n3 * es, kind));
         KF_CK(cudaMemcpy(sl.d.tw, static_cast<const char*>(src) + n3 * es, n3 * es, kind));
-        return KF_OK;
+    } else {
+        if (layout != 1) return KF_ERR_ARG;
+        if (src_bytes < n3 * 8) return KF_ERR_SHAPE;
+        float* tmp = nullptr;
+        const float* from = static_cast<const float*>(src);
+        if (from_host) {
+            KF_CK(cudaMalloc(&tmp, n3 * 8));
+            KF_CK(cudaMemcpy(tmp, src, n3 * 8, cudaMemcpyHostToDevice));
+            from = tmp;
+        }
+        cudaError_t e = launch_import_interleaved(from, sl.d.tf, sl.d.tw, (long long)n3, sl.d.fmt, 0);
+        if (e == cudaSuccess) e = cudaDeviceSynchronize();
+        if (tmp) cudaFree(tmp);
+        KF_CK(e);
     }
-    if (layout != 1) return KF_ERR_ARG;
-    if (src_bytes < n3 * 8) return KF_ERR_SHAPE;
-    float* tmp = nullptr;
-    const float* from = static_cast<const float*>(src);
-    if (from_host) {
-        KF_CK(cudaMalloc(&tmp, n3 * 8));
-        KF_CK(cudaMemcpy(tmp, src, n3 * 8, cudaMemcpyHostToDevice));
-        from = tmp;
-    }
-    cudaError_t e = launch_import_interleaved(from, sl.d.tf, sl.d.tw, (long long)n3, sl.d.fmt, 0);
-    if (e == cudaSuccess) e = cudaDeviceSynchronize();
-    if (tmp) cudaFree(tmp);
-    KF_CK(e);
+    // the raycaster's brick minima follow the new volume
+    KF_CK(launch_rebuild_bricks(sl.d.tf, sl.d.fmt, sl.cfg.volume_n, sl.d.bmin, 0));
+    KF_CK(cudaMemset(sl.d.dirty, 0, size_t(sl.d.nb) * sl.d.nb * sl.d.nb));
+    KF_CK(cudaDeviceSynchronize());
     return KF_OK;
 }
 
@@ -1309,6 +1336,8 @@ kf_status kf_batch_autotune(kf_batch* b, void* stream, char* report, size_t repo
         cudaMemcpy(sl.d.tw, static_cast<char*>(saved[i]) + sizes[i], sizes[i], cudaMemcpyDeviceToDevice);
         cudaMemcpy(sl.d.pose, static_cast<char*>(saved[i]) + 2 * sizes[i], sizeof(PoseDev), cudaMemcpyDeviceToDevice);
         cudaFree(saved[i]);
+        launch_rebuild_bricks(sl.d.tf, sl.d.fmt, sl.cfg.volume_n, sl.d.bmin, 0);
+        cudaMemset(sl.d.dirty, 0, size_t(sl.d.nb) * sl.d.nb * sl.d.nb);
     }
     KF_CK(cudaDeviceSynchronize());
     e.graph_dirty = true;

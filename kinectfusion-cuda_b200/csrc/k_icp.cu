@@ -216,20 +216,26 @@ __device__ void icp_begin(const SessionDev* S, const StepDev st) {
 
 // phase B for one session: FP64 combine of the tile pairs, solve, update, stop test
 // (ICP::computePose loop body, project/src/icp.cpp:36-54).  All threads of the block call it.
-__device__ void icp_solve(const EngineView& v, int s, double* sm) {
+__device__ void icp_solve(const EngineView& v, int s, double* sm, float* stage, int stage_tiles) {
     const SessionDev* S = &v.sess[s];
     PoseDev* P = S->pose;
     const int tid = threadIdx.x;
     const int level = ldcg(&P->level);
     const IcpRange rg = v.iranges[level * v.tb->S + s];
+    const int cnt = rg.end - rg.begin;
+    // bring the session's tile pairs on chip with every thread's loads in flight at once
+    const float* src = v.partials + size_t(rg.begin) * 54;
+    if (cnt <= stage_tiles) {
+#pragma unroll 4
+        for (int i = tid; i < cnt * 54; i += blockDim.x) stage[i] = ldcg(src + i);
+        __syncthreads();
+        src = stage;
+    }
     // 8 groups x 27 entries: each group adds every 8th tile in FP64
     if (tid < 8 * 27) {
         const int k = tid % 27, g = tid / 27;
         double acc = 0.0;
-        for (int t = rg.begin + g; t < rg.end; t += 8) {
-            const float* p = v.partials + size_t(t) * 54;
-            acc += double(ldcg(p + 2 * k)) + double(ldcg(p + 2 * k + 1));
-        }
+        for (int t = g; t < cnt; t += 8) acc += double(src[size_t(t) * 54 + 2 * k]) + double(src[size_t(t) * 54 + 2 * k + 1]);
         sm[g * 27 + k] = acc;
     }
     __syncthreads();
@@ -325,7 +331,8 @@ __device__ void icp_finish(const SessionDev* S, const StepDev st, OutDev* out) {
 
 constexpr int kIcpMaxSessionsSmem = 1024;
 
-__global__ void __launch_bounds__(kIcpThreads) icp_kernel(EngineView v) {
+__global__ void __launch_bounds__(kIcpThreads) icp_kernel(EngineView v, int stage_tiles) {
+    extern __shared__ float stage[];   // stage_tiles * 54 floats: one session's tile pairs
     __shared__ float red[8 * 32 * 2];
     __shared__ double dsm[8 * 27];
     __shared__ float mats[24];
@@ -393,9 +400,7 @@ __global__ void __launch_bounds__(kIcpThreads) icp_kernel(EngineView v) {
             for (int q = 0; q < 32; ++q) acc[q] = 0.f;
             const float dist = S->dist_th, ang = S->angle_th;
 #pragma unroll 1
-            for (int k = 0; k < kIcpPxPerThread; ++k) {
-                const int p = T.p0 + tid + k * kIcpThreads;
-                if (p >= T.p0 + T.np) break;
+            for (int p = T.p0 + tid; p < T.p0 + T.np; p += kIcpThreads) {
                 const int u = p % Lv.icw, vv = p / Lv.icw;
                 float a[6], b;
                 const bool ok = icp_pixel(vm, tv, tn, Lv.w, Lv.h, u, vv, mats, mats + 9, mats + 12, mats + 21, dist,
@@ -409,7 +414,7 @@ __global__ void __launch_bounds__(kIcpThreads) icp_kernel(EngineView v) {
 
         // phase B
         for (int s = blockIdx.x; s < S_cap; s += gridDim.x)
-            if (s_lvl[s] >= 0) icp_solve(v, s, dsm);
+            if (s_lvl[s] >= 0) icp_solve(v, s, dsm, stage, stage_tiles);
         if (!grid_barrier(v.sync, nb, epoch)) return;
     }
 
@@ -436,8 +441,11 @@ cudaError_t launch_barrier_selftest(GridSync* g, unsigned long long timeout_ns, 
 }
 
 cudaError_t launch_icp(const EngineView& v, int grid, cudaStream_t st) {
-    void* args[] = {const_cast<EngineView*>(&v)};
-    return cudaLaunchCooperativeKernel((const void*)icp_kernel, dim3(grid), dim3(kIcpThreads), args, 0, st);
+    // tiles per session-level are at most about one per block (see the tile table)
+    int stage_tiles = grid + 8 < 160 ? grid + 8 : 160;   // <= 34.6 KB, under the 48 KB default
+    const size_t smem = sizeof(float) * 54 * size_t(stage_tiles);
+    void* args[] = {const_cast<EngineView*>(&v), &stage_tiles};
+    return cudaLaunchCooperativeKernel((const void*)icp_kernel, dim3(grid), dim3(kIcpThreads), args, smem, st);
 }
 
 // ---- stage: kernel::constructIcpResiduals (A rows and b to HBM, as the reference) ----

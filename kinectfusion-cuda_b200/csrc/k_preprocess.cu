@@ -60,6 +60,7 @@ __device__ __forceinline__ float4 vertex_core(float d, int i, int j, const float
 
 __global__ void __launch_bounds__(256) preprocess_kernel(EngineView v) {
     extern __shared__ float smem[];
+    __shared__ unsigned int qmax[4];   // largest valid depth of each 16x16 quadrant (float bits)
     const int tid = threadIdx.x;
     const int ntiles = v.tb->n_pre;
     for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
@@ -75,7 +76,10 @@ __global__ void __launch_bounds__(256) preprocess_kernel(EngineView v) {
         const uint16_t* raw = S->raw;
 
         // 1. convert the tile and its clamp-to-edge halo (convertToDepthMetersKernel); the
-        //    interior is also the unfiltered metres map fusion reads
+        //    interior is also the unfiltered metres map fusion reads, and its per-16x16
+        //    largest valid depth lets fusion skip row segments that cannot update
+        if (tid < 4) qmax[tid] = 0u;
+        __syncthreads();
         for (int idx = tid; idx < pitch * pitch; idx += blockDim.x) {
             const int rx = idx % pitch, ry = idx / pitch;
             const int gx = min(max(T.x0 - R + rx, 0), W - 1);
@@ -84,10 +88,16 @@ __global__ void __launch_bounds__(256) preprocess_kernel(EngineView v) {
             const float d = raw_to_half_value(__ldg(raw + size_t(gy) * W + src)) * scale;
             reg[idx] = d;
             const int ix = T.x0 - R + rx, iy = T.y0 - R + ry;
-            if (rx >= R && rx < R + kPreTileSize && ry >= R && ry < R + kPreTileSize && ix < W && iy < H)
+            if (rx >= R && rx < R + kPreTileSize && ry >= R && ry < R + kPreTileSize && ix < W && iy < H) {
                 S->depth_m[size_t(iy) * W + ix] = d;
+                if (depth_valid(d)) atomicMax(&qmax[((ry - R) >> 4) * 2 + ((rx - R) >> 4)], __float_as_uint(d));
+            }
         }
         __syncthreads();
+        if (tid < 4) {
+            const int tx = (T.x0 >> 4) + (tid & 1), ty = (T.y0 >> 4) + (tid >> 1);
+            if (tx < S->t16w && ty < S->t16h) S->dmax16[size_t(ty) * S->t16w + tx] = __uint_as_float(qmax[tid]);
+        }
 
         // 2. bilateral filter + level-0 vertex map
         const LevelDev& L0 = S->lv[0];

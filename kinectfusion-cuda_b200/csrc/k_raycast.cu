@@ -56,25 +56,72 @@ __device__ __forceinline__ void march_ray(const SessionDev* __restrict__ S, cons
     // texel coordinate of world point p: (p / width + 0.5) * n - 0.5
     const float sc = float(n) / width, off = 0.5f * float(n) - 0.5f;
     const float large = mu * S->step_l, small = mu * S->step_s;
+    const float* __restrict__ bmin = S->bmin;
+    const int nb = S->nb;
+    // the ray in texel space, for brick exits: x(t) = tox + tdx t
+    const float tox = o.x * sc + off, toy = o.y * sc + off, toz = o.z * sc + off;
+    const float tdx = dir.x * sc, tdy = dir.y * sc, tdz = dir.z * sc;
     float inc = large, prev = 0.f, precise = 0.f;
-    int guard = 0;   // hard bound on samples per ray, whatever the configuration
-    for (float t = near_d; t < far_d && guard < kMaxMarchSamples; t += inc, ++guard) {
-        const float px = o.x + dir.x * t, py = o.y + dir.y * t, pz = o.z + dir.z * t;
-        const float tsdf = trilinear(f, n, px * sc + off, py * sc + off, pz * sc + off);
+    float prev_t = 0.f;       // position of the last non-negative sample
+    bool prev_known = true;   // false when that sample was skipped (its value not computed)
+    int guard = 0;            // hard bound on samples per ray, whatever the configuration
+    float t = near_d;
+    while (t < far_d && guard < kMaxMarchSamples) {
+        const float x = (o.x + dir.x * t) * sc + off;
+        const float y = (o.y + dir.y * t) * sc + off;
+        const float z = (o.z + dir.z * t) * sc + off;
+        if (bmin) {
+            // A brick whose minimum is >= 0.991 (large steps) or >= 0.001 (small steps) holds
+            // no sample that changes the march: the value stays >= 0.99 resp. >= 0, so the
+            // reference would only step on.  Skip this sample and every later one inside the
+            // brick (0.01 texel inside its faces), advancing t exactly as the reference does.
+            const int ix = min(max(int(floorf(x)), 0), n - 1) >> 3;
+            const int iy = min(max(int(floorf(y)), 0), n - 1) >> 3;
+            const int iz = min(max(int(floorf(z)), 0), n - 1) >> 3;
+            const float m = __ldg(bmin + (size_t(iz) * nb + iy) * nb + ix);
+            if (m >= (inc == large ? 0.991f : 0.001f)) {
+                float t_safe = far_d;
+                if (tdx > 0.f && ix < nb - 1) t_safe = fminf(t_safe, (float(8 * ix + 8) - 0.01f - tox) / tdx);
+                if (tdx < 0.f && ix > 0) t_safe = fminf(t_safe, (float(8 * ix) + 0.01f - tox) / tdx);
+                if (tdy > 0.f && iy < nb - 1) t_safe = fminf(t_safe, (float(8 * iy + 8) - 0.01f - toy) / tdy);
+                if (tdy < 0.f && iy > 0) t_safe = fminf(t_safe, (float(8 * iy) + 0.01f - toy) / tdy);
+                if (tdz > 0.f && iz < nb - 1) t_safe = fminf(t_safe, (float(8 * iz + 8) - 0.01f - toz) / tdz);
+                if (tdz < 0.f && iz > 0) t_safe = fminf(t_safe, (float(8 * iz) + 0.01f - toz) / tdz);
+                do {
+                    prev_t = t;
+                    t += inc;
+                    ++guard;
+                } while (t < t_safe && t < far_d && guard < kMaxMarchSamples);
+                prev_known = false;
+                continue;
+            }
+        }
+        const float tsdf = trilinear(f, n, x, y, z);
+        ++guard;
         if (tsdf < 0.0f) {
             if (t != near_d) {
                 if (inc == large) {   // went through the surface with a large step: back off
                     t -= mu;
                     inc = small;
+                    t += inc;
                     continue;
                 }
-                precise = t - inc * prev / (tsdf - prev);   // linear zero crossing
+                if (!prev_known) {
+                    const float ax = (o.x + dir.x * prev_t) * sc + off;
+                    const float ay = (o.y + dir.y * prev_t) * sc + off;
+                    const float az = (o.z + dir.z * prev_t) * sc + off;
+                    prev = trilinear(f, n, ax, ay, az);
+                }
+                precise = t - inc * prev / (tsdf - prev);   // the reference's zero-crossing formula
             }
             break;
         } else if (tsdf < 0.99f) {
             inc = small;
         }
         prev = tsdf;
+        prev_known = true;
+        prev_t = t;
+        t += inc;
     }
     if (precise != 0.0f) {
         const F3 vtx{o.x + dir.x * precise, o.y + dir.y * precise, o.z + dir.z * precise};

@@ -53,6 +53,8 @@ struct SessionDev {
     // maps
     const uint16_t* raw;   // input frame (w*h uint16)
     float* depth_m;        // unfiltered metres (fusion input)
+    float* dmax16;         // per 16x16-pixel tile of depth_m: largest valid depth (0: none)
+    int t16w, t16h;        // tiles per row / column
     float* depth[kMaxLevels];
     float4* vmap[kMaxLevels];
     float4* pv[kMaxLevels];   // predicted (raycast) vertices, world frame
@@ -65,6 +67,12 @@ struct SessionDev {
     void* tw;              // weight array (float or uint16)
     const float* xs;       // voxel-centre x (= y) coordinates, n floats
     const float* zs;       // voxel-centre z coordinates accumulated as the reference does
+    // 8^3-voxel bricks: minimum distance over the brick and its one-voxel apron, kept
+    // current after every fusion so the raycaster can skip samples that cannot change its
+    // decisions; `dirty` marks bricks fusion touched
+    float* bmin;
+    uint8_t* dirty;
+    int nb;                // bricks per axis (n / 8)
     float min_d, max_d, step_l, step_s;
     int keep_on_miss;
     // ICP

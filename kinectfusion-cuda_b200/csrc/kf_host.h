@@ -19,6 +19,7 @@ struct Tables {
     int max_levels;
     int pad;
     long long fuse_total;    // fusion segments over all slots
+    long long brick_total;   // bricks over all slots
 };
 
 // raw pointers the kernels take
@@ -32,9 +33,11 @@ struct EngineView {
     const IcpTile* itiles;
     const IcpRange* iranges;     // [level * S + s]
     const long long* fuse_prefix;// S + 1 entries, in segments
+    const long long* brick_prefix;// S + 1 entries, in bricks
     float* partials;             // ICP block partials, 54 floats per tile
     GridSync* sync;
-    unsigned int* counters;      // [0] raycast tiles, [1..] fusion segments (64-bit at [2])
+    unsigned int* counters;      // [0] raycast tiles, [2..3] fusion segments (64-bit),
+                                 // [4..5] brick groups (64-bit)
 };
 
 constexpr int kPreTileSize = 32;
@@ -49,6 +52,11 @@ cudaError_t launch_preprocess(const EngineView& v, int grid, cudaStream_t st);
 cudaError_t launch_raycast(const EngineView& v, int grid, cudaStream_t st);
 cudaError_t launch_icp(const EngineView& v, int grid, cudaStream_t st);
 cudaError_t launch_fuse(const EngineView& v, int grid, cudaStream_t st);
+// refresh the minimum of every brick fusion marked dirty
+cudaError_t launch_bricks(const EngineView& v, int grid, cudaStream_t st);
+// bmin = 2 (the initial distance), dirty = 0; or, with rebuild, every brick recomputed from f
+cudaError_t launch_init_bricks(float* bmin, uint8_t* dirty, long long nbricks, cudaStream_t st);
+cudaError_t launch_rebuild_bricks(const void* f, int fmt, int n, float* bmin, cudaStream_t st);
 int icp_max_grid(int num_sms);
 cudaError_t launch_barrier_selftest(GridSync* g, unsigned long long timeout_ns, int* result, cudaStream_t st);
 int fuse_segs_per_row(int n, int fmt);

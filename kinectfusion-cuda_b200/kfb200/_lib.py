@@ -11,7 +11,7 @@ LIB_DIR = os.path.join(os.path.dirname(_HERE), "lib")
 LIB_PATH = os.path.join(LIB_DIR, "libkfb200.so")
 
 KF_MAX_LEVELS = 3
-KF_WEIGHT_SCALE = 128.0
+KF_WEIGHT_SCALE = 1024.0
 
 KF_OK = 0
 KF_ERR_ARG = 1

@@ -1,6 +1,12 @@
 """End-to-end parity of the per-frame pipeline (kf_session, graph-replayed) against the CPU
 oracle's restatement of KinectFusion::startTracking on the same seeded synthetic frames.
 
+Per frame, the oracle starts from the device's state (TSDF and pose before the frame) and
+both process the same frame; that isolates each frame's arithmetic from the way the
+reference's algorithm amplifies tiny differences over a sequence (hard ICP rejections and a
+1 cm early stop: the reference algorithm's own float and FP64 restatements differ by ~1e-4
+after one frame on these scenes).  Free-running sequences are compared with a drift bound.
+
 Bounds: per-frame pose within 1e-4 rad (rotation chord) / 1e-4 m of the FP64 oracle; depth
 pyramid and valid-pixel masks equal, values within 2e-6 relative; ICP correspondence masks
 agreeing on >= 99.9% of pixels; TSDF within 1e-3 of the truncation distance on >= 99.9% of
@@ -16,6 +22,16 @@ pytestmark = pytest.mark.gpu
 NFRAMES = 10
 
 
+def synced_frame(s, P, img):
+    """Run one frame on the device and on the oracle from the device's state."""
+    f, w = s.tsdf()
+    P.set_tsdf(f, w)
+    P.set_pose(s.pose())
+    st_o, pose_o = P.process_frame(img)
+    st_g, pose_g = s.process_frame(img)
+    return st_g, st_o, pose_g, pose_o
+
+
 @pytest.fixture(scope="module")
 def run_small(kf, orc, cuda):
     from kfb200 import synth
@@ -25,8 +41,7 @@ def run_small(kf, orc, cuda):
     P = orc.Pipeline(cfg, prec=1)
     rows = []
     for i, img in enumerate(imgs):
-        st_g, pose_g = s.process_frame(img)
-        st_o, pose_o = P.process_frame(img)
+        st_g, st_o, pose_g, pose_o = synced_frame(s, P, img)
         rows.append((st_g, st_o, pose_g, pose_o, s.frame_stats()["icp_iters"], P.iters()))
     return cfg, imgs, s, P, rows
 
@@ -37,6 +52,23 @@ def test_pose_per_frame(kf, run_small):
         assert st_g == st_o == kf.KF_OK, i
         a, d = kf.poseError(po, pg)
         assert a <= 1e-4 and d <= 1e-4, (i, a, d, ig, io)
+
+
+def test_free_running_drift(kf, orc):
+    """Without re-synchronisation both runs follow the reference's algorithm; they may take
+    a different number of ICP iterations where a step sits near the 1 cm stop threshold."""
+    from kfb200 import synth
+    cfg = kf.config_small()
+    imgs, _ = synth.sequence(cfg, NFRAMES, seed=33)
+    s = kf.KinectFusion(cfg)
+    P = orc.Pipeline(cfg, prec=0)
+    worst = 0.0
+    for img in imgs:
+        _, pg = s.process_frame(img)
+        _, po = P.process_frame(img)
+        worst = max(worst, *kf.poseError(po, pg))
+    assert worst <= 3e-3, worst
+    s.close()
 
 
 def test_first_frame_fuses_only(kf, run_small):
@@ -66,7 +98,7 @@ def test_icp_masks(kf, run_small):
 
 def test_raycast_maps(kf, run_small):
     cfg, imgs, s, P, rows = run_small
-    cam = rows[-2][3][:3, 3]   # the raycast of the last frame ran at the previous pose
+    cam = rows[-2][2][:3, 3]   # the raycast of the last frame ran at the previous pose
     for level in range(3):
         gv, gn = s.raycast_maps(level)
         ov, on = P.raycast_maps(level)
@@ -138,8 +170,7 @@ def test_trunc8_compat_mode(kf, orc):
     s = kf.KinectFusion(cfg)
     P = orc.Pipeline(cfg, prec=1)
     for img in imgs:
-        _, pg = s.process_frame(img)
-        _, po = P.process_frame(img)
+        _, _, pg, po = synced_frame(s, P, img)
         a, d = kf.poseError(po, pg)
         assert a <= 1e-4 and d <= 1e-4
     # level 2 of 320x240 is 80x60: the reference's 8x8 grid never writes rows 56-59
@@ -148,25 +179,25 @@ def test_trunc8_compat_mode(kf, orc):
 
 
 def test_f16u16_precision_form_vs_fp64(kf, orc):
-    """FP16 distance + uint16 weight volume against the FP64 oracle (float volume): reported
-    error bounds for pose, TSDF (in truncation units) and raycast depth."""
+    """FP16 distance + uint16 weight volume against the FP64 oracle (float volume): per frame
+    from the device's state, pose within 1e-4 and the frame's fused TSDF within fp16 / weight
+    quantisation (RMS below 1e-3 of the truncation distance)."""
     from kfb200 import synth
     cfg16 = kf.config_small(tsdf_format=kf.KF_TSDF_F16U16)
     cfg = kf.config_small()
     imgs, _ = synth.sequence(cfg, 8, seed=37)
     s = kf.KinectFusion(cfg16)
     P = orc.Pipeline(cfg, prec=1)
-    worst = 0.0
     for img in imgs:
-        _, pg = s.process_frame(img)
-        _, po = P.process_frame(img)
-        worst = max(worst, *kf.poseError(po, pg))
-    assert worst <= 5e-4
+        _, _, pg, po = synced_frame(s, P, img)
+        a, d = kf.poseError(po, pg)
+        assert a <= 1e-4 and d <= 1e-4
     gf, gw = s.tsdf()
     of, ow = P.tsdf()
     obs = (ow > 0) & (gw > 0)
+    assert np.mean((ow > 0) == (gw > 0)) >= 0.999
     rms = np.sqrt(np.mean((gf[obs] - of[obs]) ** 2))
-    assert rms < 5e-3
+    assert rms < 1e-3
     s.close()
 
 
@@ -177,8 +208,7 @@ def test_bilateral_radius_zero_and_single_level(kf, orc):
     s = kf.KinectFusion(cfg)
     P = orc.Pipeline(cfg, prec=1)
     for img in imgs:
-        _, pg = s.process_frame(img)
-        _, po = P.process_frame(img)
+        _, _, pg, po = synced_frame(s, P, img)
         a, d = kf.poseError(po, pg)
         assert a <= 1e-4 and d <= 1e-4
     np.testing.assert_allclose(s.depth(0), s.depth(-1), rtol=0)   # a 1x1 window is the identity
