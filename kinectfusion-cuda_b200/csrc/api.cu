@@ -55,7 +55,8 @@ kf_status validate(const kf_config& c) {
     if (c.tsdf_format != KF_TSDF_F32F32 && c.tsdf_format != KF_TSDF_F16U16) return KF_ERR_ARG;
     if (c.bilateral_radius < 0 || c.bilateral_radius > kMaxBilateralRadius) return KF_ERR_ARG;
     if (!(c.bilateral_sigma_s > 0.f) || !(c.bilateral_sigma_r > 0.f)) return KF_ERR_ARG;
-    if (!(c.step_large > 0.f) || !(c.step_small > 0.f)) return KF_ERR_ARG;
+    // large steps must exceed small ones (the reference tells the two phases apart by them)
+    if (!(c.step_small > 0.f) || !(c.step_large > c.step_small)) return KF_ERR_ARG;
     // a march step must still advance t in float at the far end of the range
     if (!(c.min_depth >= 0.f) || !(c.max_depth > c.min_depth) || !(c.max_depth < 1000.f)) return KF_ERR_ARG;
     if (!(c.mu * c.step_small > c.max_depth * 1e-6f)) return KF_ERR_ARG;
@@ -240,13 +241,15 @@ kf_status slot_create(Slot& s, const kf_config& c) {
     d.keep_on_miss = c.keep_on_miss;
     KF_ALLOC(d.pose, PoseDev*, sizeof(PoseDev));
     d.nb = c.volume_n / 8;
+    d.ns = (d.nb + 3) / 4;
     const long long nbricks = (long long)d.nb * d.nb * d.nb;
-    KF_ALLOC(d.bmin, float*, sizeof(float) * size_t(nbricks));
-    KF_ALLOC(d.dirty, uint8_t*, size_t(nbricks));
+    KF_ALLOC(d.bmin, int*, sizeof(int) * size_t(nbricks));
+    KF_ALLOC(d.bdil, int*, sizeof(int) * size_t(nbricks));
+    KF_ALLOC(d.sdil, int*, sizeof(int) * size_t(d.ns) * d.ns * d.ns);
 #undef KF_ALLOC
     // grid {f = 2, w = 0} and pose = initial_pose (project/src/kinect_fusion.cpp:33-36, :80)
     err = launch_init_volume(d.tf, d.tw, (long long)n3, d.fmt, 0);
-    if (err == cudaSuccess) err = launch_init_bricks(d.bmin, d.dirty, nbricks, 0);
+    if (err == cudaSuccess) err = launch_init_bricks(d.bmin, d.bdil, d.sdil, c.volume_n, 0);
     if (err == cudaSuccess) {
         PoseDev P = make_pose_dev(c.initial_pose);
         err = cudaMemcpy(d.pose, &P, sizeof(P), cudaMemcpyHostToDevice);
@@ -265,7 +268,7 @@ kf_status slot_reset(Slot& s) {
     const kf_config& c = s.cfg;
     const size_t n3 = size_t(c.volume_n) * c.volume_n * c.volume_n;
     KF_CK(launch_init_volume(s.d.tf, s.d.tw, (long long)n3, s.d.fmt, 0));
-    KF_CK(launch_init_bricks(s.d.bmin, s.d.dirty, (long long)s.d.nb * s.d.nb * s.d.nb, 0));
+    KF_CK(launch_init_bricks(s.d.bmin, s.d.bdil, s.d.sdil, c.volume_n, 0));
     PoseDev P = make_pose_dev(c.initial_pose);
     KF_CK(cudaMemcpy(s.d.pose, &P, sizeof(P), cudaMemcpyHostToDevice));
     KF_CK(cudaDeviceSynchronize());
@@ -305,11 +308,15 @@ struct Engine {
     IcpRange* d_iranges = nullptr;
     long long* d_fprefix = nullptr;
     long long* d_bprefix = nullptr;
+    long long* d_sprefix = nullptr;
     float* d_partials = nullptr;
     GridSync* d_sync = nullptr;
     unsigned int* d_ctr = nullptr;
     static constexpr int kCounters = 8;
     int cap_pre = 0, cap_ray = 0, cap_it = 0, cap_part = 0;
+    // long-ray queue of the raycaster (bytes; entries = bytes / long_ray_bytes())
+    char* d_longq = nullptr;
+    int cap_longq = 0;
     // pinned host
     StepDev* h_step = nullptr;
     OutDev* h_out = nullptr;
@@ -346,6 +353,7 @@ struct Engine {
         KF_CK(cudaMemset(d_iranges, 0, sizeof(IcpRange) * KF_MAX_LEVELS * capacity));
         KF_CK(cudaMalloc(&d_fprefix, sizeof(long long) * (capacity + 1)));
         KF_CK(cudaMalloc(&d_bprefix, sizeof(long long) * (capacity + 1)));
+        KF_CK(cudaMalloc(&d_sprefix, sizeof(long long) * (capacity + 1)));
         KF_CK(cudaMalloc(&d_sync, sizeof(GridSync)));
         KF_CK(cudaMalloc(&d_ctr, sizeof(unsigned int) * kCounters));
         KF_CK(cudaMallocHost(&h_step, sizeof(StepDev) * capacity));
@@ -387,7 +395,9 @@ struct Engine {
         for (cudaEvent_t& e : ev)
             if (e) cudaEventDestroy(e);
         cudaFree(d_sess); cudaFree(d_step); cudaFree(d_out); cudaFree(d_tb); cudaFree(d_pre); cudaFree(d_ray);
-        cudaFree(d_itiles); cudaFree(d_iranges); cudaFree(d_fprefix); cudaFree(d_bprefix); cudaFree(d_partials);
+        cudaFree(d_itiles); cudaFree(d_iranges); cudaFree(d_fprefix); cudaFree(d_bprefix); cudaFree(d_sprefix);
+        cudaFree(d_partials);
+        cudaFree(d_longq);
         cudaFree(d_sync);
         cudaFree(d_ctr);
         cudaFreeHost(h_step); cudaFreeHost(h_out); cudaFreeHost(h_sync);
@@ -398,8 +408,11 @@ struct Engine {
         EngineView v;
         v.sess = d_sess; v.step = d_step; v.out = d_out; v.tb = d_tb; v.pre = d_pre; v.ray = d_ray;
         v.itiles = d_itiles; v.iranges = d_iranges; v.fuse_prefix = d_fprefix; v.brick_prefix = d_bprefix;
+        v.super_prefix = d_sprefix;
         v.partials = d_partials;
         v.sync = d_sync; v.counters = d_ctr;
+        v.longq = reinterpret_cast<LongRay*>(d_longq);
+        v.longq_cap = cap_longq / long_ray_bytes();
         return v;
     }
 
@@ -409,13 +422,14 @@ struct Engine {
         std::vector<RayTile> ray;
         std::vector<IcpTile> it[KF_MAX_LEVELS];
         std::vector<IcpRange> ranges(size_t(KF_MAX_LEVELS) * cap, IcpRange{0, 0});
-        std::vector<long long> fprefix(cap + 1, 0), bprefix(cap + 1, 0);
+        std::vector<long long> fprefix(cap + 1, 0), bprefix(cap + 1, 0), sprefix(cap + 1, 0);
         std::vector<SessionDev> sess(cap);
         int max_levels = 1;
         for (int s = 0; s < cap; ++s) {
             const Slot& sl = slots[s];
             fprefix[s + 1] = fprefix[s];
             bprefix[s + 1] = bprefix[s];
+            sprefix[s + 1] = sprefix[s];
             if (!sl.used) { std::memset(&sess[s], 0, sizeof(SessionDev)); continue; }
             sess[s] = sl.d;
             const kf_config& c = sl.cfg;
@@ -428,8 +442,9 @@ struct Engine {
                     for (int y = 0; y < Lv.ch; y += kRayTileH)
                         for (int x = 0; x < Lv.cw; x += kRayTileW) ray.push_back(RayTile{s, l, x, y});
                 }
-                fprefix[s + 1] += (long long)c.volume_n * c.volume_n * fuse_segs_per_row(c.volume_n, c.tsdf_format);
+                fprefix[s + 1] += fuse_units(c.volume_n);
                 bprefix[s + 1] += (long long)sl.d.nb * sl.d.nb * sl.d.nb;
+                sprefix[s + 1] += (long long)sl.d.ns * sl.d.ns * sl.d.ns;
             }
             for (int l = 0; l < c.levels; ++l) {
                 const LevelDev& Lv = sl.d.lv[l];
@@ -456,18 +471,22 @@ struct Engine {
                 rg.end += off[l];
             }
         }
-        const int old_pre = cap_pre, old_ray = cap_ray, old_it = cap_it, old_part = cap_part;
+        const int old_pre = cap_pre, old_ray = cap_ray, old_it = cap_it, old_part = cap_part, old_lq = cap_longq;
         KF_TRY(grow(d_pre, cap_pre, std::max<int>(1, int(pre.size()))));
         KF_TRY(grow(d_ray, cap_ray, std::max<int>(1, int(ray.size()))));
         KF_TRY(grow(d_itiles, cap_it, std::max<int>(1, int(all.size()))));
         KF_TRY(grow(d_partials, cap_part, std::max<int>(1, int(all.size())) * 54));
-        if (old_pre != cap_pre || old_ray != cap_ray || old_it != cap_it || old_part != cap_part) graph_dirty = true;
+        // room for a quarter of all rays to take the long-ray path (more fall back to the lane)
+        KF_TRY(grow(d_longq, cap_longq, std::max<int>(1024, int(ray.size()) * 32 / 4) * long_ray_bytes()));
+        if (old_pre != cap_pre || old_ray != cap_ray || old_it != cap_it || old_part != cap_part || old_lq != cap_longq)
+            graph_dirty = true;
         if (!pre.empty()) KF_CK(cudaMemcpy(d_pre, pre.data(), sizeof(PreTile) * pre.size(), cudaMemcpyHostToDevice));
         if (!ray.empty()) KF_CK(cudaMemcpy(d_ray, ray.data(), sizeof(RayTile) * ray.size(), cudaMemcpyHostToDevice));
         if (!all.empty()) KF_CK(cudaMemcpy(d_itiles, all.data(), sizeof(IcpTile) * all.size(), cudaMemcpyHostToDevice));
         KF_CK(cudaMemcpy(d_iranges, ranges.data(), sizeof(IcpRange) * ranges.size(), cudaMemcpyHostToDevice));
         KF_CK(cudaMemcpy(d_fprefix, fprefix.data(), sizeof(long long) * fprefix.size(), cudaMemcpyHostToDevice));
         KF_CK(cudaMemcpy(d_bprefix, bprefix.data(), sizeof(long long) * bprefix.size(), cudaMemcpyHostToDevice));
+        KF_CK(cudaMemcpy(d_sprefix, sprefix.data(), sizeof(long long) * sprefix.size(), cudaMemcpyHostToDevice));
         KF_CK(cudaMemcpy(d_sess, sess.data(), sizeof(SessionDev) * cap, cudaMemcpyHostToDevice));
         tb.S = cap;
         tb.n_pre = int(pre.size());
@@ -479,6 +498,7 @@ struct Engine {
         tb.max_levels = max_levels;
         tb.fuse_total = fprefix[cap];
         tb.brick_total = bprefix[cap];
+        tb.super_total = sprefix[cap];
         KF_CK(cudaMemcpy(d_tb, &tb, sizeof(Tables), cudaMemcpyHostToDevice));
         tables_dirty = false;
         return KF_OK;
@@ -912,8 +932,7 @@ kf_status kf_set_tsdf(kf_session* s, const void* src, size_t src_bytes, int layo
         KF_CK(e);
     }
     // the raycaster's brick minima follow the new volume
-    KF_CK(launch_rebuild_bricks(sl.d.tf, sl.d.fmt, sl.cfg.volume_n, sl.d.bmin, 0));
-    KF_CK(cudaMemset(sl.d.dirty, 0, size_t(sl.d.nb) * sl.d.nb * sl.d.nb));
+    KF_CK(launch_rebuild_bricks(sl.d.tf, sl.d.fmt, sl.cfg.volume_n, sl.d.bmin, sl.d.bdil, sl.d.sdil, 0));
     KF_CK(cudaDeviceSynchronize());
     return KF_OK;
 }
@@ -1015,7 +1034,7 @@ kf_status kf_raycast(const kf_volume* vol, const float pose[16], const float inv
     if (!pose || !inv_cam_k || !vertex || !normal || w <= 0 || h <= 0) return KF_ERR_ARG;
     KF_TRY(check_volume(vol));
     if (w != nw || h != nh) return KF_ERR_SHAPE;   // project/src/raycast.cu:155-158
-    if (!(step_large > 0.f) || !(max_depth > min_depth) || !(max_depth < 1000.f) ||
+    if (!(step_large > step_small) || !(max_depth > min_depth) || !(max_depth < 1000.f) ||
         !(vol->mu * step_small > max_depth * 1e-6f))
         return KF_ERR_ARG;
     StageTimer t(elapsed_ms, as_stream(stream));
@@ -1336,8 +1355,7 @@ kf_status kf_batch_autotune(kf_batch* b, void* stream, char* report, size_t repo
         cudaMemcpy(sl.d.tw, static_cast<char*>(saved[i]) + sizes[i], sizes[i], cudaMemcpyDeviceToDevice);
         cudaMemcpy(sl.d.pose, static_cast<char*>(saved[i]) + 2 * sizes[i], sizeof(PoseDev), cudaMemcpyDeviceToDevice);
         cudaFree(saved[i]);
-        launch_rebuild_bricks(sl.d.tf, sl.d.fmt, sl.cfg.volume_n, sl.d.bmin, 0);
-        cudaMemset(sl.d.dirty, 0, size_t(sl.d.nb) * sl.d.nb * sl.d.nb);
+        launch_rebuild_bricks(sl.d.tf, sl.d.fmt, sl.cfg.volume_n, sl.d.bmin, sl.d.bdil, sl.d.sdil, 0);
     }
     KF_CK(cudaDeviceSynchronize());
     e.graph_dirty = true;

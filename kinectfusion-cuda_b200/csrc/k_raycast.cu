@@ -4,32 +4,86 @@
 // computeGradient (:29-42), called once per pyramid level at the previous frame's pose
 // (project/src/kinect_fusion.cpp:137-144).  The reference samples a cudaArray through the
 // texture unit; here the distance array stays in linear HBM (x fastest), so fusion can stream
-// it with 16-byte vectors, and the march does its own trilinear interpolation with the
-// reference's texel mapping (uvw * n - 0.5, clamp).  The slice of the volume near the
-// surface a frame's rays touch stays resident in the 126 MB L2.  Rays of all levels and all
-// sessions form one tile list that persistent blocks pull from an atomic counter.
+// it, and the march does its own trilinear interpolation with the reference's texel mapping
+// (uvw * n - 0.5, clamp).  Every sample the reference takes is taken at the same float
+// position, in the same order; three things make that fast:
+//   - Skipping: a sample whose eight taps lie in cells (32^3 super-bricks, then 8^3 bricks)
+//     whose distance lower bound proves it cannot change the march (>= 0.991 during large
+//     steps, >= 0.001 during small steps) is not evaluated, nor is any later sample in the
+//     same cell; t still advances by the reference's repeated float additions.
+//   - Load balance: each warp pulls 8 x 4-ray tiles from an atomic counter, and a lane marches
+//     at most 64 iterations; longer rays are queued with their exact march state.
+//   - Long rays: a second kernel marches each queued ray with a whole warp, 32 consecutive
+//     samples per round, taking the first sample (in order) that changes the state.
 #include "kf_host.h"
 
 namespace kf {
 
 constexpr int kMaxMarchSamples = 1 << 16;
+constexpr int kSerialBudget = 64;   // loop iterations a lane marches before queueing the ray
 
-// one ray of raycastKernel; returns after writing (or deliberately not writing) its pixel
+struct RayGeo {
+    F3 o, dir;
+    float sc, off;                            // texel coordinate = (o + dir t) * sc + off
+    float tox, toy, toz, tdx, tdy, tdz;       // the same as an affine function of t
+    float itdx, itdy, itdz;
+};
+
+// march state: everything the reference's loop carries from one sample to the next
+struct RayState {
+    float t, prev, prev_t, near_d, far_d;
+    int small;        // 0 while stepping by 1.99 mu, 1 once stepping by 0.1 mu
+    int prev_known;   // 0 when the last non-negative sample was skipped (value not computed)
+    int guard;        // samples taken (hard bound)
+};
+
+struct LongRay {
+    int s, level, i, j;
+    RayState st;
+};
+
+__device__ __forceinline__ void ray_matrix(const SessionDev* S, const LevelDev& Lv, float* m, F3& o) {
+    // R_prev * K_l^-1 (the reference forms mat3(pose) * invK per ray)
+    const float* R = S->pose->Rpf;
+#pragma unroll
+    for (int col = 0; col < 3; ++col)
+#pragma unroll
+        for (int row = 0; row < 3; ++row)
+            m[col * 3 + row] = R[row] * Lv.ik[col * 3 + 0] + R[3 + row] * Lv.ik[col * 3 + 1] + R[6 + row] * Lv.ik[col * 3 + 2];
+    o = F3{S->pose->tpf[0], S->pose->tpf[1], S->pose->tpf[2]};
+}
+
+// ray through pixel (i, j): direction (R K^-1)(i + .5, j + .5, 1), not normalised, so t is
+// camera depth
+__device__ __forceinline__ void make_geo(const SessionDev* S, const float* m, F3 o, int i, int j, RayGeo& g) {
+    g.o = o;
+    g.dir = mv3(m, F3{float(i) + 0.5f, float(j) + 0.5f, 1.0f});
+    g.sc = float(S->n) / S->vol_w;
+    g.off = 0.5f * float(S->n) - 0.5f;
+    g.tox = o.x * g.sc + g.off; g.toy = o.y * g.sc + g.off; g.toz = o.z * g.sc + g.off;
+    g.tdx = g.dir.x * g.sc; g.tdy = g.dir.y * g.sc; g.tdz = g.dir.z * g.sc;
+    g.itdx = 1.0f / g.tdx; g.itdy = 1.0f / g.tdy; g.itdz = 1.0f / g.tdz;
+}
+
+__device__ __forceinline__ void texel(const RayGeo& g, float t, float& x, float& y, float& z) {
+    x = (g.o.x + g.dir.x * t) * g.sc + g.off;
+    y = (g.o.y + g.dir.y * t) * g.sc + g.off;
+    z = (g.o.z + g.dir.z * t) * g.sc + g.off;
+}
+
 template <class TF>
-__device__ __forceinline__ void march_ray(const SessionDev* __restrict__ S, const LevelDev& Lv, const float* Rw,
-                                          F3 o, const TF* __restrict__ f, int level, int i, int j) {
-    const int w = Lv.w;
-    float4* ov = S->pv[level] + size_t(j) * w + i;
-    float4* on = S->pn[level] + size_t(j) * w + i;
-    const int n = S->n;
-    const float width = S->vol_w, mu = S->mu;
+__device__ __forceinline__ float sample_at(const SessionDev* S, const RayGeo& g, const TF* f, float t) {
+    float x, y, z;
+    texel(g, t, x, y, z);
+    return trilinear(f, S->n, x, y, z);
+}
 
-    // direction = (R * K^-1) (i + .5, j + .5, 1), not normalised: t is camera depth
-    const F3 pix{float(i) + 0.5f, float(j) + 0.5f, 1.0f};
-    const F3 dir = mv3(Rw, pix);
-    const F3 inv{1.0f / dir.x, 1.0f / dir.y, 1.0f / dir.z};
-    const float half = width * 0.5f;
-    // intersectBBox
+// intersectBBox and the [min, max] depth clip; false when the reference returns before
+// marching (such rays keep the previous map contents unless keep_on_miss is off)
+__device__ __forceinline__ bool ray_start(const SessionDev* S, const RayGeo& g, RayState& st) {
+    const F3 inv{1.0f / g.dir.x, 1.0f / g.dir.y, 1.0f / g.dir.z};
+    const float half = S->vol_w * 0.5f;
+    const F3 o = g.o;
     const float t0x = (-half - o.x) * inv.x, t1x = (half - o.x) * inv.x;
     const float t0y = (-half - o.y) * inv.y, t1y = (half - o.y) * inv.y;
     const float t0z = (-half - o.z) * inv.z, t1z = (half - o.z) * inv.z;
@@ -39,106 +93,180 @@ __device__ __forceinline__ void march_ray(const SessionDev* __restrict__ S, cons
     tmin = fmaxf(tmin, fminf(t0z, t1z));
     tmax = fminf(tmax, fmaxf(t0z, t1z));
     if (tmax < tmin) { tmin = -1.0f; tmax = -1.0f; }
-    bool early = tmax < 0.0f;
-    float near_d = 0.f, far_d = 0.f;
-    if (!early) {
-        near_d = fmaxf(S->min_d, tmin);
-        far_d = fminf(S->max_d, tmax);
-        early = near_d >= far_d;
-    }
-    if (early) {
-        if (!S->keep_on_miss) {
-            *ov = make_float4(0.f, 0.f, 0.f, kInvalid);
-            *on = make_float4(0.f, 0.f, 0.f, kInvalid);
-        }
-        return;
-    }
-    // texel coordinate of world point p: (p / width + 0.5) * n - 0.5
-    const float sc = float(n) / width, off = 0.5f * float(n) - 0.5f;
-    const float large = mu * S->step_l, small = mu * S->step_s;
-    const float* __restrict__ bmin = S->bmin;
-    const int nb = S->nb;
-    // the ray in texel space, for brick exits: x(t) = tox + tdx t
-    const float tox = o.x * sc + off, toy = o.y * sc + off, toz = o.z * sc + off;
-    const float tdx = dir.x * sc, tdy = dir.y * sc, tdz = dir.z * sc;
-    float inc = large, prev = 0.f, precise = 0.f;
-    float prev_t = 0.f;       // position of the last non-negative sample
-    bool prev_known = true;   // false when that sample was skipped (its value not computed)
-    int guard = 0;            // hard bound on samples per ray, whatever the configuration
-    float t = near_d;
-    while (t < far_d && guard < kMaxMarchSamples) {
-        const float x = (o.x + dir.x * t) * sc + off;
-        const float y = (o.y + dir.y * t) * sc + off;
-        const float z = (o.z + dir.z * t) * sc + off;
-        if (bmin) {
-            // A brick whose minimum is >= 0.991 (large steps) or >= 0.001 (small steps) holds
-            // no sample that changes the march: the value stays >= 0.99 resp. >= 0, so the
-            // reference would only step on.  Skip this sample and every later one inside the
-            // brick (0.01 texel inside its faces), advancing t exactly as the reference does.
-            const int ix = min(max(int(floorf(x)), 0), n - 1) >> 3;
-            const int iy = min(max(int(floorf(y)), 0), n - 1) >> 3;
-            const int iz = min(max(int(floorf(z)), 0), n - 1) >> 3;
-            const float m = __ldg(bmin + (size_t(iz) * nb + iy) * nb + ix);
-            if (m >= (inc == large ? 0.991f : 0.001f)) {
-                float t_safe = far_d;
-                if (tdx > 0.f && ix < nb - 1) t_safe = fminf(t_safe, (float(8 * ix + 8) - 0.01f - tox) / tdx);
-                if (tdx < 0.f && ix > 0) t_safe = fminf(t_safe, (float(8 * ix) + 0.01f - tox) / tdx);
-                if (tdy > 0.f && iy < nb - 1) t_safe = fminf(t_safe, (float(8 * iy + 8) - 0.01f - toy) / tdy);
-                if (tdy < 0.f && iy > 0) t_safe = fminf(t_safe, (float(8 * iy) + 0.01f - toy) / tdy);
-                if (tdz > 0.f && iz < nb - 1) t_safe = fminf(t_safe, (float(8 * iz + 8) - 0.01f - toz) / tdz);
-                if (tdz < 0.f && iz > 0) t_safe = fminf(t_safe, (float(8 * iz) + 0.01f - toz) / tdz);
+    if (tmax < 0.0f) return false;
+    const float near_d = fmaxf(S->min_d, tmin), far_d = fminf(S->max_d, tmax);
+    if (near_d >= far_d) return false;
+    st.t = near_d;
+    st.near_d = near_d;
+    st.far_d = far_d;
+    st.prev = 0.f;
+    st.prev_t = 0.f;
+    st.small = 0;
+    st.prev_known = 1;
+    st.guard = 0;
+    return true;
+}
+
+// The reference's march loop for one lane (project/src/raycast.cu:75-117).  Returns 1 when
+// the ray is finished (precise = refined hit distance, 0 for none) and 0 when `budget`
+// iterations ran out with the ray still marching (state kept in st).
+template <class TF>
+__device__ int march_serial(const SessionDev* S, const RayGeo& g, const TF* f, RayState& st, int budget,
+                            float& precise) {
+    const int n = S->n;
+    const float mu = S->mu, large = mu * S->step_l, small = mu * S->step_s;
+    const int* __restrict__ bdil = S->bdil;
+    const int* __restrict__ sdil = S->sdil;
+    const int nb = S->nb, ns = S->ns;
+    // order-preserving int keys of the two skip thresholds
+    const int k_large = __float_as_int(0.991f), k_small = __float_as_int(0.001f);
+    int iters = 0;
+    while (st.t < st.far_d && st.guard < kMaxMarchSamples) {
+        if (iters++ >= budget) return 0;
+        const float inc = st.small ? small : large;
+        float x, y, z;
+        texel(g, st.t, x, y, z);
+        if (bdil) {
+            const int vx = min(max(int(floorf(x)), 0), n - 1);
+            const int vy = min(max(int(floorf(y)), 0), n - 1);
+            const int vz = min(max(int(floorf(z)), 0), n - 1);
+            const int thr = st.small ? k_small : k_large;
+            int sh = 0, cells = 0;
+            if (__ldg(sdil + (size_t(vz >> 5) * ns + (vy >> 5)) * ns + (vx >> 5)) >= thr) {
+                sh = 5;
+                cells = ns;
+            } else if (__ldg(bdil + (size_t(vz >> 3) * nb + (vy >> 3)) * nb + (vx >> 3)) >= thr) {
+                sh = 3;
+                cells = nb;
+            }
+            if (sh) {
+                // skip this sample and every later one whose base voxel stays in the cell
+                // (0.01 texel inside its faces)
+                const int ix = vx >> sh, iy = vy >> sh, iz = vz >> sh;
+                const float fs = float(1 << sh);
+                float t_safe = st.far_d;
+                if (g.tdx > 0.f && ix < cells - 1) t_safe = fminf(t_safe, (fs * float(ix + 1) - 0.01f - g.tox) * g.itdx);
+                if (g.tdx < 0.f && ix > 0) t_safe = fminf(t_safe, (fs * float(ix) + 0.01f - g.tox) * g.itdx);
+                if (g.tdy > 0.f && iy < cells - 1) t_safe = fminf(t_safe, (fs * float(iy + 1) - 0.01f - g.toy) * g.itdy);
+                if (g.tdy < 0.f && iy > 0) t_safe = fminf(t_safe, (fs * float(iy) + 0.01f - g.toy) * g.itdy);
+                if (g.tdz > 0.f && iz < cells - 1) t_safe = fminf(t_safe, (fs * float(iz + 1) - 0.01f - g.toz) * g.itdz);
+                if (g.tdz < 0.f && iz > 0) t_safe = fminf(t_safe, (fs * float(iz) + 0.01f - g.toz) * g.itdz);
                 do {
-                    prev_t = t;
-                    t += inc;
-                    ++guard;
-                } while (t < t_safe && t < far_d && guard < kMaxMarchSamples);
-                prev_known = false;
+                    st.prev_t = st.t;
+                    st.t += inc;
+                    ++st.guard;
+                } while (st.t < t_safe && st.t < st.far_d && st.guard < kMaxMarchSamples);
+                st.prev_known = 0;
                 continue;
             }
         }
         const float tsdf = trilinear(f, n, x, y, z);
-        ++guard;
+        ++st.guard;
         if (tsdf < 0.0f) {
-            if (t != near_d) {
-                if (inc == large) {   // went through the surface with a large step: back off
-                    t -= mu;
-                    inc = small;
-                    t += inc;
+            if (st.t != st.near_d) {
+                if (!st.small) {   // went through the surface with a large step: back off
+                    st.t -= mu;
+                    st.small = 1;
+                    st.t += small;
                     continue;
                 }
-                if (!prev_known) {
-                    const float ax = (o.x + dir.x * prev_t) * sc + off;
-                    const float ay = (o.y + dir.y * prev_t) * sc + off;
-                    const float az = (o.z + dir.z * prev_t) * sc + off;
-                    prev = trilinear(f, n, ax, ay, az);
-                }
-                precise = t - inc * prev / (tsdf - prev);   // the reference's zero-crossing formula
+                if (!st.prev_known) st.prev = sample_at(S, g, f, st.prev_t);
+                precise = st.t - small * st.prev / (tsdf - st.prev);   // the reference's formula
             }
-            break;
+            return 1;
         } else if (tsdf < 0.99f) {
-            inc = small;
+            st.small = 1;
         }
-        prev = tsdf;
-        prev_known = true;
-        prev_t = t;
-        t += inc;
+        st.prev = tsdf;
+        st.prev_known = 1;
+        st.prev_t = st.t;
+        st.t += st.small ? small : large;
     }
+    return 1;
+}
+
+// The same loop for one ray, carried by all 32 lanes of a warp (every lane holds the same
+// g and st): each round lane k evaluates the sample k steps ahead (its t formed by k
+// sequential float additions, exactly the reference's positions), and the first sample that
+// changes the state -- a negative value, or below 0.99 during large steps -- is applied.
+template <class TF>
+__device__ void march_coop(const SessionDev* S, const RayGeo& g, const TF* f, RayState& st, int lane,
+                           float& precise) {
+    const float mu = S->mu, large = mu * S->step_l, small = mu * S->step_s;
+    const unsigned int full = 0xffffffffu;
+    while (st.t < st.far_d && st.guard < kMaxMarchSamples) {
+        const float inc = st.small ? small : large;
+        float tk = st.t;
+        for (int q = 0; q < lane; ++q) tk += inc;
+        const bool valid = tk < st.far_d && st.guard + lane < kMaxMarchSamples;
+        const float fk = valid ? sample_at(S, g, f, tk) : 0.0f;
+        const bool event = valid && (fk < 0.0f || (!st.small && fk < 0.99f));
+        const unsigned int evm = __ballot_sync(full, event);
+        const unsigned int valm = __ballot_sync(full, valid);
+        if (!evm) {
+            if (!valm) break;
+            const int last = 31 - __clz(valm);   // valid lanes form a prefix
+            const float tl = __shfl_sync(full, tk, last);
+            st.prev = __shfl_sync(full, fk, last);
+            st.prev_t = tl;
+            st.prev_known = 1;
+            st.guard += last + 1;
+            st.t = tl + inc;
+            continue;
+        }
+        const int e = __ffs(evm) - 1;
+        const float te = __shfl_sync(full, tk, e), fe = __shfl_sync(full, fk, e);
+        if (e > 0) {
+            st.prev = __shfl_sync(full, fk, e - 1);
+            st.prev_t = __shfl_sync(full, tk, e - 1);
+            st.prev_known = 1;
+        }
+        st.guard += e + 1;
+        if (fe < 0.0f) {
+            if (te != st.near_d) {
+                if (!st.small) {
+                    st.t = te - mu;
+                    st.small = 1;
+                    st.t += small;
+                    continue;
+                }
+                if (!st.prev_known) st.prev = sample_at(S, g, f, st.prev_t);
+                precise = te - small * st.prev / (fe - st.prev);
+            }
+            return;
+        }
+        st.small = 1;   // 0 <= fe < 0.99 during large steps
+        st.prev = fe;
+        st.prev_t = te;
+        st.prev_known = 1;
+        st.t = te + small;
+    }
+}
+
+// computeGradient (project/src/raycast.cu:29-42) at the hit and the map writes (:120-144)
+template <class TF>
+__device__ void finish_ray(const SessionDev* S, const RayGeo& g, const TF* f, int level, int i, int j, float precise) {
+    const int w = S->lv[level].w;
+    float4* ov = S->pv[level] + size_t(j) * w + i;
+    float4* on = S->pn[level] + size_t(j) * w + i;
     if (precise != 0.0f) {
-        const F3 vtx{o.x + dir.x * precise, o.y + dir.y * precise, o.z + dir.z * precise};
-        // computeGradient: central differences mu / 2 apart, in uvw units
+        const int n = S->n;
+        const float mu = S->mu, width = S->vol_w;
+        const F3 vtx{g.o.x + g.dir.x * precise, g.o.y + g.dir.y * precise, g.o.z + g.dir.z * precise};
+        // central differences mu / 2 apart, in uvw units
         const float r = mu * 0.5f / width;
         const float rt = r * float(n);
-        const float x = vtx.x * sc + off, y = vtx.y * sc + off, z = vtx.z * sc + off;
+        const float x = vtx.x * g.sc + g.off, y = vtx.y * g.sc + g.off, z = vtx.z * g.sc + g.off;
         const float fx0 = trilinear(f, n, x + rt, y, z), fy0 = trilinear(f, n, x, y + rt, z);
         const float fz0 = trilinear(f, n, x, y, z + rt);
         const float fx = trilinear(f, n, x - rt, y, z), fy = trilinear(f, n, x, y - rt, z);
         const float fz = trilinear(f, n, x, y, z - rt);
-        F3 g{(fx - fx0) / r, (fy - fy0) / r, (fz - fz0) / r};
-        const float gn = sqrtf(dot3(g, g));
+        F3 gr{(fx - fx0) / r, (fy - fy0) / r, (fz - fz0) / r};
+        const float gn = sqrtf(dot3(gr, gr));
         if (depth_valid(gn)) {
-            g = F3{g.x / gn, g.y / gn, g.z / gn};
+            gr = F3{gr.x / gn, gr.y / gn, gr.z / gn};
             *ov = make_float4(vtx.x, vtx.y, vtx.z, kValid);
-            *on = make_float4(g.x, g.y, g.z, kValid);
+            *on = make_float4(gr.x, gr.y, gr.z, kValid);
             return;
         }
     }
@@ -146,49 +274,102 @@ __device__ __forceinline__ void march_ray(const SessionDev* __restrict__ S, cons
     *on = make_float4(0.f, 0.f, 0.f, kInvalid);
 }
 
-__global__ void __launch_bounds__(256) raycast_kernel(EngineView v) {
-    __shared__ int s_tile;
-    __shared__ float s_m[9];
-    __shared__ float s_o[3];
-    const int tid = threadIdx.x;
+__device__ __forceinline__ void write_miss(const SessionDev* S, int level, int i, int j) {
+    if (S->keep_on_miss) return;
+    const int w = S->lv[level].w;
+    S->pv[level][size_t(j) * w + i] = make_float4(0.f, 0.f, 0.f, kInvalid);
+    S->pn[level][size_t(j) * w + i] = make_float4(0.f, 0.f, 0.f, kInvalid);
+}
+
+template <class TF>
+__device__ void serial_ray(const EngineView& v, const SessionDev* S, int s, const float* m, F3 o, int level, int i,
+                           int j) {
+    const TF* f = static_cast<const TF*>(S->tf);
+    RayGeo g;
+    make_geo(S, m, o, i, j, g);
+    RayState st;
+    if (!ray_start(S, g, st)) {
+        write_miss(S, level, i, j);
+        return;
+    }
+    float precise = 0.0f;
+    if (!march_serial(S, g, f, st, kSerialBudget, precise)) {
+        const unsigned int slot = atomicAdd(&v.counters[6], 1u);
+        if (slot < unsigned(v.longq_cap)) {
+            v.longq[slot] = LongRay{s, level, i, j, st};
+            return;
+        }
+        march_serial(S, g, f, st, 0x7fffffff, precise);   // queue full: finish here
+    }
+    finish_ray(S, g, f, level, i, j, precise);
+}
+
+// Each warp pulls 8 x 4-ray tiles on its own (no block-wide barrier).
+__global__ void __launch_bounds__(256, 3) raycast_kernel(EngineView v) {
+    const int lane = threadIdx.x & 31;
     const int ntiles = v.tb->n_ray;
-    // lane layout: each warp owns an 8 x 4 patch of the 16 x 16 tile
-    const int warp = tid >> 5, lane = tid & 31;
-    const int lx = (warp & 1) * 8 + (lane & 7), ly = (warp >> 1) * 4 + (lane >> 3);
+    const int lx = lane & 7, ly = lane >> 3;
     while (true) {
-        if (tid == 0) s_tile = int(atomicAdd(&v.counters[0], 1u));
-        __syncthreads();
-        const int t = s_tile;
+        int t = 0;
+        if (lane == 0) t = int(atomicAdd(&v.counters[0], 1u));
+        t = __shfl_sync(0xffffffffu, t, 0);
         if (t >= ntiles) break;
         const RayTile T = v.ray[t];
         const StepDev st = v.step[T.s];
-        if (st.active && !st.first) {
-            const SessionDev* S = &v.sess[T.s];
-            const LevelDev& Lv = S->lv[T.level];
-            if (tid < 9) {
-                // R_prev * K_l^-1 (the reference forms mat3(pose) * invK per ray)
-                const int col = tid / 3, row = tid % 3;
-                const float* R = S->pose->Rpf;
-                s_m[tid] = R[row] * Lv.ik[col * 3 + 0] + R[3 + row] * Lv.ik[col * 3 + 1] + R[6 + row] * Lv.ik[col * 3 + 2];
-            } else if (tid < 12) {
-                s_o[tid - 9] = S->pose->tpf[tid - 9];
-            }
-            __syncthreads();
-            const int i = T.x0 + lx, j = T.y0 + ly;
-            if (i < Lv.cw && j < Lv.ch) {
-                const F3 o{s_o[0], s_o[1], s_o[2]};
-                if (S->fmt == KF_TSDF_F16U16)
-                    march_ray(S, Lv, s_m, o, static_cast<const __half*>(S->tf), T.level, i, j);
-                else
-                    march_ray(S, Lv, s_m, o, static_cast<const float*>(S->tf), T.level, i, j);
-            }
-        }
-        __syncthreads();
+        if (!st.active || st.first) continue;
+        const SessionDev* S = &v.sess[T.s];
+        const LevelDev& Lv = S->lv[T.level];
+        const int i = T.x0 + lx, j = T.y0 + ly;
+        if (i >= Lv.cw || j >= Lv.ch) continue;
+        float m[9];
+        F3 o;
+        ray_matrix(S, Lv, m, o);
+        if (S->fmt == KF_TSDF_F16U16)
+            serial_ray<__half>(v, S, T.s, m, o, T.level, i, j);
+        else
+            serial_ray<float>(v, S, T.s, m, o, T.level, i, j);
     }
 }
 
+template <class TF>
+__device__ void coop_ray(const SessionDev* S, const LongRay& L, int lane) {
+    const TF* f = static_cast<const TF*>(S->tf);
+    float m[9];
+    F3 o;
+    ray_matrix(S, S->lv[L.level], m, o);
+    RayGeo g;
+    make_geo(S, m, o, L.i, L.j, g);
+    RayState st = L.st;
+    float precise = 0.0f;
+    march_coop(S, g, f, st, lane, precise);
+    if (lane == 0) finish_ray(S, g, f, L.level, L.i, L.j, precise);
+}
+
+// the queued long rays, one warp each
+__global__ void __launch_bounds__(256) raycast_long_kernel(EngineView v) {
+    const int lane = threadIdx.x & 31;
+    const int count = min(int(v.counters[6]), v.longq_cap);
+    while (true) {
+        int idx = 0;
+        if (lane == 0) idx = int(atomicAdd(&v.counters[7], 1u));
+        idx = __shfl_sync(0xffffffffu, idx, 0);
+        if (idx >= count) break;
+        const LongRay L = v.longq[idx];
+        const SessionDev* S = &v.sess[L.s];
+        if (S->fmt == KF_TSDF_F16U16)
+            coop_ray<__half>(S, L, lane);
+        else
+            coop_ray<float>(S, L, lane);
+    }
+}
+
+int long_ray_bytes() { return int(sizeof(LongRay)); }
+
 cudaError_t launch_raycast(const EngineView& v, int grid, cudaStream_t st) {
     raycast_kernel<<<grid, 256, 0, st>>>(v);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    raycast_long_kernel<<<grid, 256, 0, st>>>(v);
     return cudaGetLastError();
 }
 
@@ -203,7 +384,17 @@ template <class TF>
 __global__ void raycast_stage_kernel(SessionDev S, RayStage rs, int w, int h) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y * blockDim.y + threadIdx.y;
     if (i >= w || j >= h) return;
-    march_ray(&S, S.lv[0], rs.m, F3{rs.o[0], rs.o[1], rs.o[2]}, static_cast<const TF*>(S.tf), 0, i, j);
+    const TF* f = static_cast<const TF*>(S.tf);
+    RayGeo g;
+    make_geo(&S, rs.m, F3{rs.o[0], rs.o[1], rs.o[2]}, i, j, g);
+    RayState st;
+    if (!ray_start(&S, g, st)) {
+        write_miss(&S, 0, i, j);
+        return;
+    }
+    float precise = 0.0f;
+    march_serial(&S, g, f, st, 0x7fffffff, precise);
+    finish_ray(&S, g, f, 0, i, j, precise);
 }
 
 cudaError_t stage_raycast(const kf_volume* vol, const float* pose, const float* ik, float4* vtx, float4* nrm, int w,

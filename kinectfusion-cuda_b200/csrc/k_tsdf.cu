@@ -1,42 +1,48 @@
-// k_tsdf.cu -- TSDF volume: initialisation, projective fusion, brick minima, layout conversion.
+// k_tsdf.cu -- TSDF volume: initialisation, projective fusion, brick bounds, layout conversion.
 //
 // Reference: initializeGridKernel (project/src/tsdf.cu:7-18) and fuseKernel
 // (project/src/tsdf.cu:20-75), which walks one (x, y) voxel column per thread through a
-// cudaArray surface with 4-byte reads and writes.  Here the volume is two linear arrays in
-// HBM (distance, weight; x fastest) and a warp owns a 32 x VEC-voxel segment of an x row:
-// 4 voxels per lane for float/float, 8 for fp16/uint16, moved with 16-byte vectors.
-//   - A segment whose two end voxels project outside the view frustum on the same side is
-//     skipped whole: depth and image coordinates are monotone along the row, so no voxel
-//     between them can pass the reference's frustum test.
-//   - A lane projects its voxels, issues all their depth-map gathers together, and touches
-//     the volume only when one of them updates.
-//   - Every updated voxel marks its 8^3 brick (and the brick whose one-voxel apron it is)
-//     dirty; a second kernel refreshes those bricks' minimum distance for the raycaster.
-// Segments of every session of a batch are handed to persistent warps through one atomic
+// cudaArray surface with 4-byte reads and writes, projecting every voxel of the volume.
+//
+// Here the volume is two linear arrays in HBM (distance, weight; x fastest).  A warp owns a
+// 32 x 8 x 8 block of voxels at a time:
+//   - The block is first tested as a whole from its 8 projected corners (the projection of a
+//     box in front of the camera lies inside its corners' bounding box): outside the depth
+//     range or the image, no valid depth under it, or every voxel more than mu behind the
+//     farthest valid depth under it -- then no voxel of it can update and it is skipped.
+//   - Otherwise its 64 rows are walked four at a time with one voxel per lane along x, so
+//     every depth gather and volume access of the warp touches 32 consecutive voxels, and a
+//     lane reads and writes the volume only for voxels that update.
+//   - Each 8^3 brick keeps a lower bound of its distances (an atomic minimum of every value
+//     fusion stores), and a small pass widens it to the 2 x 2 x 2 bricks a trilinear sample
+//     can touch; the raycaster skips samples whose bound proves they cannot matter.
+// Blocks of every session of a batch are handed to persistent warps through one atomic
 // counter.
 #include "kf_host.h"
 
 namespace kf {
 
-int fuse_vec(int fmt) { return fmt == KF_TSDF_F16U16 ? 8 : 4; }
-int fuse_segs_per_row(int n, int fmt) {
-    const int span = 32 * fuse_vec(fmt);
-    return (n + span - 1) / span;
+__host__ __device__ int fuse_units(int n) { return ((n + 31) / 32) * ((n + 7) / 8) * ((n + 7) / 8); }
+
+// order-preserving int key of a float (atomicMin on floats of either sign)
+__device__ __forceinline__ int fkey(float x) {
+    const int i = __float_as_int(x);
+    return i >= 0 ? i : (i ^ 0x7fffffff);
 }
 
-// per-warp fusion context (shared memory): the session's camera and volume for the segment
+// per-warp fusion context (shared memory): the session's camera and volume
 struct FuseCtx {
     float iR[9], it[3];          // world -> camera
     float fx, fy, cx, cy, min_d, max_d, mu, max_w;
     const float* depth;          // unfiltered metres map
     const float* dmax;           // per 16x16 tile: largest valid depth (null: not available)
     int t16w, t16h;
-    int w, h, n, nb;
+    int w, h, n, nb, fmt;
     void* F;
     void* W;
     const float* xs;
     const float* zs;
-    uint8_t* dirty;              // null: no brick bookkeeping (stage calls)
+    int* bmin;                   // brick lower bounds (null: none kept)
 };
 
 // running weighted average (project/src/tsdf.cu:56-69); max_w > 0 clamps the weight
@@ -47,143 +53,159 @@ __device__ __forceinline__ void fuse_update(float& F, float& Wt, float fn, float
     Wt = w1;
 }
 
-__device__ __forceinline__ void mark_dirty(const FuseCtx& c, int x0, int j, int k) {
-    const int nb = c.nb;
-    const int bx = x0 >> 3, by = j >> 3, bz = k >> 3;
-    const int bx0 = ((x0 & 7) == 0 && bx > 0) ? bx - 1 : bx;
-    const int by0 = ((j & 7) == 0 && by > 0) ? by - 1 : by;
-    const int bz0 = ((k & 7) == 0 && bz > 0) ? bz - 1 : bz;
-    for (int zz = bz0; zz <= bz; ++zz)
-        for (int yy = by0; yy <= by; ++yy)
-            for (int xx = bx0; xx <= bx; ++xx) c.dirty[(size_t(zz) * nb + yy) * nb + xx] = 1;
+// true when no voxel of the block [x0, x0+32) x [j0, j0+8) x [k0, k0+8) can update
+__device__ __forceinline__ bool block_culled(const FuseCtx& c, int x0, int j0, int k0, int lane) {
+    const int n = c.n;
+    const int q = lane & 7;
+    const float x = __ldg(c.xs + ((q & 1) ? min(x0 + 31, n - 1) : x0));
+    const float y = __ldg(c.xs + ((q & 2) ? min(j0 + 7, n - 1) : j0));
+    const float z = __ldg(c.zs + ((q & 4) ? min(k0 + 7, n - 1) : k0));
+    // same operation order as the per-voxel projection below
+    const float bx = c.iR[3] * y + c.iR[6] * z + c.it[0];
+    const float by = c.iR[4] * y + c.iR[7] * z + c.it[1];
+    const float bz = c.iR[5] * y + c.iR[8] * z + c.it[2];
+    const float ex = c.iR[0] * x + bx, ey = c.iR[1] * x + by, ez = c.iR[2] * x + bz;
+    float zmin = ez, zmax = ez;
+#pragma unroll
+    for (int off = 4; off >= 1; off >>= 1) {
+        zmin = fminf(zmin, __shfl_xor_sync(0xffffffffu, zmin, off));
+        zmax = fmaxf(zmax, __shfl_xor_sync(0xffffffffu, zmax, off));
+    }
+    if (zmax < c.min_d - 1e-4f || zmin >= c.max_d + 1e-4f) return true;
+    if (!(zmin > 1e-3f)) return false;   // a corner behind the camera: no image bound
+    float px = (c.fx * ex + c.cx * ez) / ez, py = (c.fy * ey + c.cy * ez) / ez;
+    float pxmin = px, pxmax = px, pymin = py, pymax = py;
+#pragma unroll
+    for (int off = 4; off >= 1; off >>= 1) {
+        pxmin = fminf(pxmin, __shfl_xor_sync(0xffffffffu, pxmin, off));
+        pxmax = fmaxf(pxmax, __shfl_xor_sync(0xffffffffu, pxmax, off));
+        pymin = fminf(pymin, __shfl_xor_sync(0xffffffffu, pymin, off));
+        pymax = fmaxf(pymax, __shfl_xor_sync(0xffffffffu, pymax, off));
+    }
+    if (pxmax < -0.01f || pxmin > float(c.w) + 0.01f || pymax < -0.01f || pymin > float(c.h) + 0.01f) return true;
+    if (!c.dmax) return false;
+    const int tx0 = min(max(int(pxmin - 0.01f), 0), c.w - 1) >> 4;
+    const int tx1 = min(max(int(pxmax + 0.01f), 0), c.w - 1) >> 4;
+    const int ty0 = min(max(int(pymin - 0.01f), 0), c.h - 1) >> 4;
+    const int ty1 = min(max(int(pymax + 0.01f), 0), c.h - 1) >> 4;
+    const int nx = tx1 - tx0 + 1, ntile = nx * (ty1 - ty0 + 1);
+    if (ntile > 512) return false;
+    float dm = 0.0f;
+    for (int t = lane; t < ntile; t += 32) dm = fmaxf(dm, __ldg(c.dmax + size_t(ty0 + t / nx) * c.t16w + tx0 + t % nx));
+#pragma unroll
+    for (int off = 16; off >= 1; off >>= 1) dm = fmaxf(dm, __shfl_xor_sync(0xffffffffu, dm, off));
+    // every voxel meets either an invalid depth or d - z <= dm - zmin < -mu
+    return dm == 0.0f || zmin > dm + c.mu + 1e-4f;
 }
 
-// One segment of row (j, k): voxels [seg * 32 * VEC, (seg + 1) * 32 * VEC) of the row.
-template <int VEC, class TF, class TW>
-__device__ __forceinline__ void fuse_segment(const FuseCtx& c, int j, int k, int seg, int lane) {
+// fuseKernel (project/src/tsdf.cu:28-74) for the 64 rows of one block, lanes along x
+template <class TF, class TW>
+__device__ __forceinline__ void fuse_block(const FuseCtx& c, int x0, int j0, int k0, int lane) {
     const int n = c.n;
-    const float y = __ldg(c.xs + j), z = __ldg(c.zs + k);
-    // row-constant part of the world -> camera transform
-    const F3 b{c.iR[3] * y + c.iR[6] * z + c.it[0], c.iR[4] * y + c.iR[7] * z + c.it[1],
-               c.iR[5] * y + c.iR[8] * z + c.it[2]};
-    // warp-uniform frustum test of the segment's end voxels
-    {
-        const int s0 = seg * 32 * VEC, s1 = min(n, (seg + 1) * 32 * VEC) - 1;
-        const float xa = __ldg(c.xs + s0), xb = __ldg(c.xs + s1);
-        const float za = c.iR[2] * xa + b.z, zb = c.iR[2] * xb + b.z;
-        if (fmaxf(za, zb) < c.min_d - 1e-4f || fminf(za, zb) >= c.max_d + 1e-4f) return;
-        if (fminf(za, zb) > 1e-3f) {
-            const float pxa = (c.fx * (c.iR[0] * xa + b.x) + c.cx * za) / za;
-            const float pxb = (c.fx * (c.iR[0] * xb + b.x) + c.cx * zb) / zb;
-            if (fmaxf(pxa, pxb) < -0.01f || fminf(pxa, pxb) > float(c.w) + 0.01f) return;
-            const float pya = (c.fy * (c.iR[1] * xa + b.y) + c.cy * za) / za;
-            const float pyb = (c.fy * (c.iR[1] * xb + b.y) + c.cy * zb) / zb;
-            if (fmaxf(pya, pyb) < -0.01f || fminf(pya, pyb) > float(c.h) + 0.01f) return;
-            if (c.dmax) {
-                // The voxels project onto the image segment between the two end pixels, so
-                // onto its bounding box of 16x16 tiles.  With D the largest valid depth there,
-                // a voxel either meets no valid depth or has diff <= D - z: nothing updates
-                // when D = 0 or when every voxel lies more than mu behind D.
-                const int tx0 = min(max(int(fminf(pxa, pxb) - 0.01f), 0), c.w - 1) >> 4;
-                const int tx1 = min(max(int(fmaxf(pxa, pxb) + 0.01f), 0), c.w - 1) >> 4;
-                const int ty0 = min(max(int(fminf(pya, pyb) - 0.01f), 0), c.h - 1) >> 4;
-                const int ty1 = min(max(int(fmaxf(pya, pyb) + 0.01f), 0), c.h - 1) >> 4;
-                const int nx = tx1 - tx0 + 1, ntile = nx * (ty1 - ty0 + 1);
-                if (ntile <= 256) {
-                    float dm = 0.0f;
-                    for (int q = lane; q < ntile; q += 32)
-                        dm = fmaxf(dm, __ldg(c.dmax + size_t(ty0 + q / nx) * c.t16w + tx0 + q % nx));
+    const int x = x0 + lane;
+    const bool lane_in = x < n;
+    const float xv = __ldg(c.xs + min(x, n - 1));
+    const int jn = min(8, n - j0), kn = min(8, n - k0), rows = jn * kn;
+    int kmin = 0x7fffffff;   // key of the smallest distance this lane stores
+    TF* F = static_cast<TF*>(c.F);
+    TW* Wa = static_cast<TW*>(c.W);
+    for (int r0 = 0; r0 < rows; r0 += 4) {
+        int pix[4];
+        float pz[4], d[4];
+        unsigned int cand = 0;
+        // project (steps 1-2)
 #pragma unroll
-                    for (int off = 16; off >= 1; off >>= 1) dm = fmaxf(dm, __shfl_xor_sync(0xffffffffu, dm, off));
-                    if (dm == 0.0f || fminf(za, zb) > dm + c.mu + 1e-4f) return;
+        for (int q = 0; q < 4; ++q) {
+            pix[q] = 0;
+            pz[q] = 0.f;
+            const int r = r0 + q;
+            if (r >= rows || !lane_in) continue;
+            const int j = j0 + r % jn, k = k0 + r / jn;
+            const float y = __ldg(c.xs + j), z = __ldg(c.zs + k);
+            const float bx = c.iR[3] * y + c.iR[6] * z + c.it[0];
+            const float by = c.iR[4] * y + c.iR[7] * z + c.it[1];
+            const float bz = c.iR[5] * y + c.iR[8] * z + c.it[2];
+            const float ex = c.iR[0] * xv + bx, ey = c.iR[1] * xv + by, ez = c.iR[2] * xv + bz;
+            const float iz = 1.0f / ez;
+            const float px = (c.fx * ex + c.cx * ez) * iz;
+            const float py = (c.fy * ey + c.cy * ez) * iz;
+            pz[q] = ez;
+            if (ez >= c.min_d && ez < c.max_d && px >= 0.0f && px < float(c.w) && py >= 0.0f && py < float(c.h)) {
+                pix[q] = int(py) * c.w + int(px);
+                cand |= 1u << q;
+            }
+        }
+        // nearest-pixel depth (step 3), four gathers in flight
+#pragma unroll
+        for (int q = 0; q < 4; ++q) d[q] = (cand & (1u << q)) ? __ldg(c.depth + pix[q]) : 0.0f;
+        float fn[4], wn[4];
+        unsigned int upd = 0;
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            fn[q] = wn[q] = 0.f;
+            if (!(cand & (1u << q)) || !depth_valid(d[q])) continue;
+            const float diff = d[q] - pz[q];
+            if (diff >= -c.mu) {   // step 4
+                fn[q] = fminf(1.0f, diff / c.mu);
+                wn[q] = 1.0f / d[q];
+                upd |= 1u << q;
+            }
+        }
+        if (!__any_sync(0xffffffffu, upd != 0)) continue;
+        // step 5: read-modify-write, four rows' loads in flight
+        size_t idx[4];
+        float f0[4], w0[4];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            const int r = r0 + q;
+            idx[q] = (size_t(k0 + r / jn) * n + (j0 + r % jn)) * n + x;
+            f0[q] = w0[q] = 0.f;
+            if (upd & (1u << q)) {
+                if constexpr (sizeof(TF) == 4) {
+                    f0[q] = F[idx[q]];
+                    w0[q] = Wa[idx[q]];
+                } else {
+                    f0[q] = __half2float(F[idx[q]]);
+                    w0[q] = float(Wa[idx[q]]) * (1.0f / KF_WEIGHT_SCALE);
                 }
             }
         }
-    }
-    const int x0 = seg * 32 * VEC + lane * VEC;
-    if (x0 >= n) return;
-    float xv[VEC];
 #pragma unroll
-    for (int q = 0; q < VEC; q += 4) {
-        const float4 t = __ldg(reinterpret_cast<const float4*>(c.xs + x0 + q));
-        xv[q] = t.x; xv[q + 1] = t.y; xv[q + 2] = t.z; xv[q + 3] = t.w;
-    }
-    // project (fuseKernel steps 1-2, project/src/tsdf.cu:33-44)
-    int pix[VEC];
-    float pz[VEC];
-    unsigned int cand = 0;
-#pragma unroll
-    for (int v = 0; v < VEC; ++v) {
-        const float ex = c.iR[0] * xv[v] + b.x, ey = c.iR[1] * xv[v] + b.y, ez = c.iR[2] * xv[v] + b.z;
-        const float iz = 1.0f / ez;
-        const float px = (c.fx * ex + c.cx * ez) * iz;
-        const float py = (c.fy * ey + c.cy * ez) * iz;
-        pz[v] = ez;
-        pix[v] = 0;
-        if (ez >= c.min_d && ez < c.max_d && px >= 0.0f && px < float(c.w) && py >= 0.0f && py < float(c.h)) {
-            pix[v] = int(py) * c.w + int(px);
-            cand |= 1u << v;
-        }
-    }
-    if (!cand) return;
-    // nearest-pixel depth (step 3), all gathers in flight together
-    float d[VEC];
-#pragma unroll
-    for (int v = 0; v < VEC; ++v) d[v] = (cand & (1u << v)) ? __ldg(c.depth + pix[v]) : 0.0f;
-    float fn[VEC], wn[VEC];
-    unsigned int upd = 0;
-#pragma unroll
-    for (int v = 0; v < VEC; ++v) {
-        fn[v] = 0.f;
-        wn[v] = 0.f;
-        if (!(cand & (1u << v)) || !depth_valid(d[v])) continue;
-        const float diff = d[v] - pz[v];
-        if (diff >= -c.mu) {   // step 4
-            fn[v] = fminf(1.0f, diff / c.mu);
-            wn[v] = 1.0f / d[v];
-            upd |= 1u << v;
-        }
-    }
-    if (!upd) return;
-    // step 5: read-modify-write of the voxels that update
-    const size_t base = (size_t(k) * n + j) * n + x0;
-    if constexpr (VEC == 4) {
-        float4* fp = reinterpret_cast<float4*>(static_cast<float*>(c.F) + base);
-        float4* wp = reinterpret_cast<float4*>(static_cast<float*>(c.W) + base);
-        const float4 fq = *fp, wq = *wp;
-        float fa[4] = {fq.x, fq.y, fq.z, fq.w}, wa[4] = {wq.x, wq.y, wq.z, wq.w};
-#pragma unroll
-        for (int v = 0; v < 4; ++v)
-            if (upd & (1u << v)) fuse_update(fa[v], wa[v], fn[v], wn[v], c.max_w);
-        *fp = make_float4(fa[0], fa[1], fa[2], fa[3]);
-        *wp = make_float4(wa[0], wa[1], wa[2], wa[3]);
-    } else {
-        uint4* fp = reinterpret_cast<uint4*>(static_cast<__half*>(c.F) + base);
-        uint4* wp = reinterpret_cast<uint4*>(static_cast<uint16_t*>(c.W) + base);
-        uint4 fq = *fp, wq = *wp;
-        __half* fh = reinterpret_cast<__half*>(&fq);
-        uint16_t* wh = reinterpret_cast<uint16_t*>(&wq);
-#pragma unroll
-        for (int v = 0; v < 8; ++v)
-            if (upd & (1u << v)) {
-                float f0 = __half2float(fh[v]);
-                float w0 = float(wh[v]) * (1.0f / KF_WEIGHT_SCALE);
-                fuse_update(f0, w0, fn[v], wn[v], c.max_w);
-                fh[v] = __float2half_rn(f0);
-                wh[v] = uint16_t(fminf(rintf(w0 * KF_WEIGHT_SCALE), 65535.0f));
+        for (int q = 0; q < 4; ++q) {
+            if (!(upd & (1u << q))) continue;
+            fuse_update(f0[q], w0[q], fn[q], wn[q], c.max_w);
+            if constexpr (sizeof(TF) == 4) {
+                F[idx[q]] = f0[q];
+                Wa[idx[q]] = w0[q];
+                kmin = min(kmin, fkey(f0[q]));
+            } else {
+                const __half hf = __float2half_rn(f0[q]);
+                F[idx[q]] = hf;
+                Wa[idx[q]] = uint16_t(fminf(rintf(w0[q] * KF_WEIGHT_SCALE), 65535.0f));
+                kmin = min(kmin, fkey(__half2float(hf)));
             }
-        *fp = fq;
-        *wp = wq;
+        }
     }
-    if (c.dirty) mark_dirty(c, x0, j, k);
+    if (c.bmin) {
+        // all of a lane's voxels in this block sit in brick (x >> 3, j0 >> 3, k0 >> 3):
+        // reduce over the brick's 8 lanes, one atomic per brick
+#pragma unroll
+        for (int off = 4; off >= 1; off >>= 1) kmin = min(kmin, __shfl_xor_sync(0xffffffffu, kmin, off));
+        if ((lane & 7) == 0 && kmin != 0x7fffffff && lane_in)
+            atomicMin(c.bmin + (size_t(k0 >> 3) * c.nb + (j0 >> 3)) * c.nb + (x >> 3), kmin);
+    }
 }
 
-template <int VEC, class TF, class TW>
-__device__ __forceinline__ void fuse_segment_index(const FuseCtx& c, long long seg_local, int lane) {
-    const int spr = (c.n + 32 * VEC - 1) / (32 * VEC);
-    const long long row = seg_local / spr;
-    const int seg = int(seg_local - row * spr);
-    fuse_segment<VEC, TF, TW>(c, int(row % c.n), int(row / c.n), seg, lane);
+__device__ __forceinline__ void fuse_unit(const FuseCtx& c, long long u, int lane) {
+    const int ux = (c.n + 31) / 32, uy = (c.n + 7) / 8;
+    const int x0 = int(u % ux) * 32;
+    const int j0 = int((u / ux) % uy) * 8;
+    const int k0 = int(u / ((long long)ux * uy)) * 8;
+    if (block_culled(c, x0, j0, k0, lane)) return;
+    if (c.fmt == KF_TSDF_F16U16)
+        fuse_block<__half, uint16_t>(c, x0, j0, k0, lane);
+    else
+        fuse_block<float, float>(c, x0, j0, k0, lane);
 }
 
 __device__ void load_ctx(const SessionDev* S, FuseCtx& c) {
@@ -195,11 +217,11 @@ __device__ void load_ctx(const SessionDev* S, FuseCtx& c) {
     c.depth = S->depth_m;
     c.dmax = S->dmax16;
     c.t16w = S->t16w; c.t16h = S->t16h;
-    c.w = S->W; c.h = S->H; c.n = S->n; c.nb = S->nb;
-    c.F = S->tf; c.W = S->tw; c.xs = S->xs; c.zs = S->zs; c.dirty = S->dirty;
+    c.w = S->W; c.h = S->H; c.n = S->n; c.nb = S->nb; c.fmt = S->fmt;
+    c.F = S->tf; c.W = S->tw; c.xs = S->xs; c.zs = S->zs; c.bmin = S->bmin;
 }
 
-constexpr int kFuseChunk = 4;   // segments a warp takes per atomic
+constexpr int kFuseChunk = 2;   // blocks a warp takes per atomic
 constexpr int kFuseWarps = 8;
 
 __global__ void __launch_bounds__(256, 4) fuse_kernel(EngineView v) {
@@ -219,7 +241,7 @@ __global__ void __launch_bounds__(256, 4) fuse_kernel(EngineView v) {
         for (int q = 0; q < kFuseChunk; ++q) {
             const long long g = (long long)g0 + q;
             if (g >= total) break;
-            int lo = 0, hi = S_cap;   // session of segment g (warp-uniform binary search)
+            int lo = 0, hi = S_cap;   // session of block g (warp-uniform binary search)
             while (hi - lo > 1) {
                 const int mid = (lo + hi) >> 1;
                 if (__ldg(v.fuse_prefix + mid) <= g) lo = mid; else hi = mid;
@@ -233,11 +255,7 @@ __global__ void __launch_bounds__(256, 4) fuse_kernel(EngineView v) {
                 __syncwarp();
             }
             if (!live) continue;
-            const long long local = g - __ldg(v.fuse_prefix + lo);
-            if (v.sess[lo].fmt == KF_TSDF_F16U16)
-                fuse_segment_index<8, __half, uint16_t>(c, local, lane);
-            else
-                fuse_segment_index<4, float, float>(c, local, lane);
+            fuse_unit(c, g - __ldg(v.fuse_prefix + lo), lane);
         }
     }
 }
@@ -247,116 +265,159 @@ cudaError_t launch_fuse(const EngineView& v, int grid, cudaStream_t st) {
     return cudaGetLastError();
 }
 
-// ---- brick minima ----
+// ---- brick bounds ----
 
-// min over the 9 x 9 x 9 voxels [8b, 8b + 8] (clamped) of brick (bx, by, bz); one warp
-template <class TF>
-__device__ __forceinline__ float brick_min(const TF* f, int n, int bx, int by, int bz, int lane) {
-    float m = 3.0e38f;
-    for (int q = lane; q < 729; q += 32) {
-        const int dx = q % 9, dy = (q / 9) % 9, dz = q / 81;
-        const int x = min(bx * 8 + dx, n - 1), y = min(by * 8 + dy, n - 1), z = min(bz * 8 + dz, n - 1);
-        m = fminf(m, load_f(f, (size_t(z) * n + y) * n + x));
-    }
-#pragma unroll
-    for (int off = 16; off >= 1; off >>= 1) m = fminf(m, __shfl_xor_sync(0xffffffffu, m, off));
-    return m;
-}
-
-// persistent warps take 32 bricks at a time, recompute the dirty ones, clear their flags
-__global__ void __launch_bounds__(256) brick_kernel(EngineView v) {
-    const int lane = threadIdx.x & 31;
+// bdil[b] = min of bmin over bricks {b, b+1}^3 (clamped): every brick a trilinear sample whose
+// base voxel lies in brick b can touch
+__global__ void __launch_bounds__(256) brick_dilate_kernel(EngineView v) {
     const long long total = v.tb->brick_total;
     const int S_cap = v.tb->S;
-    unsigned long long* ctr = reinterpret_cast<unsigned long long*>(v.counters + 4);
-    while (true) {
-        unsigned long long g0 = 0;
-        if (lane == 0) g0 = atomicAdd(ctr, 32ull);
-        g0 = __shfl_sync(0xffffffffu, g0, 0);
-        if ((long long)g0 >= total) break;
-        const long long g = (long long)g0 + lane;
-        int s = -1;
-        long long local = 0;
-        bool dirty = false;
-        if (g < total) {
-            int lo = 0, hi = S_cap;
-            while (hi - lo > 1) {
-                const int mid = (lo + hi) >> 1;
-                if (__ldg(v.brick_prefix + mid) <= g) lo = mid; else hi = mid;
-            }
-            s = lo;
-            local = g - __ldg(v.brick_prefix + lo);
-            const SessionDev* S = &v.sess[s];
-            dirty = v.step[s].active && S->dirty[local] != 0;
+    for (long long g = blockIdx.x * (long long)blockDim.x + threadIdx.x; g < total; g += (long long)gridDim.x * blockDim.x) {
+        int lo = 0, hi = S_cap;
+        while (hi - lo > 1) {
+            const int mid = (lo + hi) >> 1;
+            if (__ldg(v.brick_prefix + mid) <= g) lo = mid; else hi = mid;
         }
-        unsigned int mask = __ballot_sync(0xffffffffu, dirty);
-        while (mask) {
-            const int src = __ffs(mask) - 1;
-            mask &= mask - 1;
-            const int ss = __shfl_sync(0xffffffffu, s, src);
-            const long long bl = __shfl_sync(0xffffffffu, local, src);
-            const SessionDev* S = &v.sess[ss];
-            const int nb = S->nb;
-            const int bx = int(bl % nb), by = int((bl / nb) % nb), bz = int(bl / ((long long)nb * nb));
-            const float m = S->fmt == KF_TSDF_F16U16
-                                ? brick_min(static_cast<const __half*>(S->tf), S->n, bx, by, bz, lane)
-                                : brick_min(static_cast<const float*>(S->tf), S->n, bx, by, bz, lane);
-            if (lane == 0) {
-                S->bmin[bl] = m;
-                S->dirty[bl] = 0;
-            }
+        if (!v.step[lo].active) continue;
+        const SessionDev* S = &v.sess[lo];
+        const long long b = g - __ldg(v.brick_prefix + lo);
+        const int nb = S->nb;
+        const int bx = int(b % nb), by = int((b / nb) % nb), bz = int(b / ((long long)nb * nb));
+        const int x1 = min(bx + 1, nb - 1), y1 = min(by + 1, nb - 1), z1 = min(bz + 1, nb - 1);
+        const int* m = S->bmin;
+        int k = 0x7fffffff;
+        k = min(k, m[(size_t(bz) * nb + by) * nb + bx]);
+        k = min(k, m[(size_t(bz) * nb + by) * nb + x1]);
+        k = min(k, m[(size_t(bz) * nb + y1) * nb + bx]);
+        k = min(k, m[(size_t(bz) * nb + y1) * nb + x1]);
+        k = min(k, m[(size_t(z1) * nb + by) * nb + bx]);
+        k = min(k, m[(size_t(z1) * nb + by) * nb + x1]);
+        k = min(k, m[(size_t(z1) * nb + y1) * nb + bx]);
+        k = min(k, m[(size_t(z1) * nb + y1) * nb + x1]);
+        S->bdil[b] = k;
+    }
+}
+
+// sdil[s] = min of bmin over bricks [4s, 4s + 4] per axis (clamped): the bricks a sample whose
+// base voxel lies in super-brick s can touch; one warp per super-brick
+__device__ __forceinline__ int superbrick_bound(const int* bmin, int nb, int sx, int sy, int sz, int lane) {
+    const int x0 = 4 * sx, y0 = 4 * sy, z0 = 4 * sz;
+    int k = 0x7fffffff;
+    for (int q = lane; q < 125; q += 32) {
+        const int x = min(x0 + q % 5, nb - 1), y = min(y0 + (q / 5) % 5, nb - 1), z = min(z0 + q / 25, nb - 1);
+        k = min(k, bmin[(size_t(z) * nb + y) * nb + x]);
+    }
+#pragma unroll
+    for (int off = 16; off >= 1; off >>= 1) k = min(k, __shfl_xor_sync(0xffffffffu, k, off));
+    return k;
+}
+
+__global__ void __launch_bounds__(256) superbrick_kernel(EngineView v) {
+    const long long total = v.tb->super_total;
+    const int S_cap = v.tb->S;
+    const int lane = threadIdx.x & 31;
+    const long long warp = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5;
+    const long long nwarps = ((long long)gridDim.x * blockDim.x) >> 5;
+    for (long long g = warp; g < total; g += nwarps) {
+        int lo = 0, hi = S_cap;
+        while (hi - lo > 1) {
+            const int mid = (lo + hi) >> 1;
+            if (__ldg(v.super_prefix + mid) <= g) lo = mid; else hi = mid;
         }
+        if (!v.step[lo].active) continue;
+        const SessionDev* S = &v.sess[lo];
+        const long long b = g - __ldg(v.super_prefix + lo);
+        const int ns = S->ns;
+        const int k = superbrick_bound(S->bmin, S->nb, int(b % ns), int((b / ns) % ns), int(b / ((long long)ns * ns)), lane);
+        if (lane == 0) S->sdil[b] = k;
     }
 }
 
 cudaError_t launch_bricks(const EngineView& v, int grid, cudaStream_t st) {
-    brick_kernel<<<grid, 256, 0, st>>>(v);
+    brick_dilate_kernel<<<grid, 256, 0, st>>>(v);
+    superbrick_kernel<<<grid, 256, 0, st>>>(v);
     return cudaGetLastError();
 }
 
-__global__ void init_bricks_kernel(float* bmin, uint8_t* dirty, long long nbricks) {
-    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < nbricks; i += (long long)gridDim.x * blockDim.x) {
-        bmin[i] = 2.0f;
-        dirty[i] = 0;
-    }
+__global__ void fill_key_kernel(int* a, long long count, int key) {
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < count; i += (long long)gridDim.x * blockDim.x)
+        a[i] = key;
 }
 
-cudaError_t launch_init_bricks(float* bmin, uint8_t* dirty, long long nbricks, cudaStream_t st) {
-    init_bricks_kernel<<<148 * 4, 256, 0, st>>>(bmin, dirty, nbricks);
+cudaError_t launch_init_bricks(int* bmin, int* bdil, int* sdil, int n, cudaStream_t st) {
+    const int nb = n / 8, ns = (nb + 3) / 4;
+    const long long nbricks = (long long)nb * nb * nb, nsuper = (long long)ns * ns * ns;
+    const int k2 = 0x40000000;   // key of 2.0f (bits of a positive float)
+    fill_key_kernel<<<148 * 4, 256, 0, st>>>(bmin, nbricks, k2);
+    fill_key_kernel<<<148 * 4, 256, 0, st>>>(bdil, nbricks, k2);
+    fill_key_kernel<<<148, 256, 0, st>>>(sdil, nsuper, k2);
     return cudaGetLastError();
 }
 
+// exact minimum over each brick's own 8^3 voxels (after a volume load), one warp per brick
 template <class TF>
-__global__ void rebuild_bricks_kernel(const TF* f, int n, float* bmin) {
+__global__ void rebuild_bricks_kernel(const TF* f, int n, int* bmin) {
     const int nb = n / 8;
     const long long total = (long long)nb * nb * nb;
     const int lane = threadIdx.x & 31;
     const long long warp = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5;
     const long long nwarps = ((long long)gridDim.x * blockDim.x) >> 5;
     for (long long b = warp; b < total; b += nwarps) {
-        const float m = brick_min(f, n, int(b % nb), int((b / nb) % nb), int(b / ((long long)nb * nb)), lane);
-        if (lane == 0) bmin[b] = m;
+        const int bx = int(b % nb), by = int((b / nb) % nb), bz = int(b / ((long long)nb * nb));
+        float m = 3.0e38f;
+        for (int q = lane; q < 512; q += 32) {
+            const int x = bx * 8 + (q & 7), y = by * 8 + ((q >> 3) & 7), z = bz * 8 + (q >> 6);
+            m = fminf(m, load_f(f, (size_t(z) * n + y) * n + x));
+        }
+#pragma unroll
+        for (int off = 16; off >= 1; off >>= 1) m = fminf(m, __shfl_xor_sync(0xffffffffu, m, off));
+        if (lane == 0) bmin[b] = fkey(m);
     }
 }
 
-cudaError_t launch_rebuild_bricks(const void* f, int fmt, int n, float* bmin, cudaStream_t st) {
+__global__ void dilate_one_kernel(const int* bmin, int* bdil, int nb) {
+    const long long total = (long long)nb * nb * nb;
+    for (long long b = blockIdx.x * (long long)blockDim.x + threadIdx.x; b < total; b += (long long)gridDim.x * blockDim.x) {
+        const int bx = int(b % nb), by = int((b / nb) % nb), bz = int(b / ((long long)nb * nb));
+        int k = 0x7fffffff;
+        for (int dz = 0; dz < 2; ++dz)
+            for (int dy = 0; dy < 2; ++dy)
+                for (int dx = 0; dx < 2; ++dx)
+                    k = min(k, bmin[(size_t(min(bz + dz, nb - 1)) * nb + min(by + dy, nb - 1)) * nb + min(bx + dx, nb - 1)]);
+        bdil[b] = k;
+    }
+}
+
+__global__ void superbrick_one_kernel(const int* bmin, int* sdil, int nb) {
+    const int ns = (nb + 3) / 4;
+    const long long total = (long long)ns * ns * ns;
+    const int lane = threadIdx.x & 31;
+    const long long warp = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5;
+    const long long nwarps = ((long long)gridDim.x * blockDim.x) >> 5;
+    for (long long b = warp; b < total; b += nwarps) {
+        const int k = superbrick_bound(bmin, nb, int(b % ns), int((b / ns) % ns), int(b / ((long long)ns * ns)), lane);
+        if (lane == 0) sdil[b] = k;
+    }
+}
+
+cudaError_t launch_rebuild_bricks(const void* f, int fmt, int n, int* bmin, int* bdil, int* sdil, cudaStream_t st) {
     if (fmt == KF_TSDF_F16U16)
         rebuild_bricks_kernel<<<148 * 8, 256, 0, st>>>(static_cast<const __half*>(f), n, bmin);
     else
         rebuild_bricks_kernel<<<148 * 8, 256, 0, st>>>(static_cast<const float*>(f), n, bmin);
+    dilate_one_kernel<<<148 * 4, 256, 0, st>>>(bmin, bdil, n / 8);
+    superbrick_one_kernel<<<148 * 4, 256, 0, st>>>(bmin, sdil, n / 8);
     return cudaGetLastError();
 }
 
 // ---- stage fusion on a caller volume (kernel::fuse) ----
 
-template <int VEC, class TF, class TW>
 __global__ void __launch_bounds__(256) fuse_stage_kernel(FuseCtx c) {
-    const long long spr = (c.n + 32 * VEC - 1) / (32 * VEC);
-    const long long total = (long long)c.n * c.n * spr;
+    const long long total = fuse_units(c.n);
     const int lane = threadIdx.x & 31;
     const long long warp = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5;
     const long long nwarps = ((long long)gridDim.x * blockDim.x) >> 5;
-    for (long long g = warp; g < total; g += nwarps) fuse_segment_index<VEC, TF, TW>(c, g, lane);
+    for (long long u = warp; u < total; u += nwarps) fuse_unit(c, u, lane);
 }
 
 cudaError_t stage_fuse(const float* depth, int w, int h, const float* k, const kf_volume* vol, const float* pose,
@@ -371,21 +432,18 @@ cudaError_t stage_fuse(const float* depth, int w, int h, const float* k, const k
     c.min_d = min_d; c.max_d = max_d; c.mu = vol->mu; c.max_w = vol->max_weight;
     c.n = vol->n;
     c.nb = vol->n / 8;
+    c.fmt = vol->format;
     c.F = vol->f;
     c.W = vol->w;
     c.xs = xs;
     c.zs = zs;
-    c.dirty = nullptr;
+    c.bmin = nullptr;
     // inverse of the rigid pose: R^T, -R^T t
     for (int col = 0; col < 3; ++col)
         for (int row = 0; row < 3; ++row) c.iR[col * 3 + row] = pose[row * 4 + col];
     for (int row = 0; row < 3; ++row)
         c.it[row] = -(c.iR[row] * pose[12] + c.iR[3 + row] * pose[13] + c.iR[6 + row] * pose[14]);
-    const int grid = 148 * 8;
-    if (vol->format == KF_TSDF_F16U16)
-        fuse_stage_kernel<8, __half, uint16_t><<<grid, 256, 0, st>>>(c);
-    else
-        fuse_stage_kernel<4, float, float><<<grid, 256, 0, st>>>(c);
+    fuse_stage_kernel<<<148 * 8, 256, 0, st>>>(c);
     return cudaGetLastError();
 }
 

@@ -67,12 +67,14 @@ struct SessionDev {
     void* tw;              // weight array (float or uint16)
     const float* xs;       // voxel-centre x (= y) coordinates, n floats
     const float* zs;       // voxel-centre z coordinates accumulated as the reference does
-    // 8^3-voxel bricks: minimum distance over the brick and its one-voxel apron, kept
-    // current after every fusion so the raycaster can skip samples that cannot change its
-    // decisions; `dirty` marks bricks fusion touched
-    float* bmin;
-    uint8_t* dirty;
+    // 8^3-voxel bricks: a lower bound of the brick's distances (order-preserving int keys,
+    // kept by fusion with atomic minima) and the same widened to the 2 x 2 x 2 bricks a
+    // trilinear sample can touch, which the raycaster reads to skip samples
+    int* bmin;
+    int* bdil;
+    int* sdil;             // the same for 32^3 super-bricks (bricks [4s, 4s + 4] per axis)
     int nb;                // bricks per axis (n / 8)
+    int ns;                // super-bricks per axis (ceil(nb / 4))
     float min_d, max_d, step_l, step_s;
     int keep_on_miss;
     // ICP

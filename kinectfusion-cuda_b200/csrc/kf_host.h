@@ -20,7 +20,10 @@ struct Tables {
     int pad;
     long long fuse_total;    // fusion segments over all slots
     long long brick_total;   // bricks over all slots
+    long long super_total;   // super-bricks over all slots
 };
+
+struct LongRay;   // march state of a ray handed from a lane to a warp (k_raycast.cu)
 
 // raw pointers the kernels take
 struct EngineView {
@@ -34,14 +37,17 @@ struct EngineView {
     const IcpRange* iranges;     // [level * S + s]
     const long long* fuse_prefix;// S + 1 entries, in segments
     const long long* brick_prefix;// S + 1 entries, in bricks
+    const long long* super_prefix;// S + 1 entries, in super-bricks
     float* partials;             // ICP block partials, 54 floats per tile
     GridSync* sync;
-    unsigned int* counters;      // [0] raycast tiles, [2..3] fusion segments (64-bit),
-                                 // [4..5] brick groups (64-bit)
+    unsigned int* counters;      // [0] raycast tiles, [2..3] fusion blocks (64-bit),
+                                 // [6] long rays queued, [7] long rays taken
+    LongRay* longq;              // long-ray queue
+    int longq_cap;
 };
 
 constexpr int kPreTileSize = 32;
-constexpr int kRayTileW = 16, kRayTileH = 16;
+constexpr int kRayTileW = 8, kRayTileH = 4;   // one warp per ray tile
 constexpr int kIcpThreads = 256;
 constexpr int kIcpPxPerThread = 8;
 constexpr int kIcpTilePx = kIcpThreads * kIcpPxPerThread;
@@ -52,15 +58,15 @@ cudaError_t launch_preprocess(const EngineView& v, int grid, cudaStream_t st);
 cudaError_t launch_raycast(const EngineView& v, int grid, cudaStream_t st);
 cudaError_t launch_icp(const EngineView& v, int grid, cudaStream_t st);
 cudaError_t launch_fuse(const EngineView& v, int grid, cudaStream_t st);
-// refresh the minimum of every brick fusion marked dirty
+// widen the brick lower bounds to the 2 x 2 x 2 neighbourhood the raycaster reads
 cudaError_t launch_bricks(const EngineView& v, int grid, cudaStream_t st);
-// bmin = 2 (the initial distance), dirty = 0; or, with rebuild, every brick recomputed from f
-cudaError_t launch_init_bricks(float* bmin, uint8_t* dirty, long long nbricks, cudaStream_t st);
-cudaError_t launch_rebuild_bricks(const void* f, int fmt, int n, float* bmin, cudaStream_t st);
+// bounds = key(2), the initial distance; rebuild recomputes them exactly from a loaded volume
+cudaError_t launch_init_bricks(int* bmin, int* bdil, int* sdil, int n, cudaStream_t st);
+cudaError_t launch_rebuild_bricks(const void* f, int fmt, int n, int* bmin, int* bdil, int* sdil, cudaStream_t st);
 int icp_max_grid(int num_sms);
+int long_ray_bytes();
 cudaError_t launch_barrier_selftest(GridSync* g, unsigned long long timeout_ns, int* result, cudaStream_t st);
-int fuse_segs_per_row(int n, int fmt);
-int fuse_vec(int fmt);
+__host__ __device__ int fuse_units(int n);   // 32 x 8 x 8 voxel blocks of an n^3 volume
 
 cudaError_t launch_init_volume(void* f, void* w, long long nvox, int fmt, cudaStream_t st);
 cudaError_t launch_export_interleaved(const void* f, const void* w, long long nvox, int fmt, float* dst, cudaStream_t st);

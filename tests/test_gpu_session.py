@@ -109,6 +109,35 @@ def test_raycast_maps(kf, run_small):
         assert np.mean(dz <= 1e-3) >= 0.999
 
 
+def test_pipeline_raycast_equals_serial_stage(kf, cuda):
+    """The pipeline's march (cell skipping, 64-iteration lane budget, long rays marched by a
+    whole warp) takes the same samples as a plain serial march: compare with the stage
+    raycast (no skipping, no hand-off) on the same volume and pose."""
+    from kfb200 import synth
+    cfg = kf.config_full(volume_n=256)
+    imgs, _ = synth.sequence(cfg, 6, seed=41, kind=synth.LOOP)
+    s = kf.KinectFusion(cfg)
+    for img in imgs[:5]:
+        s.process_frame(img)
+    vol = s.volume()
+    pose = s.pose()
+    k = kf.level_intrinsics(cfg, 0)
+    ik = np.linalg.inv(k.astype(np.float64)).astype(np.float32)
+    vt = cuda.zeros((cfg.height, cfg.width, 4), dtype=cuda.float32, device="cuda")
+    nt = cuda.zeros_like(vt)
+    kf.kernel.raycast(vol, pose, ik, vt, nt, cfg.min_depth, cfg.max_depth, cfg.step_large, cfg.step_small)
+    sv, sn = vt.cpu().numpy(), nt.cpu().numpy()
+    s.process_frame(imgs[5])              # its raycast runs on the same volume and pose
+    gv, gn = s.raycast_maps(0)
+    written = sv[..., 3] != 0
+    gh, sh = gv[..., 3] == -1, sv[..., 3] == -1
+    assert np.mean((gh == sh)[written]) >= 0.9999
+    both = gh & sh
+    assert both.mean() > 0.1
+    assert np.max(np.abs(gv[both][:, :3] - sv[both][:, :3])) < 1e-4
+    s.close()
+
+
 def test_tsdf(kf, run_small):
     cfg, imgs, s, P, rows = run_small
     gf, gw = s.tsdf()

@@ -207,8 +207,10 @@ def test_fuse_f16u16_vs_oracle(kf, orc, cuda, frames_small):
     df = np.abs(gf[both] - f[both])
     assert np.mean(df <= 2e-3) > 0.999
     assert np.mean(df > 0.05) < 1e-3
-    assert np.sqrt(np.mean(df[df <= 0.05] ** 2)) < 5e-4
-    assert np.quantile(np.abs(gw[both] - w[both]), 0.9999) <= 3 * 0.5 / kf.KF_WEIGHT_SCALE + 1e-6
+    assert np.sqrt(np.mean(df[df <= 0.05] ** 2)) < 1e-3
+    dw = np.abs(gw[both] - w[both])
+    assert np.mean(dw > 0.05) < 1e-3                                   # pixel-edge flips
+    assert np.quantile(dw, 0.999) <= 3 * 0.5 / kf.KF_WEIGHT_SCALE + 1e-6   # 1/1024 steps
 
 
 def test_initialize_grid(kf, cuda):
