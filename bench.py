@@ -31,6 +31,11 @@ for p in (os.path.join(ROOT, "kinectfusion-cuda_b200"), os.path.join(ROOT, "orac
         sys.path.insert(0, p)
 
 
+# kernels one frame launches: preprocess, raycast, raycast_long, icp, fuse, brick_dilate,
+# superbrick (the ncu launch list of this workload shows the same seven per frame)
+KERNELS_PER_FRAME = 7
+
+
 def measured_peaks():
     try:
         with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
@@ -96,6 +101,26 @@ def dist_setup():
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
     return world, rank, local
+
+
+def rank_seed(rank):
+    """Each rank runs its own independent session on its own seeded frames (weak scaling)."""
+    return 1 + rank
+
+
+def reduce_max(x, dist, device):
+    """Max of a per-rank time over all ranks (outside the timed region)."""
+    if dist is None:
+        return x
+    import torch
+    t = torch.tensor([x], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def aggregate_rate(world, steps, seconds):
+    """Whole-job frames/s: every rank processed `steps` frames within the slowest rank's time."""
+    return world * steps / seconds
 
 
 def full_config(kf, **kw):
@@ -176,6 +201,238 @@ def algorithmic_bytes(cfg, fused_voxels, samples):
     }
 
 
+# ---------------------------------------------------------------------------------------------
+# batched and served forms (rank 0, N = 1)
+# ---------------------------------------------------------------------------------------------
+def c4_configs(kf, seed=7):
+    """16 sessions of uneven sizes: 8 at 320x240 with 128^3-256^3 volumes over 2 m, 8 at
+    640x480 with 384^3-512^3 volumes over 3 m (multiples of 32, seeded), FP16 + u16 voxels."""
+    rng = np.random.default_rng(seed)
+    cfgs = []
+    for i in range(8):
+        cfgs.append(kf.config_small(volume_n=int(rng.choice(np.arange(128, 257, 32))), tsdf_format=kf.KF_TSDF_F16U16))
+    for i in range(8):
+        cfgs.append(kf.config_full(volume_n=int(rng.choice(np.arange(384, 513, 32))), tsdf_format=kf.KF_TSDF_F16U16))
+    return cfgs
+
+
+def session_frames(kf, cfgs, count, seed0, torch):
+    """Per-session seeded loop sequences (period `count`, so cyclic reuse is smooth), stacked
+    on the device."""
+    from kfb200 import synth
+    out = []
+    for i, c in enumerate(cfgs):
+        imgs, _ = synth.sequence(c, count, seed=seed0 + i, kind=synth.LOOP)
+        out.append(torch.from_numpy(np.stack(imgs).view(np.int16)).cuda())
+    return out
+
+
+def batch_steps(kf, b, frames, steps, start, stream, host=None):
+    """`steps` batch steps through kf_batch_step (device frames, or pinned host frames when
+    `host` is given).  Returns per-step host latencies (ms) and the device time (ms)."""
+    import ctypes
+    import torch
+    n = len(frames)
+    ptrs = (ctypes.c_void_p * n)()
+    lat = []
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    src = host if host is not None else frames
+    e0.record(stream)
+    for k in range(steps):
+        for i in range(n):
+            ptrs[i] = src[i][(start + k) % src[i].shape[0]].data_ptr()
+        t0 = time.perf_counter()
+        st = kf.lib.kf_batch_step(b._b, ptrs, 0 if host is not None else 1, ctypes.c_void_p(stream.cuda_stream), None)
+        lat.append(1000.0 * (time.perf_counter() - t0))
+        if st not in (kf.KF_OK, kf.KF_ERR_NONFINITE):
+            raise kf.KfError(st, "kf_batch_step")
+    e1.record(stream)
+    torch.cuda.synchronize()
+    return lat, e0.elapsed_time(e1)
+
+
+def plain_rate(kf, cfg, frames, steps, stream):
+    """Frames/s of one plain session (graph replays, frames in HBM)."""
+    import torch
+    s = kf.KinectFusion(cfg)
+    s.process_frame(frames[0], stream=stream)
+    for i in range(3):
+        s.process_frame_async(frames[(1 + i) % frames.shape[0]], stream=stream)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for i in range(steps):
+        s.process_frame_async(frames[(4 + i) % frames.shape[0]], stream=stream)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    s.close()
+    return steps / (ms / 1000.0)
+
+
+def run_batched(kf, torch, steps, plain_fps):
+    stream = torch.cuda.current_stream()
+    out = {}
+    # C4: 16 uneven sessions, one graph replay per step, autotuned grids
+    cfgs = c4_configs(kf)
+    nfr = 150
+    frames = session_frames(kf, cfgs, nfr, 100, torch)
+    b = kf.Batch(cfgs)
+    batch_steps(kf, b, frames, 4, 0, stream)
+    tune = b.autotune(stream=stream)
+    batch_steps(kf, b, frames, 3, 4, stream)
+    lat, ms = batch_steps(kf, b, frames, min(steps, nfr - 7), 7, stream)
+    c4_fps = len(cfgs) * len(lat) / (ms / 1000.0)
+    b.close()
+    seq_ms = 0.0
+    nseq = 20
+    for i, c in enumerate(cfgs):
+        c32 = kf.default_config(**{f: getattr(c, f) for f, _ in kf._lib.KfConfig._fields_ if f not in ("iters", "initial_pose")})
+        for q in range(3):
+            c32.iters[q] = c.iters[q]
+        for q in range(16):
+            c32.initial_pose[q] = c.initial_pose[q]
+        c32.tsdf_format = kf.KF_TSDF_F32F32
+        seq_ms += 1000.0 * nseq / plain_rate(kf, c32, frames[i], nseq, stream)
+    seq_fps = len(cfgs) * nseq / (seq_ms / 1000.0)
+    out["c4"] = {"sessions": len(cfgs), "value": round(c4_fps, 2), "unit": "frames/s",
+                 "step_p50_ms": round(float(np.percentile(lat, 50)), 3),
+                 "step_p99_ms": round(float(np.percentile(lat, 99)), 3),
+                 "sequential_plain_fps": round(seq_fps, 2), "vs_sequential_plain": round(c4_fps / seq_fps, 3),
+                 "volumes": [int(c.volume_n) for c in cfgs], "tsdf": "f16+u16 (plain runs: f32+f32)",
+                 "autotune": json.loads(tune) if tune.startswith("{") else tune}
+    del frames
+    # target: K full-size sessions (640x480, 512^3 FP16 + u16), pinned host frames in and poses
+    # out every step (closed loop: each frame's latency is its step's), against the plain
+    # single-stream f32 pipeline
+    sweep = []
+    nfr = 60
+    base = kf.config_full(tsdf_format=kf.KF_TSDF_F16U16)
+    seqs = session_frames(kf, [base] * 8, nfr, 200, torch)
+    for K in (8, 16, 32):
+        cfgs = [kf.config_full(tsdf_format=kf.KF_TSDF_F16U16) for _ in range(K)]
+        host = []
+        for i in range(K):
+            h = torch.empty(seqs[i % 8].shape, dtype=torch.int16, pin_memory=True)
+            h.copy_(seqs[i % 8].cpu())
+            host.append(h)
+        b = kf.Batch(cfgs)
+        batch_steps(kf, b, seqs, 4, 0, stream, host=host)
+        b.autotune(stream=stream)
+        batch_steps(kf, b, seqs, 3, 4, stream, host=host)
+        nst = max(20, min(steps, 200) // max(1, K // 8))
+        lat, ms = batch_steps(kf, b, seqs, nst, 7, stream, host=host)
+        wall = sum(lat) / 1000.0
+        fps = K * nst / wall
+        sweep.append({"sessions": K, "value": round(fps, 2), "unit": "frames/s",
+                      "p50_ms": round(float(np.percentile(lat, 50)), 3),
+                      "p99_ms": round(float(np.percentile(lat, 99)), 3),
+                      "vs_plain_single_stream": round(fps / plain_fps, 3) if plain_fps else None})
+        b.close()
+        del host
+    ok = [r for r in sweep if r["p99_ms"] <= 10.0]
+    best = max(ok, key=lambda r: r["value"]) if ok else None
+    out["target"] = {"workload": "K sessions of 640x480, 512^3 f16+u16 TSDF over 3 m, closed loop, pinned host "
+                                 "frames in and poses out every step (latency = step time)",
+                     "plain_single_stream_fps": round(plain_fps, 2) if plain_fps else None,
+                     "sweep": sweep, "best_at_p99_le_10ms": best}
+    return out
+
+
+def run_served(kf, torch, seconds, seed=11):
+    """C5 scaled to `seconds`: 64 sessions opening and closing, lifetimes U(5, 30) s x
+    seconds/60, 30 fps Poisson arrivals per session, 50/50 of 320x240 and 640x480, volumes
+    from {128, 256, 384, 512}^3 f16+u16, admission against a 150 GB HBM budget."""
+    import threading
+    from kfb200 import synth
+    rng = np.random.default_rng(seed)
+    scale = seconds / 60.0
+    nsess = 64
+    sizes = rng.integers(0, 2, nsess)
+    vols = rng.choice([128, 256, 384, 512], nsess)
+    life = rng.uniform(5.0, 30.0, nsess) * scale
+    start = rng.uniform(0.0, 1.0, nsess) * (seconds - life)
+    seqs = {}
+    for sz in (0, 1):
+        c = kf.config_small() if sz == 0 else kf.config_full()
+        for q in range(4):
+            seqs[(sz, q)] = synth.sequence(c, 60, seed=300 + 10 * sz + q, kind=synth.LOOP)[0]
+
+    def cfg_of(i):
+        n = int(vols[i])
+        if sizes[i] == 0:
+            w = 2.0
+            c = kf.config_small(volume_n=n, tsdf_format=kf.KF_TSDF_F16U16)
+        else:
+            w = 3.0
+            c = kf.config_full(volume_n=n, tsdf_format=kf.KF_TSDF_F16U16)
+        c.mu = max(c.mu, 2.5 * w / (n - 1))
+        return c
+
+    srv = kf.Server(64, 150 * 10 ** 9)
+    stop = threading.Event()
+    steps = [0]
+
+    def gpu_loop():
+        while not stop.is_set():
+            if srv.step() == 0:
+                time.sleep(0.0002)
+            steps[0] += 1
+
+    th = threading.Thread(target=gpu_loop, daemon=True)
+    t0 = kf.Server.now_ms()
+    th.start()
+    state = {}   # i -> [sid, next_arrival_ms, frame index, backlog arrival times]
+    refused = set()
+    done = set()
+    submitted = 0
+    while True:
+        now = kf.Server.now_ms() - t0
+        if now > seconds * 1000.0:
+            break
+        for i in range(nsess):
+            if i in done:
+                continue
+            if i not in state:
+                if now >= start[i] * 1000.0:
+                    sid = srv.try_open(cfg_of(i))
+                    if sid is None:
+                        refused.add(i)
+                        continue
+                    state[i] = [sid, now, int(rng.integers(0, 60)), []]
+                continue
+            st = state[i]
+            if now >= (start[i] + life[i]) * 1000.0:
+                srv.close_session(st[0])
+                done.add(i)
+                del state[i]
+                continue
+            while st[1] <= now:
+                st[3].append(st[1])
+                st[1] += float(rng.exponential(1000.0 / 30.0))
+            if st[3]:
+                img = seqs[(int(sizes[i]), i % 4)][st[2] % 60]
+                if srv.submit(st[0], img, t0 + st[3][0]) == kf.KF_OK:
+                    st[3].pop(0)
+                    st[2] += 1
+                    submitted += 1
+        time.sleep(0.0005)
+    stop.set()
+    th.join(timeout=30)
+    stats = srv.stats()
+    srv.close()
+    wall = (kf.Server.now_ms() - t0) / 1000.0
+    return {"workload": "64 sessions over %.0f s (C5 scaled by %.2f): lifetimes U(5,30) s x %.2f, 30 fps Poisson "
+                        "arrivals, 50/50 320x240 / 640x480, volumes {128,256,384,512}^3 f16+u16, 150 GB budget"
+                        % (seconds, scale, scale),
+            "value": round(stats["frames_done"] / wall, 2), "unit": "frames/s",
+            "p50_ms": round(stats["p50_ms"], 3), "p99_ms": round(stats["p99_ms"], 3), "max_ms": round(stats["max_ms"], 3),
+            "frames": int(stats["frames_done"]), "submitted": submitted, "steps": int(stats["steps"]),
+            "admitted": int(stats["sessions_admitted"]), "refused_at_open": int(stats["sessions_refused"]),
+            "max_active": int(stats["max_active_sessions"]),
+            "latency": "arrival of the frame (client queueing included) to result ready"}
+
+
 def run_ours(args, world, rank, local):
     import torch
     import kfb200 as kf
@@ -192,17 +449,13 @@ def run_ours(args, world, rank, local):
             dist.barrier()
 
     def max_over_ranks(x):
-        if dist is None:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+        return reduce_max(x, dist, "cuda")
 
     cfg = full_config(kf)
     steps, warmup = args.steps, args.warmup
     nfr = 1 + warmup + steps
     # each rank its own seeded session (weak scaling); frames reused cyclically past 300
-    imgs, _ = render_frames(kf, cfg, min(300, nfr + steps), seed=1 + rank)
+    imgs, _ = render_frames(kf, cfg, min(300, nfr + steps), seed=rank_seed(rank))
     nimg = len(imgs)
     dev_frames = torch.from_numpy(np.stack(imgs).view(np.int16)).cuda()
 
@@ -228,38 +481,39 @@ def run_ours(args, world, rank, local):
     clocks = sampler.stop()
     ms = e0.elapsed_time(e1)
     ms_max = max_over_ranks(ms)
-    value = world * steps / (ms_max / 1000.0)
+    value = aggregate_rate(world, steps, ms_max / 1000.0)
 
     # per-stage device times over the same workload (events between the stage launches,
     # inside the replayed graph), next `steps` frames
     s.set_profiling(True)
     acc = np.zeros(4)
     base = 1 + warmup + steps
-    for i in range(steps):
+    nprof = min(steps, 200)
+    for i in range(nprof):
         s.process_frame_async(dev_frames[(base + i) % nimg], stream=stream)
         torch.cuda.synchronize()
         acc += np.array(s.stage_times())
-    stage_ms = acc / steps
+    stage_ms = acc / nprof
     s.set_profiling(False)
-    status = s.frame_stats()
 
     # e2e through the public API: pinned host frames in, pose + statistics out, every step
-    pinned = torch.empty((steps,) + imgs[0].shape, dtype=torch.int16, pin_memory=True)
-    for i in range(steps):
-        pinned[i].copy_(torch.from_numpy(imgs[(base + steps + i) % nimg].view(np.int16)))
+    npin = min(steps, 64)   # pinned frames reused cyclically along the loop
+    pinned = torch.empty((npin,) + imgs[0].shape, dtype=torch.int16, pin_memory=True)
+    for i in range(npin):
+        pinned[i].copy_(torch.from_numpy(imgs[i % nimg].view(np.int16)))
     host_frames = pinned.numpy().view(np.uint16)
     s2 = kf.KinectFusion(cfg)
-    s2.process_frame(imgs[0])
-    for i in range(min(warmup, steps)):
-        s2.process_frame(host_frames[i])
+    for i in range(warmup):
+        s2.process_frame(host_frames[i % npin])
     barrier()
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     for i in range(steps):
-        s2.process_frame(host_frames[i])
+        s2.process_frame(host_frames[(warmup + i) % npin])
     torch.cuda.synchronize()
     e2e_s = max_over_ranks(time.perf_counter() - t0)
-    e2e_value = world * steps / e2e_s
+    e2e_value = aggregate_rate(world, steps, e2e_s)
+    status = s2.frame_stats()
 
     out = None
     if rank == 0:
@@ -308,7 +562,7 @@ def run_ours(args, world, rank, local):
                        "parallelism": "replicas" if world > 1 else "single"},
             "e2e": {"value": round(e2e_value, 3), "unit": "frames/s",
                     "h2d_bytes_per_step": int(cfg.width * cfg.height * 2), "d2h_bytes_per_step": 112},
-            "gpu_launches": 4 * steps,
+            "gpu_launches": KERNELS_PER_FRAME * steps,
             "roofline": roofline,
             "cpu_baseline": cpu,
             "clocks": clocks,
@@ -323,18 +577,38 @@ def run_ours(args, world, rank, local):
         print(json.dumps(out), flush=True)
 
 
+def run_profile_frames(args, local):
+    import torch
+    import kfb200 as kf
+    torch.cuda.set_device(local)
+    cfg = full_config(kf, tsdf_format=args.tsdf_format)
+    imgs, _ = render_frames(kf, cfg, args.profile_frames, seed=1)
+    s = kf.KinectFusion(cfg)
+    for img in imgs:
+        st, _ = s.process_frame(img)
+    torch.cuda.synchronize()
+    print("profile frames done:", args.profile_frames, "status", st, s.frame_stats(), flush=True)
+    s.close()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=100)
-    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--steps", type=int, default=1000)
+    ap.add_argument("--warmup", type=int, default=10)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
+    ap.add_argument("--profile-frames", type=int, default=0,
+                    help="run this many frames of the workload through kf_process_frame and exit, "
+                         "printing no measurement (a short command for ncu captures of one kernel)")
+    ap.add_argument("--tsdf-format", type=int, default=0, help="0: f32+f32 volume, 1: fp16+u16 (with --profile-frames)")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
     world, rank, local = dist_setup()
-    if args.impl == "reference":
+    if args.profile_frames > 0:
+        run_profile_frames(args, local)
+    elif args.impl == "reference":
         run_reference(args, world, rank)
     else:
         run_ours(args, world, rank, local)
