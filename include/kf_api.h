@@ -51,7 +51,8 @@ typedef enum kf_status {
     KF_ERR_OOM_BUDGET = 5,  /* admission refused: the session does not fit the HBM budget */
     KF_ERR_TIMEOUT = 6,     /* a bounded device-side wait expired; the context stays usable */
     KF_ERR_STATE = 7,       /* call not valid in the object's current state */
-    KF_ERR_CAPACITY = 8     /* no free slot */
+    KF_ERR_CAPACITY = 8,    /* no free slot */
+    KF_ERR_TOO_LARGE = 9    /* problem larger than the fixed scratch of a no-allocation entry point */
 } kf_status;
 
 typedef enum kf_tsdf_format {
@@ -214,6 +215,29 @@ kf_status kf_construct_icp_residuals(const float* vertex, const float* target_ve
  * device; only the 6 floats of x come back. */
 kf_status kf_solve_linear_least_squares(const float* mat_a, const float* vec_b, int n,
                                         float x_out[6], void* stream);
+/* Row limit of kf_solve_linear_least_squares_noalloc (2^20: a 1280 x 720 frame fits). */
+#define KF_LLS_NOALLOC_MAX_ROWS 1048576
+/* kf_solve_linear_least_squares without any device allocation.  No counterpart in the
+ * reference: its LinearLeastSquares::solve (project/src/linear_least_squares.cpp:23-44)
+ * allocates, and so does kf_solve_linear_least_squares, which grows a process-wide scratch
+ * with cudaFree + cudaMalloc when a larger n arrives.  Some callers cannot allow that: a
+ * tracking loop that shares the device with other sessions (cudaFree waits for the whole
+ * device, stalling their frames) and a process whose device memory is all reserved up
+ * front by a caching allocator or an HBM budget (an unplanned allocation can fail with out
+ * of memory in mid-sequence).  This entry point runs the same two kernels, with the same
+ * block count, on a scratch that is a fixed 110,640-byte array in the library's device
+ * image; its result is bit-identical to kf_solve_linear_least_squares.
+ *   - n above KF_LLS_NOALLOC_MAX_ROWS returns KF_ERR_TOO_LARGE before touching the device.
+ *   - The first call on each device does a one-time set-up with that device current (it
+ *     looks up the scratch's device address, which may load the library's device code):
+ *     make it before any latency-critical work.
+ *   - Nothing has to start at zero: each call writes every scratch value it reads.
+ *   - All calls on one device share the one scratch, so calls that overlap (two host
+ *     threads, or two streams in flight) race and give wrong results: serialise them.
+ *   - Like kf_solve_linear_least_squares it returns x to the host and synchronises
+ *     `stream`. */
+kf_status kf_solve_linear_least_squares_noalloc(const float* mat_a, const float* vec_b, int n,
+                                                float x_out[6], void* stream);
 /* ICP::computePose, project/src/icp.h:35-36.  Coarse-to-fine point-to-plane ICP of the
  * vertex pyramid against the predicted (world-frame) pyramid, starting at pose; each map
  * pointer array holds `levels` device pointers.  One cooperative device launch runs every

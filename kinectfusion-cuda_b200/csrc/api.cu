@@ -700,6 +700,7 @@ const char* kf_status_string(int s) {
         case KF_ERR_TIMEOUT: return "device wait timed out";
         case KF_ERR_STATE: return "call not valid in this state";
         case KF_ERR_CAPACITY: return "no free slot";
+        case KF_ERR_TOO_LARGE: return "problem larger than the fixed scratch of a no-allocation entry point";
         default: return "unknown status";
     }
 }

@@ -14,6 +14,8 @@
 //   B. one block per session adds its tiles' pairs in FP64, solves the 6x6 system by FP64
 //      Cholesky, updates the FP64 pose and applies the reference's early-stop test;
 // separated by bounded grid barriers.  Nothing returns to the host until the frame is done.
+#include <mutex>
+
 #include "kf_host.h"
 
 namespace kf {
@@ -543,3 +545,61 @@ cudaError_t stage_lls(const float* A, const float* b, int n, float* partials, do
 }
 
 }  // namespace kf
+
+// ---- kf_solve_linear_least_squares_noalloc: the same two kernels on a fixed scratch ----
+//
+// The scratch is this file's static device array: the partial sums of up to 512 blocks
+// (KF_LLS_NOALLOC_MAX_ROWS rows / 2048 rows per block, 54 floats each) followed by the FP64
+// solution (6 doubles), 110,640 bytes, part of the library's device image.  For
+// n <= KF_LLS_NOALLOC_MAX_ROWS, lls_num_blocks(n) is the same block count the allocating
+// entry point uses, so both reduce in the same order.  Each call writes every partial slot
+// it reads and the solution before reading them: nothing has to start at zero.  One scratch
+// per device, shared by all calls on it: overlapping calls race.
+
+namespace {
+constexpr int kNaMaxBlocks = KF_LLS_NOALLOC_MAX_ROWS / kf::kIcpTilePx;
+constexpr int kNaXOffset = kNaMaxBlocks * 54;        // in floats; the solution follows the partials
+constexpr int kNaFloats = kNaXOffset + 2 * 6;        // 6 doubles
+constexpr int kNaMaxDevices = 64;
+static_assert(kNaMaxBlocks * kf::kIcpTilePx == KF_LLS_NOALLOC_MAX_ROWS, "row limit is a whole number of blocks");
+static_assert(kNaMaxBlocks <= 148 * 4, "lls_num_blocks does not clamp below the limit");
+static_assert(kNaXOffset % 2 == 0, "the FP64 solution is 8-byte aligned");
+static_assert(sizeof(float) * kNaFloats == 110640, "scratch size stated in kf_api.h");
+
+std::mutex g_na_mu;                        // guards the one-time set-up only
+float* g_na_base[kNaMaxDevices] = {};      // device address of the scratch, per device ordinal
+}  // namespace
+
+static __device__ __align__(256) float g_lls_noalloc_scratch[kNaFloats];
+
+extern "C" kf_status kf_solve_linear_least_squares_noalloc(const float* mat_a, const float* vec_b, int n,
+                                                           float x_out[6], void* stream) {
+    if (!mat_a || !vec_b || !x_out || n <= 0) return KF_ERR_ARG;
+    if (n > KF_LLS_NOALLOC_MAX_ROWS) return KF_ERR_TOO_LARGE;
+    int dev = -1;
+    if (cudaGetDevice(&dev) != cudaSuccess) return KF_ERR_CUDA;
+    if (dev < 0 || dev >= kNaMaxDevices) return KF_ERR_ARG;
+    float* base = nullptr;
+    {
+        std::lock_guard<std::mutex> lk(g_na_mu);
+        if (!g_na_base[dev]) {
+            // set-up, once per device, with that device current
+            float* ptr = nullptr;
+            if (cudaGetSymbolAddress((void**)&ptr, g_lls_noalloc_scratch) != cudaSuccess || !ptr) return KF_ERR_CUDA;
+            g_na_base[dev] = ptr;
+        }
+        base = g_na_base[dev];
+    }
+    const int nb = kf::lls_num_blocks(n);
+    if (nb > kNaMaxBlocks) return KF_ERR_TOO_LARGE;
+    double* x_dev = reinterpret_cast<double*>(base + kNaXOffset);
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    if (kf::stage_lls(mat_a, vec_b, n, base, x_dev, nb, st) != cudaSuccess) return KF_ERR_CUDA;
+    double x[6];
+    if (cudaMemcpyAsync(x, x_dev, sizeof(x), cudaMemcpyDeviceToHost, st) != cudaSuccess) return KF_ERR_CUDA;
+    if (cudaStreamSynchronize(st) != cudaSuccess) return KF_ERR_CUDA;
+    for (int q = 0; q < 6; ++q) x_out[q] = float(x[q]);
+    for (int q = 0; q < 6; ++q)
+        if (!isfinite(x[q])) return KF_ERR_NONFINITE;
+    return KF_OK;
+}

@@ -22,6 +22,8 @@ KF_ERR_OOM_BUDGET = 5
 KF_ERR_TIMEOUT = 6
 KF_ERR_STATE = 7
 KF_ERR_CAPACITY = 8
+KF_ERR_TOO_LARGE = 9
+KF_LLS_NOALLOC_MAX_ROWS = 1048576   # row limit of kf_solve_linear_least_squares_noalloc
 
 KF_TSDF_F32F32 = 0
 KF_TSDF_F16U16 = 1
@@ -110,6 +112,7 @@ SIGNATURES = {
     "kf_raycast": (_I, [_VOL, _FP, _FP, _P, _I, _I, _P, _I, _I, _F, _F, _F, _F, _P, _FP]),
     "kf_construct_icp_residuals": (_I, [_P, _P, _P, _I, _I, _FP, _FP, _FP, _FP, _FP, _F, _F, _P, _P, _P, _FP]),
     "kf_solve_linear_least_squares": (_I, [_P, _P, _I, _FP, _P]),
+    "kf_solve_linear_least_squares_noalloc": (_I, [_P, _P, _I, _FP, _P]),
     "kf_compute_pose": (_I, [ctypes.POINTER(_P), ctypes.POINTER(_P), ctypes.POINTER(_P), _I, _I, _I, _CFG, _FP, _FP,
                              _IP, _P]),
     "kf_pose_error": (_I, [_FP, _FP, _FP]),
