@@ -31,9 +31,17 @@ for p in (os.path.join(ROOT, "kinectfusion-cuda_b200"), os.path.join(ROOT, "orac
         sys.path.insert(0, p)
 
 
-# kernels one frame launches: preprocess, raycast, raycast_long, icp, fuse, brick_dilate,
-# superbrick (the ncu launch list of this workload shows the same seven per frame)
-KERNELS_PER_FRAME = 7
+# kernels one frame launches: preprocess, raycast, raycast_long, icp, fuse_cull, fuse, brick_dilate,
+# superbrick (the ncu launch list of this workload shows the same eight per frame)
+KERNELS_PER_FRAME = 8
+
+
+def progress(msg):
+    """Phase marks on stderr (the JSON line alone goes to stdout)."""
+    print("[bench %.1fs] %s" % (time.perf_counter() - _T0, msg), file=sys.stderr, flush=True)
+
+
+_T0 = time.perf_counter()
 
 
 def measured_peaks():
@@ -232,11 +240,13 @@ def batch_steps(kf, b, frames, steps, start, stream, host=None):
     `host` is given).  Returns per-step host latencies (ms) and the device time (ms)."""
     import ctypes
     import torch
-    n = len(frames)
+    src = host if host is not None else frames
+    n = len(src)
+    if n != len(b):
+        raise ValueError("one frame sequence per session: %d for %d sessions" % (n, len(b)))
     ptrs = (ctypes.c_void_p * n)()
     lat = []
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    src = host if host is not None else frames
     e0.record(stream)
     for k in range(steps):
         for i in range(n):
@@ -277,24 +287,25 @@ def run_batched(kf, torch, steps, plain_fps):
     cfgs = c4_configs(kf)
     nfr = 150
     frames = session_frames(kf, cfgs, nfr, 100, torch)
+    progress("batched: C4 frames rendered")
     b = kf.Batch(cfgs)
     batch_steps(kf, b, frames, 4, 0, stream)
+    progress("batched: C4 first steps")
     tune = b.autotune(stream=stream)
+    progress("batched: C4 autotuned " + tune)
     batch_steps(kf, b, frames, 3, 4, stream)
     lat, ms = batch_steps(kf, b, frames, min(steps, nfr - 7), 7, stream)
+    progress("batched: C4 timed")
     c4_fps = len(cfgs) * len(lat) / (ms / 1000.0)
     b.close()
     seq_ms = 0.0
     nseq = 20
     for i, c in enumerate(cfgs):
-        c32 = kf.default_config(**{f: getattr(c, f) for f, _ in kf._lib.KfConfig._fields_ if f not in ("iters", "initial_pose")})
-        for q in range(3):
-            c32.iters[q] = c.iters[q]
-        for q in range(16):
-            c32.initial_pose[q] = c.initial_pose[q]
+        c32 = type(c).from_buffer_copy(c)
         c32.tsdf_format = kf.KF_TSDF_F32F32
         seq_ms += 1000.0 * nseq / plain_rate(kf, c32, frames[i], nseq, stream)
     seq_fps = len(cfgs) * nseq / (seq_ms / 1000.0)
+    progress("batched: sequential plain timed")
     out["c4"] = {"sessions": len(cfgs), "value": round(c4_fps, 2), "unit": "frames/s",
                  "step_p50_ms": round(float(np.percentile(lat, 50)), 3),
                  "step_p99_ms": round(float(np.percentile(lat, 99)), 3),
@@ -309,19 +320,22 @@ def run_batched(kf, torch, steps, plain_fps):
     nfr = 60
     base = kf.config_full(tsdf_format=kf.KF_TSDF_F16U16)
     seqs = session_frames(kf, [base] * 8, nfr, 200, torch)
+    pins = []
+    for q in range(8):
+        h = torch.empty(seqs[q].shape, dtype=torch.int16, pin_memory=True)
+        h.copy_(seqs[q].cpu())
+        pins.append(h)
     for K in (8, 16, 32):
         cfgs = [kf.config_full(tsdf_format=kf.KF_TSDF_F16U16) for _ in range(K)]
-        host = []
-        for i in range(K):
-            h = torch.empty(seqs[i % 8].shape, dtype=torch.int16, pin_memory=True)
-            h.copy_(seqs[i % 8].cpu())
-            host.append(h)
+        host = [pins[i % 8] for i in range(K)]
+        devs = [seqs[i % 8] for i in range(K)]
         b = kf.Batch(cfgs)
-        batch_steps(kf, b, seqs, 4, 0, stream, host=host)
+        progress("batched: target K=%d created" % K)
+        batch_steps(kf, b, devs, 4, 0, stream, host=host)
         b.autotune(stream=stream)
-        batch_steps(kf, b, seqs, 3, 4, stream, host=host)
+        batch_steps(kf, b, devs, 3, 4, stream, host=host)
         nst = max(20, min(steps, 200) // max(1, K // 8))
-        lat, ms = batch_steps(kf, b, seqs, nst, 7, stream, host=host)
+        lat, ms = batch_steps(kf, b, devs, nst, 7, stream, host=host)
         wall = sum(lat) / 1000.0
         fps = K * nst / wall
         sweep.append({"sessions": K, "value": round(fps, 2), "unit": "frames/s",
@@ -369,6 +383,7 @@ def run_served(kf, torch, seconds, seed=11):
         c.mu = max(c.mu, 2.5 * w / (n - 1))
         return c
 
+    progress("served: frames rendered")
     srv = kf.Server(64, 150 * 10 ** 9)
     stop = threading.Event()
     steps = [0]
@@ -419,6 +434,7 @@ def run_served(kf, torch, seconds, seed=11):
         time.sleep(0.0005)
     stop.set()
     th.join(timeout=30)
+    progress("served: loop done")
     stats = srv.stats()
     srv.close()
     wall = (kf.Server.now_ms() - t0) / 1000.0
@@ -461,6 +477,7 @@ def run_ours(args, world, rank, local):
 
     s = kf.KinectFusion(cfg)
     stream = torch.cuda.current_stream()
+    progress("plain: frames rendered, session created")
     s.process_frame(dev_frames[0], stream=stream)
     for i in range(warmup):
         s.process_frame_async(dev_frames[(1 + i) % nimg], stream=stream)
@@ -485,6 +502,7 @@ def run_ours(args, world, rank, local):
 
     # per-stage device times over the same workload (events between the stage launches,
     # inside the replayed graph), next `steps` frames
+    progress("plain: timed region done")
     s.set_profiling(True)
     acc = np.zeros(4)
     base = 1 + warmup + steps
@@ -507,13 +525,17 @@ def run_ours(args, world, rank, local):
         s2.process_frame(host_frames[i % npin])
     barrier()
     torch.cuda.synchronize()
+    lat = np.zeros(steps)
     t0 = time.perf_counter()
     for i in range(steps):
+        t1 = time.perf_counter()
         s2.process_frame(host_frames[(warmup + i) % npin])
+        lat[i] = time.perf_counter() - t1
     torch.cuda.synchronize()
     e2e_s = max_over_ranks(time.perf_counter() - t0)
     e2e_value = aggregate_rate(world, steps, e2e_s)
     status = s2.frame_stats()
+    progress("plain: e2e done")
 
     out = None
     if rank == 0:
@@ -546,6 +568,7 @@ def run_ours(args, world, rank, local):
                     "stage_ms": {k: round(float(v), 5) for k, v in zip(names, stage_ms)},
                     "fuse_updated_voxels": fused, "raycast_samples": samples,
                     "fuse_updated_bytes": ab["fuse_updated"]}
+        progress("plain: roofline sample done")
         cpu = None
         if world == 1 and not args.no_cpu:
             fps, nf, dt = cpu_pipeline_rate(kf, cfg, imgs[: min(nimg, 60)], budget_s=args.cpu_seconds)
@@ -561,7 +584,9 @@ def run_ours(args, world, rank, local):
                        "l2": "inputs larger than L2 (the 1 GiB volume is streamed every frame)",
                        "parallelism": "replicas" if world > 1 else "single"},
             "e2e": {"value": round(e2e_value, 3), "unit": "frames/s",
-                    "h2d_bytes_per_step": int(cfg.width * cfg.height * 2), "d2h_bytes_per_step": 112},
+                    "h2d_bytes_per_step": int(cfg.width * cfg.height * 2), "d2h_bytes_per_step": 112,
+                    "p50_ms": round(1000 * float(np.percentile(lat, 50)), 4),
+                    "p99_ms": round(1000 * float(np.percentile(lat, 99)), 4)},
             "gpu_launches": KERNELS_PER_FRAME * steps,
             "roofline": roofline,
             "cpu_baseline": cpu,
@@ -570,6 +595,13 @@ def run_ours(args, world, rank, local):
         }
     s.close()
     s2.close()
+    del dev_frames, pinned
+    if out is not None and world == 1:
+        torch.cuda.empty_cache()
+        if not args.no_batched:
+            out["batched"] = run_batched(kf, torch, min(steps, 150), value)
+        if not args.no_served:
+            out["served"] = run_served(kf, torch, args.served_seconds)
     if dist is not None:
         dist.barrier()
         dist.destroy_process_group()
@@ -599,6 +631,10 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
+    ap.add_argument("--no-batched", action="store_true", help="skip the batched-form measurement")
+    ap.add_argument("--no-served", action="store_true", help="skip the served-form measurement")
+    ap.add_argument("--served-seconds", type=float, default=20.0,
+                    help="length of the served run (the 64-session schedule is scaled to it)")
     ap.add_argument("--profile-frames", type=int, default=0,
                     help="run this many frames of the workload through kf_process_frame and exit, "
                          "printing no measurement (a short command for ncu captures of one kernel)")

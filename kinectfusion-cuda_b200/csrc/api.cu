@@ -104,8 +104,8 @@ PoseDev make_pose_dev(const float* pose16) {
     pose16_to_double(pose16, P.Rp, P.tp);
     std::memcpy(P.R, P.Rp, sizeof(P.R));
     std::memcpy(P.t, P.tp, sizeof(P.t));
-    for (int q = 0; q < 9; ++q) { P.Rpf[q] = float(P.Rp[q]); P.Rf[q] = P.Rpf[q]; }
-    for (int q = 0; q < 3; ++q) { P.tpf[q] = float(P.tp[q]); P.tf[q] = P.tpf[q]; }
+    for (int q = 0; q < 9; ++q) P.Rpf[q] = float(P.Rp[q]);
+    for (int q = 0; q < 3; ++q) P.tpf[q] = float(P.tp[q]);
     for (int c = 0; c < 3; ++c)
         for (int r = 0; r < 3; ++r) P.iRf[c * 3 + r] = float(P.Rp[r * 3 + c]);
     for (int r = 0; r < 3; ++r)
@@ -310,6 +310,8 @@ struct Engine {
     long long* d_bprefix = nullptr;
     long long* d_sprefix = nullptr;
     float* d_partials = nullptr;
+    int4* d_icp_sched = nullptr;
+    float* d_icp_mats = nullptr;
     GridSync* d_sync = nullptr;
     unsigned int* d_ctr = nullptr;
     static constexpr int kCounters = 8;
@@ -317,6 +319,9 @@ struct Engine {
     // long-ray queue of the raycaster (bytes; entries = bytes / long_ray_bytes())
     char* d_longq = nullptr;
     int cap_longq = 0;
+    // fusion queue (one entry per block of every slot at most)
+    unsigned int* d_fuseq = nullptr;
+    int cap_fuseq = 0;
     // pinned host
     StepDev* h_step = nullptr;
     OutDev* h_out = nullptr;
@@ -354,6 +359,10 @@ struct Engine {
         KF_CK(cudaMalloc(&d_fprefix, sizeof(long long) * (capacity + 1)));
         KF_CK(cudaMalloc(&d_bprefix, sizeof(long long) * (capacity + 1)));
         KF_CK(cudaMalloc(&d_sprefix, sizeof(long long) * (capacity + 1)));
+        KF_CK(cudaMalloc(&d_icp_sched, sizeof(int4) * capacity));
+        KF_CK(cudaMemset(d_icp_sched, 0, sizeof(int4) * capacity));
+        KF_CK(cudaMalloc(&d_icp_mats, sizeof(float) * 24 * capacity));
+        KF_CK(cudaMemset(d_icp_mats, 0, sizeof(float) * 24 * capacity));
         KF_CK(cudaMalloc(&d_sync, sizeof(GridSync)));
         KF_CK(cudaMalloc(&d_ctr, sizeof(unsigned int) * kCounters));
         KF_CK(cudaMallocHost(&h_step, sizeof(StepDev) * capacity));
@@ -397,7 +406,10 @@ struct Engine {
         cudaFree(d_sess); cudaFree(d_step); cudaFree(d_out); cudaFree(d_tb); cudaFree(d_pre); cudaFree(d_ray);
         cudaFree(d_itiles); cudaFree(d_iranges); cudaFree(d_fprefix); cudaFree(d_bprefix); cudaFree(d_sprefix);
         cudaFree(d_partials);
+        cudaFree(d_icp_sched);
+        cudaFree(d_icp_mats);
         cudaFree(d_longq);
+        cudaFree(d_fuseq);
         cudaFree(d_sync);
         cudaFree(d_ctr);
         cudaFreeHost(h_step); cudaFreeHost(h_out); cudaFreeHost(h_sync);
@@ -410,9 +422,13 @@ struct Engine {
         v.itiles = d_itiles; v.iranges = d_iranges; v.fuse_prefix = d_fprefix; v.brick_prefix = d_bprefix;
         v.super_prefix = d_sprefix;
         v.partials = d_partials;
+        v.icp_sched = d_icp_sched;
+        v.icp_mats = d_icp_mats;
         v.sync = d_sync; v.counters = d_ctr;
         v.longq = reinterpret_cast<LongRay*>(d_longq);
         v.longq_cap = cap_longq / long_ray_bytes();
+        v.fuseq = d_fuseq;
+        v.fuseq_cap = cap_fuseq;
         return v;
     }
 
@@ -449,8 +465,11 @@ struct Engine {
             for (int l = 0; l < c.levels; ++l) {
                 const LevelDev& Lv = sl.d.lv[l];
                 const int np = Lv.icw * Lv.ich;
-                // about one tile per ICP block per session-level, at least a block's worth
-                int tile = (np + grid_icp - 1) / grid_icp;
+                // a few tiles per ICP block per session-level (the grid's blocks take them
+                // round robin, which evens out tiles of mostly invalid pixels), at least a
+                // block's worth of pixels each
+                const int ntiles = grid_icp * kIcpTilesPerBlock;
+                int tile = (np + ntiles - 1) / ntiles;
                 tile = std::max(kIcpThreads, (tile + 31) / 32 * 32);
                 IcpRange rg;
                 rg.begin = int(it[l].size());
@@ -471,14 +490,19 @@ struct Engine {
                 rg.end += off[l];
             }
         }
-        const int old_pre = cap_pre, old_ray = cap_ray, old_it = cap_it, old_part = cap_part, old_lq = cap_longq;
+        const int old_pre = cap_pre, old_ray = cap_ray, old_it = cap_it, old_part = cap_part, old_lq = cap_longq,
+                  old_fq = cap_fuseq;
+        // fusion queue entries are 32-bit and each is taken in 4 parts counted in 32 bits
+        if (fprefix[cap] > (long long)(1 << 29)) return KF_ERR_CAPACITY;
+        KF_TRY(grow(d_fuseq, cap_fuseq, std::max<int>(1, int(fprefix[cap]))));
         KF_TRY(grow(d_pre, cap_pre, std::max<int>(1, int(pre.size()))));
         KF_TRY(grow(d_ray, cap_ray, std::max<int>(1, int(ray.size()))));
         KF_TRY(grow(d_itiles, cap_it, std::max<int>(1, int(all.size()))));
-        KF_TRY(grow(d_partials, cap_part, std::max<int>(1, int(all.size())) * 54));
+        KF_TRY(grow(d_partials, cap_part, std::max<int>(1, int(all.size())) * kIcpPartialStride));
         // room for a quarter of all rays to take the long-ray path (more fall back to the lane)
         KF_TRY(grow(d_longq, cap_longq, std::max<int>(1024, int(ray.size()) * 32 / 4) * long_ray_bytes()));
-        if (old_pre != cap_pre || old_ray != cap_ray || old_it != cap_it || old_part != cap_part || old_lq != cap_longq)
+        if (old_pre != cap_pre || old_ray != cap_ray || old_it != cap_it || old_part != cap_part || old_lq != cap_longq ||
+            old_fq != cap_fuseq)
             graph_dirty = true;
         if (!pre.empty()) KF_CK(cudaMemcpy(d_pre, pre.data(), sizeof(PreTile) * pre.size(), cudaMemcpyHostToDevice));
         if (!ray.empty()) KF_CK(cudaMemcpy(d_ray, ray.data(), sizeof(RayTile) * ray.size(), cudaMemcpyHostToDevice));

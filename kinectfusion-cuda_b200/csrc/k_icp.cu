@@ -62,6 +62,89 @@ __device__ __forceinline__ bool icp_pixel(const float4* __restrict__ vm, const f
     return true;
 }
 
+// U pixels of a tile per thread and step (p0, p0 + 256, ...), with the same arithmetic as
+// icp_pixel: the source vertices and their right and lower neighbours (for the normal) of all
+// U pixels are loaded together, then all correspondences are gathered together, so up to
+// 5 U loads are in flight per thread instead of one dependent chain per pixel.  Rejection
+// tests are conjunctive, so evaluating them in a different order gives the same mask and
+// rows; products are accumulated in pixel order.
+struct IcpMats { const float* R; const float* t; const float* M; const float* tp; };
+
+template <int U, class Acc>
+__device__ __forceinline__ void icp_multi(const float4* __restrict__ vm, const float4* __restrict__ tv,
+                                        const float4* __restrict__ tn, int w, int h, int icw, int p0, int pend,
+                                        const IcpMats& m, float dist_th, float ang_th, uint8_t* mask, Acc&& accumulate) {
+    int u[U], vv[U];
+    bool in[U];
+    float4 vc[U], vr[U], vd[U];
+    const float4 none = make_float4(0.f, 0.f, 0.f, kInvalid);
+#pragma unroll
+    for (int q = 0; q < U; ++q) {
+        const int p = p0 + q * kIcpThreads;
+        in[q] = p < pend;
+        u[q] = p % icw;
+        vv[q] = p / icw;
+        const size_t i = size_t(vv[q]) * w + u[q];
+        vc[q] = in[q] ? __ldg(vm + i) : none;
+        vr[q] = in[q] && u[q] + 1 < w ? __ldg(vm + i + 1) : none;
+        vd[q] = in[q] && vv[q] + 1 < h ? __ldg(vm + i + w) : none;
+    }
+    F3 s[U];
+    int uc[U], vcor[U];
+    bool ok[U];
+#pragma unroll
+    for (int q = 0; q < U; ++q) {
+        ok[q] = in[q] && vc[q].w == kValid;
+        uc[q] = vcor[q] = 0;
+        if (ok[q]) {
+            s[q] = mv3(m.R, f3(vc[q])) + F3{m.t[0], m.t[1], m.t[2]};
+            const F3 pt = mv3(m.M, s[q] - F3{m.tp[0], m.tp[1], m.tp[2]});
+            uc[q] = int(floorf(pt.x / pt.z));   // cvt.rzi: NaN -> 0, as in the reference
+            vcor[q] = int(floorf(pt.y / pt.z));
+            ok[q] = !(uc[q] < 0 || vcor[q] < 0 || uc[q] >= w || vcor[q] >= h);
+        }
+    }
+    float4 d4[U], n4[U];
+#pragma unroll
+    for (int q = 0; q < U; ++q) {
+        d4[q] = ok[q] ? __ldg(tv + size_t(vcor[q]) * w + uc[q]) : none;
+        n4[q] = ok[q] ? __ldg(tn + size_t(vcor[q]) * w + uc[q]) : none;
+    }
+#pragma unroll
+    for (int q = 0; q < U; ++q) {
+        bool good = ok[q] && d4[q].w == kValid && n4[q].w == kValid;
+        float a[6], b = 0.f;
+        if (good) {
+            const F3 d = f3(d4[q]);
+            const F3 e = s[q] - d;
+            good = !(sqrtf(dot3(e, e)) > dist_th);
+            // computeNormal: the vertex, its right and its lower neighbour valid
+            good = good && vr[q].w == kValid && vd[q].w == kValid;
+            if (good) {
+                const F3 c = f3(vc[q]);
+                F3 nn = cross3(f3(vr[q]) - c, f3(vd[q]) - c);
+                nn = nn * rsqrtf(dot3(nn, nn));
+                F3 nr = mv3(m.R, nn);
+                nr = nr * rsqrtf(dot3(nr, nr));
+                const F3 n = f3(n4[q]);
+                good = !(acosf(dot3(nr, n)) > ang_th);   // NaN passes, as in the reference
+                if (good) {
+                    const F3 sv = s[q];
+                    a[0] = n.y * sv.z - n.z * sv.y;
+                    a[1] = n.z * sv.x - n.x * sv.z;
+                    a[2] = n.x * sv.y - n.y * sv.x;
+                    a[3] = n.x;
+                    a[4] = n.y;
+                    a[5] = n.z;
+                    b = n.x * d.x + n.y * d.y + n.z * d.z - n.x * sv.x - n.y * sv.y - n.z * sv.z;
+                }
+            }
+        }
+        if (in[q] && mask) mask[size_t(vv[q]) * w + u[q]] = good ? 1 : 0;
+        if (good) accumulate(a, b);
+    }
+}
+
 // the 27 distinct products: upper triangle of A^T A row by row, then A^T b
 __device__ __forceinline__ void accumulate_products(float acc[32], const float a[6], float b) {
     int k = 0;
@@ -131,44 +214,52 @@ __device__ __forceinline__ void block_reduce_store(float (&acc)[32], float* red,
 // ---- FP64 solve and pose algebra (thread-level) ----
 
 // Cholesky (LLT) solve of the 6x6 normal equations (the reference: Eigen LLT<float>,
-// project/src/linear_least_squares.cpp:41).  Returns false for a non-positive pivot.
-__device__ bool cholesky6(const double* ata, const double* atb, double* x) {
-    double L[6][6];
+// project/src/linear_least_squares.cpp:41).  Returns false for a non-positive pivot.  Fully
+// unrolled so the factor stays in registers; each pivot costs one reciprocal square root and
+// the substitutions multiply by it.
+__device__ __forceinline__ bool cholesky6(const double (&ata)[36], const double (&atb)[6], double (&x)[6]) {
+    double L[6][6], inv[6];
+#pragma unroll
     for (int j = 0; j < 6; ++j) {
         double d = ata[j * 6 + j];
+#pragma unroll
         for (int k = 0; k < j; ++k) d -= L[j][k] * L[j][k];
         if (!(d > 0.0)) return false;
-        const double ljj = sqrt(d);
-        L[j][j] = ljj;
+        inv[j] = rsqrt(d);
+#pragma unroll
         for (int i = j + 1; i < 6; ++i) {
-            double s = ata[i * 6 + j];
-            for (int k = 0; k < j; ++k) s -= L[i][k] * L[j][k];
-            L[i][j] = s / ljj;
+            double t = ata[i * 6 + j];
+#pragma unroll
+            for (int k = 0; k < j; ++k) t -= L[i][k] * L[j][k];
+            L[i][j] = t * inv[j];
         }
     }
     double y[6];
+#pragma unroll
     for (int i = 0; i < 6; ++i) {
-        double s = atb[i];
-        for (int k = 0; k < i; ++k) s -= L[i][k] * y[k];
-        y[i] = s / L[i][i];
+        double t = atb[i];
+#pragma unroll
+        for (int k = 0; k < i; ++k) t -= L[i][k] * y[k];
+        y[i] = t * inv[i];
     }
+#pragma unroll
     for (int i = 5; i >= 0; --i) {
-        double s = y[i];
-        for (int k = i + 1; k < 6; ++k) s -= L[k][i] * x[k];
-        x[i] = s / L[i][i];
+        double t = y[i];
+#pragma unroll
+        for (int k = i + 1; k < 6; ++k) t -= L[k][i] * x[k];
+        x[i] = t * inv[i];
     }
-    for (int i = 0; i < 6; ++i)
-        if (!isfinite(x[i])) return false;
-    return true;
+    bool fin = true;
+#pragma unroll
+    for (int i = 0; i < 6; ++i) fin = fin && isfinite(x[i]);
+    return fin;
 }
 
 // glm::orientate3(vec3(beta, alpha, gamma)) of project/src/icp.cpp:82: the Euler composition
-// Y * X * Z, i.e. R_y(gamma) R_x(beta) R_z(alpha); column-major out
-__device__ void euler_yxz(double beta, double gamma, double alpha, double* m) {
-    double sx, cx, sy, cy, sz, cz;
-    sincos(beta, &sx, &cx);
-    sincos(gamma, &sy, &cy);
-    sincos(alpha, &sz, &cz);
+// Y * X * Z, i.e. R_y(gamma) R_x(beta) R_z(alpha); column-major out, from the sines and
+// cosines of beta (x), gamma (y) and alpha (z)
+__device__ __forceinline__ void euler_yxz_sc(double sx, double cx, double sy, double cy, double sz, double cz,
+                                             double (&m)[9]) {
     m[0] = cy * cz + sy * sx * sz;  m[1] = cx * sz;  m[2] = -sy * cz + cy * sx * sz;
     m[3] = -cy * sz + sy * sx * cz; m[4] = cx * cz;  m[5] = sy * sz + cy * sx * cz;
     m[6] = sy * cx;                 m[7] = -sx;      m[8] = cy * cx;
@@ -178,19 +269,21 @@ __device__ __forceinline__ void m3d_vec(const double* m, const double* v, double
     for (int r = 0; r < 3; ++r) o[r] = m[r] * v[0] + m[3 + r] * v[1] + m[6 + r] * v[2];
 }
 
-// the float data phase A of the next pass reads: estimate and K_l * R_prev^T
-__device__ void publish_pass(PoseDev* P, const LevelDev& Lv) {
-    for (int q = 0; q < 9; ++q) P->Rf[q] = float(P->R[q]);
-    for (int q = 0; q < 3; ++q) P->tf[q] = float(P->t[q]);
+// the 24 floats phase A of the next pass reads for a session at level Lv: the estimate
+// (R, t), M = K_l * R_prev^T and t_prev
+__device__ void publish_mats(float* m, const double* R, const double* t, const double* Rp, const float* tpf,
+                             const LevelDev& Lv) {
+    for (int q = 0; q < 9; ++q) m[q] = float(R[q]);
+    for (int q = 0; q < 3; ++q) m[9 + q] = float(t[q]);
     // K = [fx 0 cx; 0 fy cy; 0 0 1];  M = K * Rp^T;  (Rp^T)(r, c) = Rp(c, r) = Rp[r * 3 + c]
     for (int col = 0; col < 3; ++col) {
         // column col of Rp^T = row col of Rp = (Rp[col], Rp[3 + col], Rp[6 + col])
-        const double a0 = P->Rp[col], a1 = P->Rp[3 + col], a2 = P->Rp[6 + col];
-        P->M[col * 3 + 0] = float(double(Lv.fx) * a0 + double(Lv.cx) * a2);
-        P->M[col * 3 + 1] = float(double(Lv.fy) * a1 + double(Lv.cy) * a2);
-        P->M[col * 3 + 2] = float(a2);
+        const double a0 = Rp[col], a1 = Rp[3 + col], a2 = Rp[6 + col];
+        m[12 + col * 3 + 0] = float(double(Lv.fx) * a0 + double(Lv.cx) * a2);
+        m[12 + col * 3 + 1] = float(double(Lv.fy) * a1 + double(Lv.cy) * a2);
+        m[12 + col * 3 + 2] = float(a2);
     }
-    __threadfence();
+    for (int q = 0; q < 3; ++q) m[21 + q] = tpf[q];
 }
 
 // first ICP level with iterations at or below `from`
@@ -200,103 +293,191 @@ __device__ __forceinline__ int next_level(const SessionDev* S, int from) {
     return l;
 }
 
-// phase 0 for one session (one thread)
-__device__ void icp_begin(const SessionDev* S, const StepDev st) {
-    if (!st.active) return;   // empty or idle slot: its state is not touched
+// schedule entry of a session: the level of its next pass and that level's tiles
+__device__ __forceinline__ int4 sched_entry(const EngineView& v, int s, int level) {
+    if (level < 0) return make_int4(-1, 0, 0, 0);
+    const IcpRange rg = v.iranges[level * v.tb->S + s];
+    return make_int4(level, rg.begin, rg.end - rg.begin, 0);
+}
+
+// phase 0 for one session (one thread); every slot gets a schedule entry
+__device__ void icp_begin(const EngineView& v, int s) {
+    const SessionDev* S = &v.sess[s];
+    const StepDev st = v.step[s];
+    if (!st.active) {   // empty or idle slot: its state is not touched
+        v.icp_sched[s] = make_int4(-1, 0, 0, 0);
+        return;
+    }
     PoseDev* P = S->pose;
     P->status = KF_OK;
     for (int l = 0; l < kMaxLevels; ++l) P->iters[l] = 0;
     P->it = 0;
-    if (st.first) { P->level = -1; P->cont = 0; __threadfence(); return; }
-    for (int q = 0; q < 9; ++q) P->R[q] = P->Rp[q];
-    for (int q = 0; q < 3; ++q) P->t[q] = P->tp[q];
-    P->level = next_level(S, S->L - 1);
-    if (P->level >= 0) publish_pass(P, S->lv[P->level]);
-    P->cont = P->level >= 0 ? 1 : 0;
+    int level = -1;
+    if (!st.first) {
+        for (int q = 0; q < 9; ++q) P->R[q] = P->Rp[q];
+        for (int q = 0; q < 3; ++q) P->t[q] = P->tp[q];
+        level = next_level(S, S->L - 1);
+        if (level >= 0) publish_mats(v.icp_mats + size_t(s) * 24, P->Rp, P->tp, P->Rp, P->tpf, S->lv[level]);
+    }
+    P->level = level;
+    P->cont = level >= 0 ? 1 : 0;
+    v.icp_sched[s] = sched_entry(v, s, level);
     __threadfence();
 }
 
 // phase B for one session: FP64 combine of the tile pairs, solve, update, stop test
 // (ICP::computePose loop body, project/src/icp.cpp:36-54).  All threads of the block call it.
-__device__ void icp_solve(const EngineView& v, int s, double* sm, float* stage, int stage_tiles) {
+// sm: 19 * 28 doubles of shared scratch.  Warp 0 runs the solve redundantly on every lane
+// (identical values), so the three sines and cosines are computed on three lanes at once and
+// no lane waits on another through memory; lane 0 stores the results.
+__device__ void icp_solve(const EngineView& v, int s, int level, int begin, int cnt, double* sm) {
     const SessionDev* S = &v.sess[s];
     PoseDev* P = S->pose;
-    const int tid = threadIdx.x;
-    const int level = ldcg(&P->level);
-    const IcpRange rg = v.iranges[level * v.tb->S + s];
-    const int cnt = rg.end - rg.begin;
-    // bring the session's tile pairs on chip with every thread's loads in flight at once
-    const float* src = v.partials + size_t(rg.begin) * 54;
-    if (cnt <= stage_tiles) {
-#pragma unroll 4
-        for (int i = tid; i < cnt * 54; i += blockDim.x) stage[i] = ldcg(src + i);
-        __syncthreads();
-        src = stage;
+    const int tid = threadIdx.x, lane = tid & 31;
+    // warp 0 fetches everything the update needs while the block sums the tiles
+    double R0[9], t0[3], Rp[9];
+    int it0 = 0, done0 = 0, S_cap = 0, siters[kMaxLevels];
+    float stop_a = 0.f, stop_d = 0.f, tpf[3], lfx[kMaxLevels], lfy[kMaxLevels], lcx[kMaxLevels], lcy[kMaxLevels];
+    IcpRange rng[kMaxLevels];
+    if (tid < 32) {
+#pragma unroll
+        for (int q = 0; q < 9; ++q) { R0[q] = ldcg(&P->R[q]); Rp[q] = ldcg(&P->Rp[q]); }
+#pragma unroll
+        for (int q = 0; q < 3; ++q) { t0[q] = ldcg(&P->t[q]); tpf[q] = ldcg(&P->tpf[q]); }
+        it0 = ldcg(&P->it);
+        done0 = ldcg(&P->iters[level]);
+        S_cap = v.tb->S;
+        stop_a = S->stop_a;
+        stop_d = S->stop_d;
+#pragma unroll
+        for (int l = 0; l < kMaxLevels; ++l) {
+            siters[l] = S->iters[l];
+            lfx[l] = S->lv[l].fx; lfy[l] = S->lv[l].fy; lcx[l] = S->lv[l].cx; lcy[l] = S->lv[l].cy;
+        }
+#pragma unroll
+        for (int l = 0; l < kMaxLevels; ++l) rng[l] = v.iranges[l * S_cap + s];
     }
-    // 8 groups x 27 entries: each group adds every 8th tile in FP64
-    if (tid < 8 * 27) {
-        const int k = tid % 27, g = tid / 27;
-        double acc = 0.0;
-        for (int t = g; t < cnt; t += 8) acc += double(src[size_t(t) * 54 + 2 * k]) + double(src[size_t(t) * 54 + 2 * k + 1]);
-        sm[g * 27 + k] = acc;
+    // partial pairs as float4 (two entries each): thread (g, q) adds, in FP64 and in tile
+    // order, entries 2q and 2q + 1 of tiles g, g + 18, g + 36, ...; 8 tiles' loads in flight
+    constexpr int kGroups = kIcpThreads / 14;   // 18
+    const int q = tid % 14, g = tid / 14;
+    if (g < kGroups) {
+        const float4* src = reinterpret_cast<const float4*>(v.partials + size_t(begin) * kIcpPartialStride) + q;
+        double a0 = 0.0, a1 = 0.0;
+        for (int t = g; t < cnt; t += 8 * kGroups) {
+            float4 p[8];
+#pragma unroll
+            for (int u = 0; u < 8; ++u)
+                p[u] = t + kGroups * u < cnt ? __ldcg(src + size_t(t + kGroups * u) * (kIcpPartialStride / 4))
+                                             : make_float4(0.f, 0.f, 0.f, 0.f);
+#pragma unroll
+            for (int u = 0; u < 8; ++u)
+                if (t + kGroups * u < cnt) {
+                    a0 += double(p[u].x) + double(p[u].y);
+                    a1 += double(p[u].z) + double(p[u].w);
+                }
+        }
+        sm[g * 28 + 2 * q] = a0;
+        sm[g * 28 + 2 * q + 1] = a1;
     }
     __syncthreads();
-    if (tid == 0) {
-        double tot[27];
-        for (int k = 0; k < 27; ++k) {
-            double a = 0.0;
-            for (int g = 0; g < 8; ++g) a += sm[g * 27 + k];
-            tot[k] = a;
-        }
-        double ata[36], atb[6];
+    if (tid < 27) {
+        double a = 0.0;
+        for (int r = 0; r < kGroups; ++r) a += sm[r * 28 + tid];
+        sm[kGroups * 28 + tid] = a;
+    }
+    __syncthreads();
+    if (tid >= 32) return;
+    const double* tot = sm + kGroups * 28;
+    double ata[36], atb[6];
+    {
         int k = 0;
+#pragma unroll
         for (int r = 0; r < 6; ++r)
+#pragma unroll
             for (int c = r; c < 6; ++c) { ata[r * 6 + c] = tot[k]; ata[c * 6 + r] = tot[k]; ++k; }
+#pragma unroll
         for (int r = 0; r < 6; ++r) atb[r] = tot[21 + r];
-        double x[6];
-        if (!cholesky6(ata, atb, x)) {
+    }
+    double x[6];
+    const bool solved = cholesky6(ata, atb, x);   // warp-uniform
+    if (!solved) {
+        if (lane == 0) {
             // the reference throws (project/src/icp.cpp:67-73): keep the previous pose, no fusion
             P->status = KF_ERR_NONFINITE;
             P->level = -1;
             P->cont = 0;
-            __threadfence();
-        } else {
-            double dR[9], R0[9], t0[3];
-            for (int q = 0; q < 9; ++q) R0[q] = P->R[q];
-            for (int q = 0; q < 3; ++q) t0[q] = P->t[q];
-            euler_yxz(x[0], x[1], x[2], dR);
-            // R <- dR^T R, t <- dR^T t + dt (ICP::updatePose, project/src/icp.cpp:85-86)
-            double dRt[9];
-            for (int c = 0; c < 3; ++c)
-                for (int r = 0; r < 3; ++r) dRt[c * 3 + r] = dR[r * 3 + c];
-            for (int c = 0; c < 3; ++c) m3d_vec(dRt, R0 + 3 * c, P->R + 3 * c);
-            double nt[3];
-            m3d_vec(dRt, t0, nt);
-            for (int q = 0; q < 3; ++q) P->t[q] = nt[q] + x[3 + q];
-            P->iters[level] += 1;
-            // poseError(previous estimate, new estimate) (project/src/general_helper.cpp:11-21)
-            const double iv = 0.57735026918962576451;
-            double a0[3], a1[3], vv[3] = {iv, iv, iv};
-            m3d_vec(R0, vv, a0);
-            m3d_vec(P->R, vv, a1);
-            const double ang = sqrt((a0[0] - a1[0]) * (a0[0] - a1[0]) + (a0[1] - a1[1]) * (a0[1] - a1[1]) +
-                                    (a0[2] - a1[2]) * (a0[2] - a1[2]));
-            const double dist = sqrt((t0[0] - P->t[0]) * (t0[0] - P->t[0]) + (t0[1] - P->t[1]) * (t0[1] - P->t[1]) +
-                                     (t0[2] - P->t[2]) * (t0[2] - P->t[2]));
-            int it = P->it + 1;
-            int lvl = level;
-            if ((ang < double(S->stop_a) && dist < double(S->stop_d)) || it >= S->iters[level]) {
-                lvl = next_level(S, level - 1);
-                it = 0;
-            }
-            P->it = it;
-            P->level = lvl;
-            if (lvl >= 0) publish_pass(P, S->lv[lvl]);
-            P->cont = lvl >= 0 ? 1 : 0;
+            v.icp_sched[s] = make_int4(-1, 0, 0, 0);
             __threadfence();
         }
+        return;
     }
-    __syncthreads();
+    // sin / cos of beta (x[0]), gamma (x[1]), alpha (x[2]) on lanes 0, 1, 2
+    double sn = 0.0, cs = 1.0;
+    if (lane < 3) sincos(x[lane], &sn, &cs);
+    const double sx = __shfl_sync(0xffffffffu, sn, 0), cx = __shfl_sync(0xffffffffu, cs, 0);
+    const double sy = __shfl_sync(0xffffffffu, sn, 1), cy = __shfl_sync(0xffffffffu, cs, 1);
+    const double sz = __shfl_sync(0xffffffffu, sn, 2), cz = __shfl_sync(0xffffffffu, cs, 2);
+    double dR[9], R1[9], t1[3];
+    euler_yxz_sc(sx, cx, sy, cy, sz, cz, dR);
+    // R <- dR^T R, t <- dR^T t + dt (ICP::updatePose, project/src/icp.cpp:85-86)
+    double dRt[9];
+#pragma unroll
+    for (int c = 0; c < 3; ++c)
+#pragma unroll
+        for (int r = 0; r < 3; ++r) dRt[c * 3 + r] = dR[r * 3 + c];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) m3d_vec(dRt, R0 + 3 * c, R1 + 3 * c);
+    double nt[3];
+    m3d_vec(dRt, t0, nt);
+#pragma unroll
+    for (int r = 0; r < 3; ++r) t1[r] = nt[r] + x[3 + r];
+    // poseError(previous estimate, new estimate) (project/src/general_helper.cpp:11-21)
+    const double iv = 0.57735026918962576451;
+    double a0[3], a1[3], vv[3] = {iv, iv, iv};
+    m3d_vec(R0, vv, a0);
+    m3d_vec(R1, vv, a1);
+    const double ang = sqrt((a0[0] - a1[0]) * (a0[0] - a1[0]) + (a0[1] - a1[1]) * (a0[1] - a1[1]) +
+                            (a0[2] - a1[2]) * (a0[2] - a1[2]));
+    const double dist = sqrt((t0[0] - t1[0]) * (t0[0] - t1[0]) + (t0[1] - t1[1]) * (t0[1] - t1[1]) +
+                             (t0[2] - t1[2]) * (t0[2] - t1[2]));
+    int it = it0 + 1;
+    int lvl = level;
+    if ((ang < double(stop_a) && dist < double(stop_d)) || it >= siters[level]) {
+        lvl = level - 1;   // next level with iterations (next_level)
+        while (lvl >= 0 && siters[lvl] <= 0) --lvl;
+        it = 0;
+    }
+    if (lane != 0) return;
+#pragma unroll
+    for (int r = 0; r < 9; ++r) P->R[r] = R1[r];
+#pragma unroll
+    for (int r = 0; r < 3; ++r) P->t[r] = t1[r];
+    P->iters[level] = done0 + 1;
+    P->it = it;
+    P->level = lvl;
+    P->cont = lvl >= 0 ? 1 : 0;
+    if (lvl >= 0) {
+        float* m = v.icp_mats + size_t(s) * 24;
+#pragma unroll
+        for (int r = 0; r < 9; ++r) m[r] = float(R1[r]);
+#pragma unroll
+        for (int r = 0; r < 3; ++r) m[9 + r] = float(t1[r]);
+        // M = K_l * Rp^T (as publish_mats)
+#pragma unroll
+        for (int col = 0; col < 3; ++col) {
+            const double b0 = Rp[col], b1 = Rp[3 + col], b2 = Rp[6 + col];
+            m[12 + col * 3 + 0] = float(double(lfx[lvl]) * b0 + double(lcx[lvl]) * b2);
+            m[12 + col * 3 + 1] = float(double(lfy[lvl]) * b1 + double(lcy[lvl]) * b2);
+            m[12 + col * 3 + 2] = float(b2);
+        }
+#pragma unroll
+        for (int r = 0; r < 3; ++r) m[21 + r] = tpf[r];
+        v.icp_sched[s] = make_int4(lvl, rng[lvl].begin, rng[lvl].end - rng[lvl].begin, 0);
+    } else {
+        v.icp_sched[s] = make_int4(-1, 0, 0, 0);
+    }
+    __threadfence();
 }
 
 // phase C for one session (one thread): the frame's pose becomes the previous pose; the
@@ -329,94 +510,120 @@ __device__ void icp_finish(const SessionDev* S, const StepDev st, OutDev* out) {
     __threadfence();
 }
 
+// In-place inclusive scan of a[0..n) in shared memory by the whole block (n <= 1024).
+__device__ void block_inclusive_scan(int* a, int n, int* warp_tot) {
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nthreads = blockDim.x;
+    const int per = (n + nthreads - 1) / nthreads;
+    const int lo = min(n, tid * per), hi = min(n, lo + per);
+    int run = 0;
+    for (int i = lo; i < hi; ++i) run += a[i];
+    int incl = run;
+#pragma unroll
+    for (int off = 1; off < 32; off <<= 1) {
+        const int y = __shfl_up_sync(0xffffffffu, incl, off);
+        if (lane >= off) incl += y;
+    }
+    if (lane == 31) warp_tot[warp] = incl;
+    __syncthreads();
+    if (tid == 0) {
+        int acc = 0;
+        for (int w = 0; w < (nthreads >> 5); ++w) { const int x = warp_tot[w]; warp_tot[w] = acc; acc += x; }
+    }
+    __syncthreads();
+    int base = warp_tot[warp] + incl - run;   // exclusive prefix of this thread's chunk
+    for (int i = lo; i < hi; ++i) { base += a[i]; a[i] = base; }
+    __syncthreads();
+}
+
 // ---- the persistent cooperative kernel ----
 
 constexpr int kIcpMaxSessionsSmem = 1024;
+constexpr int kIcpPixelsPerStep = 4;   // pixels a thread carries through one pipelined step
 
-__global__ void __launch_bounds__(kIcpThreads) icp_kernel(EngineView v, int stage_tiles) {
-    extern __shared__ float stage[];   // stage_tiles * 54 floats: one session's tile pairs
+__global__ void __launch_bounds__(kIcpThreads, 1) icp_kernel(EngineView v) {
     __shared__ float red[8 * 32 * 2];
-    __shared__ double dsm[8 * 27];
+    __shared__ double dsm[(kIcpThreads / 14 + 1) * 28];
     __shared__ float mats[24];
-    __shared__ int s_pre[kIcpMaxSessionsSmem + 1];
-    __shared__ int s_lvl[kIcpMaxSessionsSmem];
-    __shared__ int s_any;
+    __shared__ int s_pre[kIcpMaxSessionsSmem + 1];   // tiles of sessions before s in this pass
+    __shared__ short s_lvl[kIcpMaxSessionsSmem];
+    __shared__ int s_beg[kIcpMaxSessionsSmem];
+    __shared__ int s_wtot[kIcpThreads / 32];
     const int tid = threadIdx.x;
     const unsigned int nb = gridDim.x;
     unsigned int epoch = 0;
     const int S_cap = v.tb->S;
 
     for (int s = blockIdx.x; s < S_cap; s += gridDim.x)
-        if (tid == 0) icp_begin(&v.sess[s], v.step[s]);
+        if (tid == 0) icp_begin(v, s);
     if (!grid_barrier(v.sync, nb, epoch)) return;
 
     for (int pass = 0; pass < kIcpMaxPasses; ++pass) {
-        // which sessions iterate in this pass, at which level; virtual tile prefix
-        if (tid == 0) s_any = 0;
-        __syncthreads();
+        // which sessions iterate in this pass, at which level, with which tiles
         for (int s = tid; s < S_cap; s += blockDim.x) {
-            int cnt = 0, lvl = -1;
-            const StepDev st = v.step[s];
-            if (st.active && !st.first && ldcg(&v.sess[s].pose->cont)) {
-                lvl = ldcg(&v.sess[s].pose->level);
-                const IcpRange rg = v.iranges[lvl * S_cap + s];
-                cnt = rg.end - rg.begin;
-                s_any = 1;
-            }
-            s_lvl[s] = lvl;
-            s_pre[s + 1] = cnt;
+            const int4 e = __ldcg(v.icp_sched + s);
+            s_lvl[s] = short(e.x);
+            s_beg[s] = e.y;
+            s_pre[s + 1] = e.x >= 0 ? e.z : 0;
         }
+        if (tid == 0) s_pre[0] = 0;
         __syncthreads();
-        if (!s_any) break;   // block-uniform: every block sees the same flags
-        if (tid == 0) {
-            s_pre[0] = 0;
-            for (int s = 0; s < S_cap; ++s) s_pre[s + 1] += s_pre[s];
-        }
-        __syncthreads();
+        block_inclusive_scan(s_pre + 1, S_cap, s_wtot);
         const int total = s_pre[S_cap];
+        if (total == 0) break;   // block-uniform: every block reads the same schedule
 
-        // phase A
-        for (int vt = blockIdx.x; vt < total; vt += gridDim.x) {
-            int lo = 0, hi = S_cap;
-            while (hi - lo > 1) {
-                const int mid = (lo + hi) >> 1;
-                if (s_pre[mid] <= vt) lo = mid; else hi = mid;
-            }
-            const int s = lo, lvl = s_lvl[s];
-            const int abs_t = v.iranges[lvl * S_cap + s].begin + (vt - s_pre[s]);
-            const IcpTile T = v.itiles[abs_t];
-            const SessionDev* S = &v.sess[s];
-            const PoseDev* P = S->pose;
-            if (tid < 9) mats[tid] = ldcg(&P->Rf[tid]);
-            else if (tid < 12) mats[tid] = ldcg(&P->tf[tid - 9]);
-            else if (tid < 21) mats[tid] = ldcg(&P->M[tid - 12]);
-            else if (tid < 24) mats[tid] = ldcg(&P->tpf[tid - 21]);
-            __syncthreads();
-            const LevelDev& Lv = S->lv[lvl];
-            const float4* vm = S->vmap[lvl];
-            const float4* tv = S->pv[lvl];
-            const float4* tn = S->pn[lvl];
-            uint8_t* mask = S->mask[lvl];
+        // phase A: tiles of every iterating session, round robin over the grid.  A block
+        // accumulates all its tiles of a session and stores one partial, in slot j mod grid
+        // of the session (j: the session's tile index), so a session's partials and their
+        // summation order depend on its own tiles only, not on the other sessions of a batch.
+        {
+            int run_s = -1, run_slot = 0;
             float acc[32];
 #pragma unroll
             for (int q = 0; q < 32; ++q) acc[q] = 0.f;
-            const float dist = S->dist_th, ang = S->angle_th;
+            for (int vt = blockIdx.x; vt < total; vt += gridDim.x) {
+                int lo = 0, hi = S_cap;
+                while (hi - lo > 1) {
+                    const int mid = (lo + hi) >> 1;
+                    if (s_pre[mid] <= vt) lo = mid; else hi = mid;
+                }
+                const int s = lo, lvl = s_lvl[s];
+                if (s != run_s) {
+                    if (run_s >= 0) {
+                        block_reduce_store(acc, red, v.partials + size_t(s_beg[run_s] + run_slot) * kIcpPartialStride);
+#pragma unroll
+                        for (int q = 0; q < 32; ++q) acc[q] = 0.f;
+                    }
+                    run_s = s;
+                    run_slot = vt - s_pre[s];
+                    if (tid < 24) mats[tid] = ldcg(v.icp_mats + size_t(s) * 24 + tid);
+                    __syncthreads();
+                }
+                const IcpTile T = v.itiles[s_beg[s] + (vt - s_pre[s])];
+                const SessionDev* S = &v.sess[s];
+                const LevelDev& Lv = S->lv[lvl];
+                const float4* vm = S->vmap[lvl];
+                const float4* tv = S->pv[lvl];
+                const float4* tn = S->pn[lvl];
+                uint8_t* mask = S->mask[lvl];
+                const float dist = S->dist_th, ang = S->angle_th;
+                const IcpMats m{mats, mats + 9, mats + 12, mats + 21};
+                const int pend = T.p0 + T.np;
 #pragma unroll 1
-            for (int p = T.p0 + tid; p < T.p0 + T.np; p += kIcpThreads) {
-                const int u = p % Lv.icw, vv = p / Lv.icw;
-                float a[6], b;
-                const bool ok = icp_pixel(vm, tv, tn, Lv.w, Lv.h, u, vv, mats, mats + 9, mats + 12, mats + 21, dist,
-                                          ang, a, b);
-                if (mask) mask[size_t(vv) * Lv.w + u] = ok ? 1 : 0;
-                if (ok) accumulate_products(acc, a, b);
+                for (int p = T.p0 + tid; p < pend; p += kIcpPixelsPerStep * kIcpThreads)
+                    icp_multi<kIcpPixelsPerStep>(vm, tv, tn, Lv.w, Lv.h, Lv.icw, p, pend, m, dist, ang, mask,
+                                                 [&](const float (&a)[6], float b) { accumulate_products(acc, a, b); });
             }
-            block_reduce_store(acc, red, v.partials + size_t(abs_t) * 54);
+            if (run_s >= 0)
+                block_reduce_store(acc, red, v.partials + size_t(s_beg[run_s] + run_slot) * kIcpPartialStride);
         }
         if (!grid_barrier(v.sync, nb, epoch)) return;
 
-        // phase B
-        for (int s = blockIdx.x; s < S_cap; s += gridDim.x)
-            if (s_lvl[s] >= 0) icp_solve(v, s, dsm, stage, stage_tiles);
+        // phase B: the block that owns a session solves it
+        for (int s = blockIdx.x; s < S_cap; s += gridDim.x) {
+            if (s_lvl[s] < 0) continue;
+            icp_solve(v, s, s_lvl[s], s_beg[s], min(s_pre[s + 1] - s_pre[s], int(gridDim.x)), dsm);
+            __syncthreads();
+        }
         if (!grid_barrier(v.sync, nb, epoch)) return;
     }
 
@@ -443,11 +650,8 @@ cudaError_t launch_barrier_selftest(GridSync* g, unsigned long long timeout_ns, 
 }
 
 cudaError_t launch_icp(const EngineView& v, int grid, cudaStream_t st) {
-    // tiles per session-level are at most about one per block (see the tile table)
-    int stage_tiles = grid + 8 < 160 ? grid + 8 : 160;   // <= 34.6 KB, under the 48 KB default
-    const size_t smem = sizeof(float) * 54 * size_t(stage_tiles);
-    void* args[] = {const_cast<EngineView*>(&v), &stage_tiles};
-    return cudaLaunchCooperativeKernel((const void*)icp_kernel, dim3(grid), dim3(kIcpThreads), args, smem, st);
+    void* args[] = {const_cast<EngineView*>(&v)};
+    return cudaLaunchCooperativeKernel((const void*)icp_kernel, dim3(grid), dim3(kIcpThreads), args, 0, st);
 }
 
 // ---- stage: kernel::constructIcpResiduals (A rows and b to HBM, as the reference) ----

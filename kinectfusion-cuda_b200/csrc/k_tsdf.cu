@@ -4,20 +4,21 @@
 // (project/src/tsdf.cu:20-75), which walks one (x, y) voxel column per thread through a
 // cudaArray surface with 4-byte reads and writes, projecting every voxel of the volume.
 //
-// Here the volume is two linear arrays in HBM (distance, weight; x fastest).  A warp owns a
-// 32 x 8 x 8 block of voxels at a time:
-//   - The block is first tested as a whole from its 8 projected corners (the projection of a
-//     box in front of the camera lies inside its corners' bounding box): outside the depth
-//     range or the image, no valid depth under it, or every voxel more than mu behind the
-//     farthest valid depth under it -- then no voxel of it can update and it is skipped.
-//   - Otherwise its 64 rows are walked four at a time with one voxel per lane along x, so
-//     every depth gather and volume access of the warp touches 32 consecutive voxels, and a
-//     lane reads and writes the volume only for voxels that update.
-//   - Each 8^3 brick keeps a lower bound of its distances (an atomic minimum of every value
-//     fusion stores), and a small pass widens it to the 2 x 2 x 2 bricks a trilinear sample
-//     can touch; the raycaster skips samples whose bound proves they cannot matter.
-// Blocks of every session of a batch are handed to persistent warps through one atomic
-// counter.
+// Here the volume is two linear arrays in HBM (distance, weight; x fastest), cut into
+// 32 x 8 x 8 voxel blocks.  Two launches per frame:
+//   - fuse_cull_kernel tests every block of every session as a whole, one block per thread,
+//     from its 8 projected corners (the projection of a box in front of the camera lies
+//     inside its corners' bounding box): outside the depth range or the image, no valid depth
+//     under it, or every voxel more than mu behind the farthest valid depth under it -- then
+//     no voxel of it can update.  The surviving blocks (a few percent of a 512^3 volume) are
+//     appended to a queue with one atomic per warp.
+//   - fuse_kernel's persistent warps take queue entries a quarter block (16 rows) at a time
+//     and walk the rows four at a time with one voxel per lane along x, so every depth gather
+//     and volume access of the warp touches 32 consecutive voxels, and a lane reads and
+//     writes the volume only for voxels that update.
+// Each 8^3 brick keeps a lower bound of its distances (an atomic minimum of every value
+// fusion stores), and a small pass widens it to the 2 x 2 x 2 bricks a trilinear sample can
+// touch; the raycaster skips samples whose bound proves they cannot matter.
 #include "kf_host.h"
 
 namespace kf {
@@ -53,34 +54,38 @@ __device__ __forceinline__ void fuse_update(float& F, float& Wt, float fn, float
     Wt = w1;
 }
 
-// true when no voxel of the block [x0, x0+32) x [j0, j0+8) x [k0, k0+8) can update
-__device__ __forceinline__ bool block_culled(const FuseCtx& c, int x0, int j0, int k0, int lane) {
+// true when no voxel of the block [x0, x0+32) x [j0, j0+8) x [k0, k0+8) can update; one
+// thread tests one block
+__device__ __forceinline__ bool block_culled(const FuseCtx& c, int x0, int j0, int k0) {
     const int n = c.n;
-    const int q = lane & 7;
-    const float x = __ldg(c.xs + ((q & 1) ? min(x0 + 31, n - 1) : x0));
-    const float y = __ldg(c.xs + ((q & 2) ? min(j0 + 7, n - 1) : j0));
-    const float z = __ldg(c.zs + ((q & 4) ? min(k0 + 7, n - 1) : k0));
-    // same operation order as the per-voxel projection below
-    const float bx = c.iR[3] * y + c.iR[6] * z + c.it[0];
-    const float by = c.iR[4] * y + c.iR[7] * z + c.it[1];
-    const float bz = c.iR[5] * y + c.iR[8] * z + c.it[2];
-    const float ex = c.iR[0] * x + bx, ey = c.iR[1] * x + by, ez = c.iR[2] * x + bz;
-    float zmin = ez, zmax = ez;
+    const float xa = __ldg(c.xs + x0), xb = __ldg(c.xs + min(x0 + 31, n - 1));
+    const float ya = __ldg(c.xs + j0), yb = __ldg(c.xs + min(j0 + 7, n - 1));
+    const float za = __ldg(c.zs + k0), zb = __ldg(c.zs + min(k0 + 7, n - 1));
+    float ex[8], ey[8], ez[8];
+    float zmin = 3.0e38f, zmax = -3.0e38f;
 #pragma unroll
-    for (int off = 4; off >= 1; off >>= 1) {
-        zmin = fminf(zmin, __shfl_xor_sync(0xffffffffu, zmin, off));
-        zmax = fmaxf(zmax, __shfl_xor_sync(0xffffffffu, zmax, off));
+    for (int q = 0; q < 8; ++q) {
+        const float x = (q & 1) ? xb : xa, y = (q & 2) ? yb : ya, z = (q & 4) ? zb : za;
+        // same operation order as the per-voxel projection below
+        const float bx = c.iR[3] * y + c.iR[6] * z + c.it[0];
+        const float by = c.iR[4] * y + c.iR[7] * z + c.it[1];
+        const float bz = c.iR[5] * y + c.iR[8] * z + c.it[2];
+        ex[q] = c.iR[0] * x + bx;
+        ey[q] = c.iR[1] * x + by;
+        ez[q] = c.iR[2] * x + bz;
+        zmin = fminf(zmin, ez[q]);
+        zmax = fmaxf(zmax, ez[q]);
     }
     if (zmax < c.min_d - 1e-4f || zmin >= c.max_d + 1e-4f) return true;
     if (!(zmin > 1e-3f)) return false;   // a corner behind the camera: no image bound
-    float px = (c.fx * ex + c.cx * ez) / ez, py = (c.fy * ey + c.cy * ez) / ez;
-    float pxmin = px, pxmax = px, pymin = py, pymax = py;
+    float pxmin = 3.0e38f, pxmax = -3.0e38f, pymin = 3.0e38f, pymax = -3.0e38f;
 #pragma unroll
-    for (int off = 4; off >= 1; off >>= 1) {
-        pxmin = fminf(pxmin, __shfl_xor_sync(0xffffffffu, pxmin, off));
-        pxmax = fmaxf(pxmax, __shfl_xor_sync(0xffffffffu, pxmax, off));
-        pymin = fminf(pymin, __shfl_xor_sync(0xffffffffu, pymin, off));
-        pymax = fmaxf(pymax, __shfl_xor_sync(0xffffffffu, pymax, off));
+    for (int q = 0; q < 8; ++q) {
+        const float px = (c.fx * ex[q] + c.cx * ez[q]) / ez[q], py = (c.fy * ey[q] + c.cy * ez[q]) / ez[q];
+        pxmin = fminf(pxmin, px);
+        pxmax = fmaxf(pxmax, px);
+        pymin = fminf(pymin, py);
+        pymax = fmaxf(pymax, py);
     }
     if (pxmax < -0.01f || pxmin > float(c.w) + 0.01f || pymax < -0.01f || pymin > float(c.h) + 0.01f) return true;
     if (!c.dmax) return false;
@@ -88,28 +93,36 @@ __device__ __forceinline__ bool block_culled(const FuseCtx& c, int x0, int j0, i
     const int tx1 = min(max(int(pxmax + 0.01f), 0), c.w - 1) >> 4;
     const int ty0 = min(max(int(pymin - 0.01f), 0), c.h - 1) >> 4;
     const int ty1 = min(max(int(pymax + 0.01f), 0), c.h - 1) >> 4;
-    const int nx = tx1 - tx0 + 1, ntile = nx * (ty1 - ty0 + 1);
-    if (ntile > 512) return false;
+    if ((tx1 - tx0 + 1) * (ty1 - ty0 + 1) > 512) return false;
     float dm = 0.0f;
-    for (int t = lane; t < ntile; t += 32) dm = fmaxf(dm, __ldg(c.dmax + size_t(ty0 + t / nx) * c.t16w + tx0 + t % nx));
-#pragma unroll
-    for (int off = 16; off >= 1; off >>= 1) dm = fmaxf(dm, __shfl_xor_sync(0xffffffffu, dm, off));
+    for (int ty = ty0; ty <= ty1; ++ty)
+        for (int tx = tx0; tx <= tx1; ++tx) dm = fmaxf(dm, __ldg(c.dmax + size_t(ty) * c.t16w + tx));
     // every voxel meets either an invalid depth or d - z <= dm - zmin < -mu
     return dm == 0.0f || zmin > dm + c.mu + 1e-4f;
 }
 
-// fuseKernel (project/src/tsdf.cu:28-74) for the 64 rows of one block, lanes along x
+// block coordinates of fusion unit u of an n^3 volume (units: 32 x 8 x 8 blocks, x fastest)
+__device__ __forceinline__ void unit_origin(int n, int u, int& x0, int& j0, int& k0) {
+    const int ux = (n + 31) >> 5, uy = (n + 7) >> 3;
+    x0 = (u % ux) * 32;
+    j0 = ((u / ux) % uy) * 8;
+    k0 = (u / (ux * uy)) * 8;
+}
+
+// fuseKernel (project/src/tsdf.cu:28-74) for rows [r_begin, r_end) of one block (row r is
+// y = j0 + r % 8, z = k0 + r / 8), lanes along x
 template <class TF, class TW>
-__device__ __forceinline__ void fuse_block(const FuseCtx& c, int x0, int j0, int k0, int lane) {
+__device__ __forceinline__ void fuse_block(const FuseCtx& c, int x0, int j0, int k0, int r_begin, int r_end, int lane) {
     const int n = c.n;
     const int x = x0 + lane;
     const bool lane_in = x < n;
     const float xv = __ldg(c.xs + min(x, n - 1));
-    const int jn = min(8, n - j0), kn = min(8, n - k0), rows = jn * kn;
+    const int jn = min(8, n - j0), kn = min(8, n - k0);
+    const int rows = min(r_end, jn * kn);
     int kmin = 0x7fffffff;   // key of the smallest distance this lane stores
     TF* F = static_cast<TF*>(c.F);
     TW* Wa = static_cast<TW*>(c.W);
-    for (int r0 = 0; r0 < rows; r0 += 4) {
+    for (int r0 = r_begin; r0 < rows; r0 += 4) {
         int pix[4];
         float pz[4], d[4];
         unsigned int cand = 0;
@@ -196,16 +209,11 @@ __device__ __forceinline__ void fuse_block(const FuseCtx& c, int x0, int j0, int
     }
 }
 
-__device__ __forceinline__ void fuse_unit(const FuseCtx& c, long long u, int lane) {
-    const int ux = (c.n + 31) / 32, uy = (c.n + 7) / 8;
-    const int x0 = int(u % ux) * 32;
-    const int j0 = int((u / ux) % uy) * 8;
-    const int k0 = int(u / ((long long)ux * uy)) * 8;
-    if (block_culled(c, x0, j0, k0, lane)) return;
+__device__ __forceinline__ void fuse_rows(const FuseCtx& c, int x0, int j0, int k0, int r_begin, int r_end, int lane) {
     if (c.fmt == KF_TSDF_F16U16)
-        fuse_block<__half, uint16_t>(c, x0, j0, k0, lane);
+        fuse_block<__half, uint16_t>(c, x0, j0, k0, r_begin, r_end, lane);
     else
-        fuse_block<float, float>(c, x0, j0, k0, lane);
+        fuse_block<float, float>(c, x0, j0, k0, r_begin, r_end, lane);
 }
 
 __device__ void load_ctx(const SessionDev* S, FuseCtx& c) {
@@ -221,46 +229,86 @@ __device__ void load_ctx(const SessionDev* S, FuseCtx& c) {
     c.F = S->tf; c.W = S->tw; c.xs = S->xs; c.zs = S->zs; c.bmin = S->bmin;
 }
 
-constexpr int kFuseChunk = 2;   // blocks a warp takes per atomic
+// session of global fusion unit g (binary search over the per-slot prefix)
+__device__ __forceinline__ int unit_session(const EngineView& v, long long g, int S_cap) {
+    int lo = 0, hi = S_cap;
+    while (hi - lo > 1) {
+        const int mid = (lo + hi) >> 1;
+        if (__ldg(v.fuse_prefix + mid) <= g) lo = mid; else hi = mid;
+    }
+    return lo;
+}
+
+// one thread per block of every stepping session: append the blocks that can update to the
+// queue (counters[4] = entries), one atomic per warp
+__global__ void __launch_bounds__(256) fuse_cull_kernel(EngineView v) {
+    const long long total = v.tb->fuse_total;
+    const int S_cap = v.tb->S;
+    const int lane = threadIdx.x & 31;
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    FuseCtx c;
+    int cur_s = -1;
+    bool live = false;
+    for (long long base = (long long)blockIdx.x * blockDim.x + (threadIdx.x & ~31); base < total; base += stride) {
+        const long long g = base + lane;
+        bool keep = false;
+        if (g < total) {
+            const int s = unit_session(v, g, S_cap);
+            if (s != cur_s) {
+                cur_s = s;
+                const SessionDev* S = &v.sess[s];
+                live = v.step[s].active && S->pose->fuse_ok;
+                if (live) load_ctx(S, c);
+            }
+            if (live) {
+                int x0, j0, k0;
+                unit_origin(c.n, int(g - __ldg(v.fuse_prefix + s)), x0, j0, k0);
+                keep = !block_culled(c, x0, j0, k0);
+            }
+        }
+        const unsigned int m = __ballot_sync(0xffffffffu, keep);
+        if (m == 0) continue;
+        unsigned int slot = 0;
+        if (lane == 0) slot = atomicAdd(&v.counters[4], unsigned(__popc(m)));
+        slot = __shfl_sync(0xffffffffu, slot, 0);
+        const unsigned int at = slot + __popc(m & ((1u << lane) - 1u));
+        if (keep && at < unsigned(v.fuseq_cap)) v.fuseq[at] = unsigned(g);   // capacity >= all blocks
+    }
+}
+
 constexpr int kFuseWarps = 8;
+constexpr int kFuseSplit = 4;    // queue entries are taken a quarter block (16 rows) at a time
 
 __global__ void __launch_bounds__(256, 4) fuse_kernel(EngineView v) {
     __shared__ FuseCtx ctx[kFuseWarps];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const long long total = v.tb->fuse_total;
     const int S_cap = v.tb->S;
-    unsigned long long* ctr = reinterpret_cast<unsigned long long*>(v.counters + 2);
+    const unsigned int items = min(__ldcg(&v.counters[4]), unsigned(v.fuseq_cap)) * kFuseSplit;
     FuseCtx& c = ctx[warp];
     int cur_s = -1;
-    bool live = false;
     while (true) {
-        unsigned long long g0 = 0;
-        if (lane == 0) g0 = atomicAdd(ctr, (unsigned long long)kFuseChunk);
-        g0 = __shfl_sync(0xffffffffu, g0, 0);
-        if ((long long)g0 >= total) break;
-        for (int q = 0; q < kFuseChunk; ++q) {
-            const long long g = (long long)g0 + q;
-            if (g >= total) break;
-            int lo = 0, hi = S_cap;   // session of block g (warp-uniform binary search)
-            while (hi - lo > 1) {
-                const int mid = (lo + hi) >> 1;
-                if (__ldg(v.fuse_prefix + mid) <= g) lo = mid; else hi = mid;
-            }
-            if (lo != cur_s) {
-                cur_s = lo;
-                const SessionDev* S = &v.sess[lo];
-                live = v.step[lo].active && S->pose->fuse_ok;
-                __syncwarp();
-                if (live && lane == 0) load_ctx(S, c);
-                __syncwarp();
-            }
-            if (!live) continue;
-            fuse_unit(c, g - __ldg(v.fuse_prefix + lo), lane);
+        unsigned int i = 0;
+        if (lane == 0) i = atomicAdd(&v.counters[5], 1u);
+        i = __shfl_sync(0xffffffffu, i, 0);
+        if (i >= items) break;
+        const long long g = __ldcg(v.fuseq + i / kFuseSplit);
+        const int part = int(i % kFuseSplit);
+        const int s = unit_session(v, g, S_cap);
+        if (s != cur_s) {
+            cur_s = s;
+            __syncwarp();
+            if (lane == 0) load_ctx(&v.sess[s], c);
+            __syncwarp();
         }
+        int x0, j0, k0;
+        unit_origin(c.n, int(g - __ldg(v.fuse_prefix + s)), x0, j0, k0);
+        fuse_rows(c, x0, j0, k0, part * (64 / kFuseSplit), (part + 1) * (64 / kFuseSplit), lane);
     }
 }
 
 cudaError_t launch_fuse(const EngineView& v, int grid, cudaStream_t st) {
+    const int cull_grid = grid;   // grid-stride over all blocks of all sessions
+    fuse_cull_kernel<<<cull_grid, 256, 0, st>>>(v);
     fuse_kernel<<<grid, 256, 0, st>>>(v);
     return cudaGetLastError();
 }
@@ -413,11 +461,28 @@ cudaError_t launch_rebuild_bricks(const void* f, int fmt, int n, int* bmin, int*
 // ---- stage fusion on a caller volume (kernel::fuse) ----
 
 __global__ void __launch_bounds__(256) fuse_stage_kernel(FuseCtx c) {
-    const long long total = fuse_units(c.n);
+    const int total = fuse_units(c.n);
     const int lane = threadIdx.x & 31;
-    const long long warp = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5;
-    const long long nwarps = ((long long)gridDim.x * blockDim.x) >> 5;
-    for (long long u = warp; u < total; u += nwarps) fuse_unit(c, u, lane);
+    const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int nwarps = (gridDim.x * blockDim.x) >> 5;
+    // each warp tests 32 consecutive blocks (one per lane), then fuses the survivors together
+    for (int base = warp * 32; base < total; base += nwarps * 32) {
+        const int u = base + lane;
+        int x0 = 0, j0 = 0, k0 = 0;
+        bool keep = false;
+        if (u < total) {
+            unit_origin(c.n, u, x0, j0, k0);
+            keep = !block_culled(c, x0, j0, k0);
+        }
+        unsigned int m = __ballot_sync(0xffffffffu, keep);
+        while (m) {
+            const int q = __ffs(m) - 1;
+            m &= m - 1;
+            const int bx = __shfl_sync(0xffffffffu, x0, q), by = __shfl_sync(0xffffffffu, j0, q),
+                      bz = __shfl_sync(0xffffffffu, k0, q);
+            fuse_rows(c, bx, by, bz, 0, 64, lane);
+        }
+    }
 }
 
 cudaError_t stage_fuse(const float* depth, int w, int h, const float* k, const kf_volume* vol, const float* pose,

@@ -29,9 +29,7 @@ struct LevelDev {
 struct PoseDev {
     double R[9], t[3];      // ICP estimate, camera->world, column-major R
     double Rp[9], tp[3];    // pose of the previous frame
-    float Rf[9], tf[3];     // float copy of the estimate for the per-pixel kernels
     float Rpf[9], tpf[3];   // float copy of the previous pose (raycast, correspondence)
-    float M[9];             // K_l * Rp^T for the level the next ICP pass runs at
     float iRf[9], itf[3];   // inverse of the frame's final pose (world->camera) for fusion
     int iters[kMaxLevels];  // ICP iterations run per level in the current frame
     int level;              // level of the next ICP pass (-1 once ICP is finished)

@@ -38,19 +38,25 @@ struct EngineView {
     const long long* fuse_prefix;// S + 1 entries, in segments
     const long long* brick_prefix;// S + 1 entries, in bricks
     const long long* super_prefix;// S + 1 entries, in super-bricks
-    float* partials;             // ICP block partials, 54 floats per tile
+    float* partials;             // ICP tile partials, kIcpPartialStride floats per tile
+    int4* icp_sched;             // per slot: {level of the next ICP pass or -1, first tile, tiles, 0}
+    float* icp_mats;             // per slot: 24 floats phase A reads (R, t, K_l R_prev^T, t_prev)
     GridSync* sync;
-    unsigned int* counters;      // [0] raycast tiles, [2..3] fusion blocks (64-bit),
-                                 // [6] long rays queued, [7] long rays taken
+    unsigned int* counters;      // [0] raycast tiles, [4] fusion blocks queued, [5] fusion
+                                 // items taken, [6] long rays queued, [7] long rays taken
     LongRay* longq;              // long-ray queue
     int longq_cap;
+    unsigned int* fuseq;         // fusion queue: global unit index of each block that can update
+    int fuseq_cap;
 };
 
 constexpr int kPreTileSize = 32;
 constexpr int kRayTileW = 8, kRayTileH = 4;   // one warp per ray tile
 constexpr int kIcpThreads = 256;
 constexpr int kIcpPxPerThread = 8;
-constexpr int kIcpTilePx = kIcpThreads * kIcpPxPerThread;
+constexpr int kIcpTilePx = kIcpThreads * kIcpPxPerThread;   // rows per block of the LLS stage
+constexpr int kIcpTilesPerBlock = 4;  // ICP tiles per session-level per block of the grid
+constexpr int kIcpPartialStride = 56; // floats per ICP tile partial: 27 (sum, compensation) pairs + pad
 constexpr int kIcpMaxPasses = 64;     // hard cap on ICP passes per frame
 
 // launch helpers (each returns the CUDA error of its launch)

@@ -445,6 +445,8 @@ class Batch:
         """frames: list (one per session) of (h, w) uint16 numpy arrays or None to skip.
         Returns (status, poses (n, 4, 4))."""
         n = len(self.configs)
+        if len(frames) != n:
+            raise ValueError("one entry per session: %d for %d sessions" % (len(frames), n))
         keep = []
         ptrs = (ctypes.c_void_p * n)()
         for i, f in enumerate(frames):
