@@ -80,6 +80,10 @@ size_t footprint(const kf_config& c) {
         if (c.export_icp_mask) b += level_px(c, l);
     }
     b += sizeof(float) * 2 * c.volume_n + sizeof(PoseDev);
+    // brick bounds (bmin, bdil), super-brick bounds, depth-tile maxima
+    const size_t nb = size_t(c.volume_n / 8), ns = (nb + 3) / 4;
+    b += nb * nb * nb * 2 * sizeof(int) + ns * ns * ns * sizeof(int);
+    b += sizeof(float) * size_t((c.width + 15) / 16) * ((c.height + 15) / 16);
     return b;
 }
 
@@ -242,10 +246,10 @@ kf_status slot_create(Slot& s, const kf_config& c) {
     KF_ALLOC(d.pose, PoseDev*, sizeof(PoseDev));
     d.nb = c.volume_n / 8;
     d.ns = (d.nb + 3) / 4;
-    const long long nbricks = (long long)d.nb * d.nb * d.nb;
+    const long long nbricks = (long long)d.nb * d.nb * d.nb, nsuper = (long long)d.ns * d.ns * d.ns;
     KF_ALLOC(d.bmin, int*, sizeof(int) * size_t(nbricks));
     KF_ALLOC(d.bdil, int*, sizeof(int) * size_t(nbricks));
-    KF_ALLOC(d.sdil, int*, sizeof(int) * size_t(d.ns) * d.ns * d.ns);
+    KF_ALLOC(d.sdil, int*, sizeof(int) * size_t(nsuper));
 #undef KF_ALLOC
     // grid {f = 2, w = 0} and pose = initial_pose (project/src/kinect_fusion.cpp:33-36, :80)
     err = launch_init_volume(d.tf, d.tw, (long long)n3, d.fmt, 0);

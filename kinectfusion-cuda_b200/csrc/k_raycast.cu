@@ -7,10 +7,10 @@
 // it, and the march does its own trilinear interpolation with the reference's texel mapping
 // (uvw * n - 0.5, clamp).  Every sample the reference takes is taken at the same float
 // position, in the same order; three things make that fast:
-//   - Skipping: a sample whose eight taps lie in cells (32^3 super-bricks, then 8^3 bricks)
-//     whose distance lower bound proves it cannot change the march (>= 0.991 during large
-//     steps, >= 0.001 during small steps) is not evaluated, nor is any later sample in the
-//     same cell; t still advances by the reference's repeated float additions.
+//   - Skipping: a sample whose eight taps lie in cells (32^3 super-bricks during large steps,
+//     then 8^3 bricks) whose distance lower bound proves it cannot change the march (>= 0.991
+//     during large steps, >= 0.001 during small steps) is not evaluated, nor is any later
+//     sample in the same cell; t still advances by the reference's repeated float additions.
 //   - Load balance: each warp pulls 8 x 4-ray tiles from an atomic counter, and a lane marches
 //     at most 64 iterations; longer rays are queued with their exact march state.
 //   - Long rays: a second kernel marches each queued ray with a whole warp, 32 consecutive
@@ -107,6 +107,20 @@ __device__ __forceinline__ bool ray_start(const SessionDev* S, const RayGeo& g, 
     return true;
 }
 
+// t at which the base voxel of the march leaves the voxel box [lo, hi) per axis (0.01 texel
+// inside its faces); faces on the volume's edge do not bound (coordinates clamp there)
+__device__ __forceinline__ float box_exit(const RayGeo& g, int n, int lox, int hix, int loy, int hiy, int loz, int hiz,
+                                          float t_far) {
+    float t = t_far;
+    if (g.tdx > 0.f && hix < n) t = fminf(t, (float(hix) - 0.01f - g.tox) * g.itdx);
+    if (g.tdx < 0.f && lox > 0) t = fminf(t, (float(lox) + 0.01f - g.tox) * g.itdx);
+    if (g.tdy > 0.f && hiy < n) t = fminf(t, (float(hiy) - 0.01f - g.toy) * g.itdy);
+    if (g.tdy < 0.f && loy > 0) t = fminf(t, (float(loy) + 0.01f - g.toy) * g.itdy);
+    if (g.tdz > 0.f && hiz < n) t = fminf(t, (float(hiz) - 0.01f - g.toz) * g.itdz);
+    if (g.tdz < 0.f && loz > 0) t = fminf(t, (float(loz) + 0.01f - g.toz) * g.itdz);
+    return t;
+}
+
 // The reference's march loop for one lane (project/src/raycast.cu:75-117).  Returns 1 when
 // the ray is finished (precise = refined hit distance, 0 for none) and 0 when `budget`
 // iterations ran out with the ray still marching (state kept in st).
@@ -130,27 +144,31 @@ __device__ int march_serial(const SessionDev* S, const RayGeo& g, const TF* f, R
             const int vx = min(max(int(floorf(x)), 0), n - 1);
             const int vy = min(max(int(floorf(y)), 0), n - 1);
             const int vz = min(max(int(floorf(z)), 0), n - 1);
-            const int thr = st.small ? k_small : k_large;
-            int sh = 0, cells = 0;
-            if (__ldg(sdil + (size_t(vz >> 5) * ns + (vy >> 5)) * ns + (vx >> 5)) >= thr) {
-                sh = 5;
-                cells = ns;
-            } else if (__ldg(bdil + (size_t(vz >> 3) * nb + (vy >> 3)) * nb + (vx >> 3)) >= thr) {
-                sh = 3;
-                cells = nb;
+            // the skippable box around the sample's base voxel, in voxels: its super-brick
+            // (large steps), else its brick
+            int lox = 0, hix = 0, loy = 0, hiy = 0, loz = 0, hiz = 0;
+            bool skip = false;
+            if (!st.small) {
+                const int sx = vx >> 5, sy = vy >> 5, sz = vz >> 5;
+                if (__ldg(sdil + (size_t(sz) * ns + sy) * ns + sx) >= k_large) {
+                    lox = sx * 32; hix = lox + 32;
+                    loy = sy * 32; hiy = loy + 32;
+                    loz = sz * 32; hiz = loz + 32;
+                    skip = true;
+                }
             }
-            if (sh) {
-                // skip this sample and every later one whose base voxel stays in the cell
-                // (0.01 texel inside its faces)
-                const int ix = vx >> sh, iy = vy >> sh, iz = vz >> sh;
-                const float fs = float(1 << sh);
-                float t_safe = st.far_d;
-                if (g.tdx > 0.f && ix < cells - 1) t_safe = fminf(t_safe, (fs * float(ix + 1) - 0.01f - g.tox) * g.itdx);
-                if (g.tdx < 0.f && ix > 0) t_safe = fminf(t_safe, (fs * float(ix) + 0.01f - g.tox) * g.itdx);
-                if (g.tdy > 0.f && iy < cells - 1) t_safe = fminf(t_safe, (fs * float(iy + 1) - 0.01f - g.toy) * g.itdy);
-                if (g.tdy < 0.f && iy > 0) t_safe = fminf(t_safe, (fs * float(iy) + 0.01f - g.toy) * g.itdy);
-                if (g.tdz > 0.f && iz < cells - 1) t_safe = fminf(t_safe, (fs * float(iz + 1) - 0.01f - g.toz) * g.itdz);
-                if (g.tdz < 0.f && iz > 0) t_safe = fminf(t_safe, (fs * float(iz) + 0.01f - g.toz) * g.itdz);
+            if (!skip) {
+                const int bx = vx >> 3, by = vy >> 3, bz = vz >> 3;
+                if (__ldg(bdil + (size_t(bz) * nb + by) * nb + bx) >= (st.small ? k_small : k_large)) {
+                    lox = bx * 8; hix = lox + 8;
+                    loy = by * 8; hiy = loy + 8;
+                    loz = bz * 8; hiz = loz + 8;
+                    skip = true;
+                }
+            }
+            if (skip) {
+                // skip this sample and every later one whose base voxel stays in the box
+                const float t_safe = box_exit(g, n, lox, hix, loy, hiy, loz, hiz, st.far_d);
                 do {
                     st.prev_t = st.t;
                     st.t += inc;
@@ -170,7 +188,11 @@ __device__ int march_serial(const SessionDev* S, const RayGeo& g, const TF* f, R
                     st.t += small;
                     continue;
                 }
-                if (!st.prev_known) st.prev = sample_at(S, g, f, st.prev_t);
+                if (!st.prev_known) {
+                    float px, py, pz;
+                    texel(g, st.prev_t, px, py, pz);
+                    st.prev = trilinear(f, n, px, py, pz);
+                }
                 precise = st.t - small * st.prev / (tsdf - st.prev);   // the reference's formula
             }
             return 1;

@@ -46,9 +46,10 @@ struct FuseCtx {
     int* bmin;                   // brick lower bounds (null: none kept)
 };
 
-// running weighted average (project/src/tsdf.cu:56-69); max_w > 0 clamps the weight
+// running weighted average (project/src/tsdf.cu:56-69, built with -use_fast_math: the
+// division is the approximate one); max_w > 0 clamps the weight
 __device__ __forceinline__ void fuse_update(float& F, float& Wt, float fn, float wn, float max_w) {
-    F = (F * Wt + fn * wn) / (Wt + wn);
+    F = __fdividef(F * Wt + fn * wn, Wt + wn);
     float w1 = Wt + wn;
     if (max_w > 0.0f) w1 = fminf(w1, max_w);
     Wt = w1;
@@ -110,15 +111,15 @@ __device__ __forceinline__ void unit_origin(int n, int u, int& x0, int& j0, int&
 }
 
 // fuseKernel (project/src/tsdf.cu:28-74) for rows [r_begin, r_end) of one block (row r is
-// y = j0 + r % 8, z = k0 + r / 8), lanes along x
+// y = j0 + r % 8, z = k0 + r / 8; n is a multiple of 8, so every block has 64 rows), lanes
+// along x
 template <class TF, class TW>
 __device__ __forceinline__ void fuse_block(const FuseCtx& c, int x0, int j0, int k0, int r_begin, int r_end, int lane) {
     const int n = c.n;
     const int x = x0 + lane;
     const bool lane_in = x < n;
     const float xv = __ldg(c.xs + min(x, n - 1));
-    const int jn = min(8, n - j0), kn = min(8, n - k0);
-    const int rows = min(r_end, jn * kn);
+    const int rows = min(r_end, 64);
     int kmin = 0x7fffffff;   // key of the smallest distance this lane stores
     TF* F = static_cast<TF*>(c.F);
     TW* Wa = static_cast<TW*>(c.W);
@@ -133,7 +134,7 @@ __device__ __forceinline__ void fuse_block(const FuseCtx& c, int x0, int j0, int
             pz[q] = 0.f;
             const int r = r0 + q;
             if (r >= rows || !lane_in) continue;
-            const int j = j0 + r % jn, k = k0 + r / jn;
+            const int j = j0 + (r & 7), k = k0 + (r >> 3);
             const float y = __ldg(c.xs + j), z = __ldg(c.zs + k);
             const float bx = c.iR[3] * y + c.iR[6] * z + c.it[0];
             const float by = c.iR[4] * y + c.iR[7] * z + c.it[1];
@@ -158,8 +159,8 @@ __device__ __forceinline__ void fuse_block(const FuseCtx& c, int x0, int j0, int
             fn[q] = wn[q] = 0.f;
             if (!(cand & (1u << q)) || !depth_valid(d[q])) continue;
             const float diff = d[q] - pz[q];
-            if (diff >= -c.mu) {   // step 4
-                fn[q] = fminf(1.0f, diff / c.mu);
+            if (diff >= -c.mu) {   // step 4 (the reference divides with -use_fast_math)
+                fn[q] = fminf(1.0f, __fdividef(diff, c.mu));
                 wn[q] = 1.0f / d[q];
                 upd |= 1u << q;
             }
@@ -171,7 +172,7 @@ __device__ __forceinline__ void fuse_block(const FuseCtx& c, int x0, int j0, int
 #pragma unroll
         for (int q = 0; q < 4; ++q) {
             const int r = r0 + q;
-            idx[q] = (size_t(k0 + r / jn) * n + (j0 + r % jn)) * n + x;
+            idx[q] = (size_t(k0 + (r >> 3)) * n + (j0 + (r & 7))) * n + x;
             f0[q] = w0[q] = 0.f;
             if (upd & (1u << q)) {
                 if constexpr (sizeof(TF) == 4) {
@@ -314,76 +315,86 @@ cudaError_t launch_fuse(const EngineView& v, int grid, cudaStream_t st) {
 }
 
 // ---- brick bounds ----
+//
+// bmin: lower bound of each 8^3 brick's distances (fusion's atomic minima).
+// bdil: bmin widened to bricks {b, b+1}^3 (clamped), every brick a trilinear sample whose base
+//       voxel lies in brick b can touch; the raycaster's brick-level skip test reads it.
+// sdil: the same for 32^3 super-bricks: the minimum of bmin over bricks [4s, 4s + 4] per axis.
+//       The raycaster reads the two small arrays (sdil stays in L1) to skip samples.
 
-// bdil[b] = min of bmin over bricks {b, b+1}^3 (clamped): every brick a trilinear sample whose
-// base voxel lies in brick b can touch
-__global__ void __launch_bounds__(256) brick_dilate_kernel(EngineView v) {
-    const long long total = v.tb->brick_total;
-    const int S_cap = v.tb->S;
-    for (long long g = blockIdx.x * (long long)blockDim.x + threadIdx.x; g < total; g += (long long)gridDim.x * blockDim.x) {
-        int lo = 0, hi = S_cap;
-        while (hi - lo > 1) {
-            const int mid = (lo + hi) >> 1;
-            if (__ldg(v.brick_prefix + mid) <= g) lo = mid; else hi = mid;
-        }
-        if (!v.step[lo].active) continue;
-        const SessionDev* S = &v.sess[lo];
-        const long long b = g - __ldg(v.brick_prefix + lo);
-        const int nb = S->nb;
-        const int bx = int(b % nb), by = int((b / nb) % nb), bz = int(b / ((long long)nb * nb));
-        const int x1 = min(bx + 1, nb - 1), y1 = min(by + 1, nb - 1), z1 = min(bz + 1, nb - 1);
-        const int* m = S->bmin;
-        int k = 0x7fffffff;
-        k = min(k, m[(size_t(bz) * nb + by) * nb + bx]);
-        k = min(k, m[(size_t(bz) * nb + by) * nb + x1]);
-        k = min(k, m[(size_t(bz) * nb + y1) * nb + bx]);
-        k = min(k, m[(size_t(bz) * nb + y1) * nb + x1]);
-        k = min(k, m[(size_t(z1) * nb + by) * nb + bx]);
-        k = min(k, m[(size_t(z1) * nb + by) * nb + x1]);
-        k = min(k, m[(size_t(z1) * nb + y1) * nb + bx]);
-        k = min(k, m[(size_t(z1) * nb + y1) * nb + x1]);
-        S->bdil[b] = k;
-    }
+__device__ __forceinline__ int large_key() { return __float_as_int(0.991f); }
+
+// bdil[b] = min of bmin over bricks {b, b+1}^3 (clamped)
+__device__ __forceinline__ void dilate_brick(const int* __restrict__ m, int* bdil, int nb, long long b) {
+    const int bx = int(b % nb), by = int((b / nb) % nb), bz = int(b / ((long long)nb * nb));
+    const int x1 = min(bx + 1, nb - 1), y1 = min(by + 1, nb - 1), z1 = min(bz + 1, nb - 1);
+    int k = 0x7fffffff;
+    k = min(k, __ldg(m + (size_t(bz) * nb + by) * nb + bx));
+    k = min(k, __ldg(m + (size_t(bz) * nb + by) * nb + x1));
+    k = min(k, __ldg(m + (size_t(bz) * nb + y1) * nb + bx));
+    k = min(k, __ldg(m + (size_t(bz) * nb + y1) * nb + x1));
+    k = min(k, __ldg(m + (size_t(z1) * nb + by) * nb + bx));
+    k = min(k, __ldg(m + (size_t(z1) * nb + by) * nb + x1));
+    k = min(k, __ldg(m + (size_t(z1) * nb + y1) * nb + bx));
+    k = min(k, __ldg(m + (size_t(z1) * nb + y1) * nb + x1));
+    bdil[b] = k;
 }
 
-// sdil[s] = min of bmin over bricks [4s, 4s + 4] per axis (clamped): the bricks a sample whose
-// base voxel lies in super-brick s can touch; one warp per super-brick
+// sdil of super-brick (sx, sy, sz): min of bmin over bricks [4s, 4s + 4] per axis (clamped),
+// one warp
 __device__ __forceinline__ int superbrick_bound(const int* bmin, int nb, int sx, int sy, int sz, int lane) {
     const int x0 = 4 * sx, y0 = 4 * sy, z0 = 4 * sz;
     int k = 0x7fffffff;
     for (int q = lane; q < 125; q += 32) {
         const int x = min(x0 + q % 5, nb - 1), y = min(y0 + (q / 5) % 5, nb - 1), z = min(z0 + q / 25, nb - 1);
-        k = min(k, bmin[(size_t(z) * nb + y) * nb + x]);
+        k = min(k, __ldg(bmin + (size_t(z) * nb + y) * nb + x));
     }
 #pragma unroll
     for (int off = 16; off >= 1; off >>= 1) k = min(k, __shfl_xor_sync(0xffffffffu, k, off));
     return k;
 }
 
-__global__ void __launch_bounds__(256) superbrick_kernel(EngineView v) {
-    const long long total = v.tb->super_total;
+__device__ __forceinline__ int slot_of(const long long* prefix, long long g, int S_cap) {
+    int lo = 0, hi = S_cap;
+    while (hi - lo > 1) {
+        const int mid = (lo + hi) >> 1;
+        if (__ldg(prefix + mid) <= g) lo = mid; else hi = mid;
+    }
+    return lo;
+}
+
+// bdil of every brick (the first half of the grid) and sdil of every super-brick (the second
+// half, one warp each) of the stepping sessions
+__global__ void __launch_bounds__(256) bricks_kernel(EngineView v) {
     const int S_cap = v.tb->S;
-    const int lane = threadIdx.x & 31;
-    const long long warp = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5;
-    const long long nwarps = ((long long)gridDim.x * blockDim.x) >> 5;
-    for (long long g = warp; g < total; g += nwarps) {
-        int lo = 0, hi = S_cap;
-        while (hi - lo > 1) {
-            const int mid = (lo + hi) >> 1;
-            if (__ldg(v.super_prefix + mid) <= g) lo = mid; else hi = mid;
+    const int half = gridDim.x / 2;
+    if (int(blockIdx.x) < half) {
+        const long long total = v.tb->brick_total;
+        for (long long g = blockIdx.x * (long long)blockDim.x + threadIdx.x; g < total; g += (long long)half * blockDim.x) {
+            const int s = slot_of(v.brick_prefix, g, S_cap);
+            if (!v.step[s].active) continue;
+            const SessionDev* S = &v.sess[s];
+            dilate_brick(S->bmin, S->bdil, S->nb, g - __ldg(v.brick_prefix + s));
         }
-        if (!v.step[lo].active) continue;
-        const SessionDev* S = &v.sess[lo];
-        const long long b = g - __ldg(v.super_prefix + lo);
-        const int ns = S->ns;
-        const int k = superbrick_bound(S->bmin, S->nb, int(b % ns), int((b / ns) % ns), int(b / ((long long)ns * ns)), lane);
-        if (lane == 0) S->sdil[b] = k;
+    } else {
+        const long long total = v.tb->super_total;
+        const int lane = threadIdx.x & 31;
+        const long long warp = ((blockIdx.x - half) * (long long)blockDim.x + threadIdx.x) >> 5;
+        const long long nwarps = ((long long)(gridDim.x - half) * blockDim.x) >> 5;
+        for (long long g = warp; g < total; g += nwarps) {
+            const int s = slot_of(v.super_prefix, g, S_cap);
+            if (!v.step[s].active) continue;
+            const SessionDev* S = &v.sess[s];
+            const long long b = g - __ldg(v.super_prefix + s);
+            const int ns = S->ns;
+            const int k = superbrick_bound(S->bmin, S->nb, int(b % ns), int((b / ns) % ns), int(b / ((long long)ns * ns)), lane);
+            if (lane == 0) S->sdil[b] = k;
+        }
     }
 }
 
 cudaError_t launch_bricks(const EngineView& v, int grid, cudaStream_t st) {
-    brick_dilate_kernel<<<grid, 256, 0, st>>>(v);
-    superbrick_kernel<<<grid, 256, 0, st>>>(v);
+    bricks_kernel<<<grid, 256, 0, st>>>(v);
     return cudaGetLastError();
 }
 
@@ -425,15 +436,8 @@ __global__ void rebuild_bricks_kernel(const TF* f, int n, int* bmin) {
 
 __global__ void dilate_one_kernel(const int* bmin, int* bdil, int nb) {
     const long long total = (long long)nb * nb * nb;
-    for (long long b = blockIdx.x * (long long)blockDim.x + threadIdx.x; b < total; b += (long long)gridDim.x * blockDim.x) {
-        const int bx = int(b % nb), by = int((b / nb) % nb), bz = int(b / ((long long)nb * nb));
-        int k = 0x7fffffff;
-        for (int dz = 0; dz < 2; ++dz)
-            for (int dy = 0; dy < 2; ++dy)
-                for (int dx = 0; dx < 2; ++dx)
-                    k = min(k, bmin[(size_t(min(bz + dz, nb - 1)) * nb + min(by + dy, nb - 1)) * nb + min(bx + dx, nb - 1)]);
-        bdil[b] = k;
-    }
+    for (long long b = blockIdx.x * (long long)blockDim.x + threadIdx.x; b < total; b += (long long)gridDim.x * blockDim.x)
+        dilate_brick(bmin, bdil, nb, b);
 }
 
 __global__ void superbrick_one_kernel(const int* bmin, int* sdil, int nb) {

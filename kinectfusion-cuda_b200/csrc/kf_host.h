@@ -64,7 +64,8 @@ cudaError_t launch_preprocess(const EngineView& v, int grid, cudaStream_t st);
 cudaError_t launch_raycast(const EngineView& v, int grid, cudaStream_t st);
 cudaError_t launch_icp(const EngineView& v, int grid, cudaStream_t st);
 cudaError_t launch_fuse(const EngineView& v, int grid, cudaStream_t st);
-// widen the brick lower bounds to the 2 x 2 x 2 neighbourhood the raycaster reads
+// widen the brick lower bounds to the 2 x 2 x 2 bricks the raycaster reads, and bound the
+// super-bricks (one launch)
 cudaError_t launch_bricks(const EngineView& v, int grid, cudaStream_t st);
 // bounds = key(2), the initial distance; rebuild recomputes them exactly from a loaded volume
 cudaError_t launch_init_bricks(int* bmin, int* bdil, int* sdil, int n, cudaStream_t st);
