@@ -305,6 +305,14 @@ kf_status kf_server_step(kf_server* srv, int* served);
 kf_status kf_server_result(kf_server* srv, int id, float pose[16], kf_frame_stats* stats);
 kf_status kf_server_get_session(kf_server* srv, int id, kf_session** out);
 kf_status kf_server_stats_get(kf_server* srv, kf_server_stats* out);
+/* Capacity planning: allocate device arenas for `count` sessions shaped like cfg (and pinned
+ * staging for as many slots) into the server's pool, so that opening such sessions later
+ * allocates nothing.  Cached arenas count against the HBM budget; KF_ERR_OOM_BUDGET when
+ * they would not fit. */
+kf_status kf_server_reserve(kf_server* srv, const kf_config* cfg, int count);
+/* Start a new statistics window: latencies, frame, step and session counters restart from
+ * zero (after a warm-up, say); sessions and their state are untouched. */
+kf_status kf_server_stats_reset(kf_server* srv);
 /* Clock used for latency accounting (milliseconds, monotonic). */
 double kf_now_ms(void);
 

@@ -121,29 +121,100 @@ PoseDev make_pose_dev(const float* pose16) {
 
 // ---- one session's device resources ----
 
+// Device arenas a server keeps after its sessions close, for the next sessions to reuse: a
+// session opening or closing then allocates and frees nothing (cudaFree waits for the whole
+// device, which would stall every other session's frames).
+struct ArenaPool {
+    std::mutex mu;
+    std::vector<std::pair<char*, size_t>> free;
+    size_t cached = 0;   // bytes held in `free` (read without the lock only as an estimate)
+
+    // the smallest cached arena of at least `need` bytes and at most about twice that
+    char* take(size_t need, size_t& cap) {
+        std::lock_guard<std::mutex> g(mu);
+        int best = -1;
+        for (int i = 0; i < int(free.size()); ++i)
+            if (free[i].second >= need && free[i].second <= 2 * need + (16u << 20) &&
+                (best < 0 || free[i].second < free[best].second))
+                best = i;
+        if (best < 0) return nullptr;
+        char* p = free[best].first;
+        cap = free[best].second;
+        free.erase(free.begin() + best);
+        cached -= cap;
+        return p;
+    }
+    void put(char* p, size_t cap) {
+        std::lock_guard<std::mutex> g(mu);
+        free.emplace_back(p, cap);
+        cached += cap;
+    }
+    // free cached arenas, largest first, until at most `keep` bytes stay cached
+    void trim(size_t keep) {
+        std::lock_guard<std::mutex> g(mu);
+        while (cached > keep && !free.empty()) {
+            int big = 0;
+            for (int i = 1; i < int(free.size()); ++i)
+                if (free[i].second > free[big].second) big = i;
+            cudaFree(free[big].first);
+            cached -= free[big].second;
+            free.erase(free.begin() + big);
+        }
+    }
+};
+
 struct Slot {
     bool used = false;
     kf_config cfg{};
     SessionDev d{};
-    std::vector<void*> allocs;
+    std::vector<void*> allocs;    // buffers outside the arena
+    char* arena = nullptr;        // one device allocation holding the session's buffers
+    size_t arena_cap = 0, arena_used = 0;
+    ArenaPool* pool = nullptr;    // set by a server: arenas come from and go back to it
     size_t bytes = 0;
     int frames = 0;
     kf_frame_stats stats{};
     float pose[16]{};
     bool external = false;   // maps supplied by the caller (kf_compute_pose)
 
+    // reserve (and zero, on st) one arena for buffers of `need` bytes in all
+    cudaError_t begin_arena(size_t need, cudaStream_t st) {
+        if (pool) arena = pool->take(need, arena_cap);
+        if (!arena) {
+            cudaError_t e = cudaMalloc(&arena, need);
+            if (e != cudaSuccess) { arena = nullptr; return e; }
+            arena_cap = need;
+        }
+        arena_used = 0;
+        zero_stream = st;
+        return cudaMemsetAsync(arena, 0, need, st);
+    }
+    cudaStream_t zero_stream = nullptr;
     void* alloc(size_t nbytes, cudaError_t& err) {
+        const size_t off = (arena_used + 255) & ~size_t(255);
+        if (arena && off + nbytes <= arena_cap) {
+            arena_used = off + nbytes;
+            bytes += nbytes;
+            err = cudaSuccess;
+            return arena + off;
+        }
         void* p = nullptr;
         err = cudaMalloc(&p, nbytes);
         if (err != cudaSuccess) return nullptr;
         allocs.push_back(p);
         bytes += nbytes;
-        err = cudaMemset(p, 0, nbytes);
+        err = cudaMemsetAsync(p, 0, nbytes, zero_stream);
         return p;
     }
     void release() {
         for (void* p : allocs) cudaFree(p);
         allocs.clear();
+        if (arena) {
+            if (pool) pool->put(arena, arena_cap);
+            else cudaFree(arena);
+        }
+        arena = nullptr;
+        arena_cap = arena_used = 0;
         bytes = 0;
         used = false;
         external = false;
@@ -179,7 +250,9 @@ void fill_levels(SessionDev& d, const kf_config& c) {
     d.stop_d = c.stop_dist;
 }
 
-kf_status slot_create(Slot& s, const kf_config& c) {
+// allocate and initialise a session's buffers; all device work on st, synchronised before
+// returning (so a server can build a session while other sessions' steps run)
+kf_status slot_create(Slot& s, const kf_config& c, cudaStream_t st = nullptr) {
     KF_TRY(validate(c));
     s.release();
     s.cfg = c;
@@ -193,7 +266,8 @@ kf_status slot_create(Slot& s, const kf_config& c) {
     d.bil_inv_sr = 1.0f / (c.bilateral_sigma_r * c.bilateral_sigma_r);
     d.down_thr = 3.0f * c.bilateral_sigma_r;
     d.bil_r = c.bilateral_radius;
-    cudaError_t err = cudaSuccess;
+    cudaError_t err = s.begin_arena(footprint(c) + (64u << 10), st);   // + alignment of ~30 buffers
+    if (err != cudaSuccess) { g_last_cuda = err; s.release(); return KF_ERR_CUDA; }
 #define KF_ALLOC(ptr, type, bytes)                                   \
     do {                                                             \
         ptr = static_cast<type>(s.alloc((bytes), err));              \
@@ -229,13 +303,11 @@ kf_status slot_create(Slot& s, const kf_config& c) {
     float* zs;
     KF_ALLOC(xs, float*, sizeof(float) * c.volume_n);
     KF_ALLOC(zs, float*, sizeof(float) * c.volume_n);
-    {
-        std::vector<float> hx(c.volume_n), hz(c.volume_n);
-        voxel_axes(c.volume_n, c.volume_width, hx.data(), hz.data());
-        err = cudaMemcpy(xs, hx.data(), sizeof(float) * c.volume_n, cudaMemcpyHostToDevice);
-        if (err == cudaSuccess) err = cudaMemcpy(zs, hz.data(), sizeof(float) * c.volume_n, cudaMemcpyHostToDevice);
-        if (err != cudaSuccess) { g_last_cuda = err; s.release(); return KF_ERR_CUDA; }
-    }
+    std::vector<float> hx(c.volume_n), hz(c.volume_n);   // alive until the stream sync below
+    voxel_axes(c.volume_n, c.volume_width, hx.data(), hz.data());
+    err = cudaMemcpyAsync(xs, hx.data(), sizeof(float) * c.volume_n, cudaMemcpyHostToDevice, st);
+    if (err == cudaSuccess) err = cudaMemcpyAsync(zs, hz.data(), sizeof(float) * c.volume_n, cudaMemcpyHostToDevice, st);
+    if (err != cudaSuccess) { g_last_cuda = err; s.release(); return KF_ERR_CUDA; }
     d.xs = xs;
     d.zs = zs;
     d.min_d = c.min_depth;
@@ -252,13 +324,11 @@ kf_status slot_create(Slot& s, const kf_config& c) {
     KF_ALLOC(d.sdil, int*, sizeof(int) * size_t(nsuper));
 #undef KF_ALLOC
     // grid {f = 2, w = 0} and pose = initial_pose (project/src/kinect_fusion.cpp:33-36, :80)
-    err = launch_init_volume(d.tf, d.tw, (long long)n3, d.fmt, 0);
-    if (err == cudaSuccess) err = launch_init_bricks(d.bmin, d.bdil, d.sdil, c.volume_n, 0);
-    if (err == cudaSuccess) {
-        PoseDev P = make_pose_dev(c.initial_pose);
-        err = cudaMemcpy(d.pose, &P, sizeof(P), cudaMemcpyHostToDevice);
-    }
-    if (err == cudaSuccess) err = cudaDeviceSynchronize();
+    err = launch_init_volume(d.tf, d.tw, (long long)n3, d.fmt, st);
+    if (err == cudaSuccess) err = launch_init_bricks(d.bmin, d.bdil, d.sdil, c.volume_n, st);
+    const PoseDev P = make_pose_dev(c.initial_pose);
+    if (err == cudaSuccess) err = cudaMemcpyAsync(d.pose, &P, sizeof(P), cudaMemcpyHostToDevice, st);
+    if (err == cudaSuccess) err = cudaStreamSynchronize(st);
     if (err != cudaSuccess) { g_last_cuda = err; s.release(); return KF_ERR_CUDA; }
     s.used = true;
     s.frames = 0;
@@ -326,6 +396,8 @@ struct Engine {
     // fusion queue (one entry per block of every slot at most)
     unsigned int* d_fuseq = nullptr;
     int cap_fuseq = 0;
+    // work-list entries reserved ahead for sessions not open yet (reserve_work)
+    long long res_pre = 0, res_ray = 0, res_it = 0, res_fq = 0;
     // pinned host
     StepDev* h_step = nullptr;
     OutDev* h_out = nullptr;
@@ -434,6 +506,49 @@ struct Engine {
         v.fuseq = d_fuseq;
         v.fuseq_cap = cap_fuseq;
         return v;
+    }
+
+    // Grow the work-list buffers for `count` more sessions like c on top of the current
+    // tables, ahead of time (a server's capacity planning): growing them while serving frees
+    // and reallocates device memory and re-instantiates the step graph.
+    kf_status reserve_work(const kf_config& c, int count) {
+        SessionDev d{};
+        fill_levels(d, c);
+        long long pre = 0, ray = 0, itiles = 0;
+        pre = (long long)((c.width + kPreTileSize - 1) / kPreTileSize) * ((c.height + kPreTileSize - 1) / kPreTileSize);
+        for (int l = 0; l < c.levels; ++l) {
+            const LevelDev& Lv = d.lv[l];
+            ray += (long long)((Lv.cw + kRayTileW - 1) / kRayTileW) * ((Lv.ch + kRayTileH - 1) / kRayTileH);
+            itiles += (long long)grid_icp * kIcpTilesPerBlock + 1;   // at most that many per level
+        }
+        // reservations add up: every kind reserved so far may be open at once
+        const long long k = count;
+        res_pre += k * pre;
+        res_ray += k * ray;
+        res_it += k * itiles;
+        res_fq += k * fuse_units(c.volume_n);
+        const long long need_pre = tb.n_pre + res_pre, need_ray = tb.n_ray + res_ray;
+        long long cur_it = 0;
+        for (int l = 0; l < KF_MAX_LEVELS; ++l) cur_it += tb.n_itiles[l];
+        const long long need_it = cur_it + res_it;
+        const long long need_fq = tb.fuse_total + res_fq;
+        if (need_pre > INT32_MAX || need_ray * 32 / 4 > INT32_MAX / long_ray_bytes() ||
+            need_it * kIcpPartialStride > INT32_MAX || need_fq > (1 << 29))
+            return KF_ERR_CAPACITY;
+        const int old_pre = cap_pre, old_ray = cap_ray, old_it = cap_it, old_part = cap_part, old_lq = cap_longq,
+                  old_fq = cap_fuseq;
+        KF_TRY(grow(d_pre, cap_pre, int(need_pre)));
+        KF_TRY(grow(d_ray, cap_ray, int(need_ray)));
+        KF_TRY(grow(d_itiles, cap_it, int(need_it)));
+        KF_TRY(grow(d_partials, cap_part, int(need_it) * kIcpPartialStride));
+        KF_TRY(grow(d_longq, cap_longq, std::max<int>(1024, int(need_ray) * 32 / 4) * long_ray_bytes()));
+        KF_TRY(grow(d_fuseq, cap_fuseq, int(need_fq)));
+        if (old_pre != cap_pre || old_ray != cap_ray || old_it != cap_it || old_part != cap_part || old_lq != cap_longq ||
+            old_fq != cap_fuseq) {
+            graph_dirty = true;
+            tables_dirty = true;
+        }
+        return KF_OK;
     }
 
     // rebuild and upload work lists (synchronous; callers hold the engine)
@@ -1404,8 +1519,10 @@ namespace {
 
 struct ServerSlot {
     int id = -1;                  // session id, -1 = free
-    uint16_t* stage[2] = {nullptr, nullptr};   // pinned staging buffers
-    size_t stage_bytes = 0;
+    uint16_t* stage[2] = {nullptr, nullptr};   // pinned staging buffers (kept across sessions)
+    size_t stage_bytes = 0;       // frame bytes of the current session
+    size_t stage_cap = 0;         // bytes each staging buffer holds
+    bool reserved = false;        // being opened or closed: not free, not yet serving
     int pending = -1;             // staged buffer waiting for a step
     int inflight = -1;            // staged buffer a running step reads
     double t_submit[2] = {0, 0};
@@ -1421,6 +1538,7 @@ double now_ms() {
 
 struct kf_server {
     Engine eng;
+    ArenaPool pool;      // device arenas of closed sessions, reused by the next ones
     int max_slots = 0;
     size_t budget = 0, in_use = 0;
     std::vector<ServerSlot> hs;
@@ -1468,6 +1586,7 @@ kf_status kf_server_destroy(kf_server* s) {
             if (h.stage[b]) cudaFreeHost(h.stage[b]);
     for (kf_session* v : s->views) delete v;
     s->eng.destroy();
+    s->pool.trim(0);
     if (s->stream) cudaStreamDestroy(s->stream);
     delete s;
     return KF_OK;
@@ -1476,45 +1595,125 @@ kf_status kf_server_destroy(kf_server* s) {
 kf_status kf_server_open(kf_server* s, const kf_config* cfg, int* id) {
     if (!s || !cfg || !id) return KF_ERR_ARG;
     KF_TRY(validate(*cfg));
-    std::lock_guard<std::mutex> g(s->gpu_mu);
     const size_t need = footprint(*cfg) + size_t(cfg->width) * cfg->height * 2 * 2;
-    if (s->in_use + need > s->budget) {
-        s->refused++;
-        return KF_ERR_OOM_BUDGET;
-    }
     int slot = -1;
-    for (int i = 0; i < s->max_slots; ++i)
-        if (s->hs[i].id < 0) { slot = i; break; }
-    if (slot < 0) {
-        s->refused++;
-        return KF_ERR_CAPACITY;
-    }
-    KF_CK(cudaStreamSynchronize(s->stream));
-    KF_TRY(slot_create(s->eng.slots[slot], *cfg));
-    ServerSlot& h = s->hs[slot];
-    h.stage_bytes = size_t(cfg->width) * cfg->height * 2;
-    for (int b = 0; b < 2; ++b) {
-        if (cudaMallocHost(&h.stage[b], h.stage_bytes) != cudaSuccess) {
-            s->eng.slots[slot].release();
-            return KF_ERR_CUDA;
-        }
-    }
-    h.pending = h.inflight = -1;
-    h.has_result = false;
+    size_t keep_cached = 0;
     {
         std::lock_guard<std::mutex> q(s->q_mu);
-        h.id = s->next_id++;
+        if (s->in_use + need > s->budget) {
+            s->refused++;
+            return KF_ERR_OOM_BUDGET;
+        }
+        for (int i = 0; i < s->max_slots; ++i)
+            if (s->hs[i].id < 0 && !s->hs[i].reserved) { slot = i; break; }
+        if (slot < 0) {
+            s->refused++;
+            return KF_ERR_CAPACITY;
+        }
+        s->hs[slot].reserved = true;
+        s->in_use += need;   // held while the session is built
+        keep_cached = s->budget - s->in_use;
     }
-    s->in_use += s->eng.slots[slot].bytes + 2 * h.stage_bytes;
-    s->eng.tables_dirty = true;
-    s->admitted++;
-    *id = h.id;
+    // Build the session outside the GPU lock, on a stream of its own, so that the other
+    // sessions' steps go on meanwhile.  Cached arenas count against the budget too.
+    if (s->pool.cached > keep_cached) s->pool.trim(keep_cached);
+    ServerSlot& h = s->hs[slot];   // reserved: no other thread touches it until registered
+    Slot tmp;
+    tmp.pool = &s->pool;
+    cudaStream_t st = nullptr;
+    kf_status r = cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking) == cudaSuccess ? KF_OK : KF_ERR_CUDA;
+    if (r == KF_OK) r = slot_create(tmp, *cfg, st);
+    if (st) cudaStreamDestroy(st);
+    const size_t frame_bytes = size_t(cfg->width) * cfg->height * 2;
+    if (r == KF_OK && h.stage_cap < frame_bytes) {
+        for (int b = 0; b < 2; ++b) {
+            if (h.stage[b]) cudaFreeHost(h.stage[b]);
+            h.stage[b] = nullptr;
+        }
+        h.stage_cap = 0;
+        for (int b = 0; b < 2 && r == KF_OK; ++b)
+            if (cudaMallocHost(&h.stage[b], frame_bytes) != cudaSuccess) r = KF_ERR_CUDA;
+        if (r == KF_OK) h.stage_cap = frame_bytes;
+    }
+    if (r != KF_OK) {
+        tmp.release();
+        std::lock_guard<std::mutex> q(s->q_mu);
+        h.reserved = false;
+        s->in_use -= need;
+        return r;
+    }
+    {
+        std::lock_guard<std::mutex> g(s->gpu_mu);
+        std::swap(s->eng.slots[slot], tmp);   // tmp receives the empty slot
+        s->eng.tables_dirty = true;
+    }
+    tmp.release();
+    {
+        std::lock_guard<std::mutex> q(s->q_mu);
+        h.stage_bytes = frame_bytes;
+        h.pending = h.inflight = -1;
+        h.has_result = false;
+        h.id = s->next_id++;
+        h.reserved = false;
+        s->in_use = s->in_use - need + s->eng.slots[slot].bytes + 2 * frame_bytes;
+        s->admitted++;
+        *id = h.id;
+    }
+    return KF_OK;
+}
+
+kf_status kf_server_reserve(kf_server* s, const kf_config* cfg, int count) {
+    if (!s || !cfg || count < 0) return KF_ERR_ARG;
+    KF_TRY(validate(*cfg));
+    const size_t arena = footprint(*cfg) + (64u << 10);   // what slot_create reserves
+    const size_t frame_bytes = size_t(cfg->width) * cfg->height * 2;
+    {
+        std::lock_guard<std::mutex> q(s->q_mu);
+        if (s->in_use + s->pool.cached + size_t(count) * arena > s->budget) return KF_ERR_OOM_BUDGET;
+    }
+    for (int k = 0; k < count; ++k) {
+        char* p = nullptr;
+        KF_CK(cudaMalloc(&p, arena));
+        s->pool.put(p, arena);
+    }
+    {
+        // the engine's work lists, sized for these sessions on top of the current ones
+        std::lock_guard<std::mutex> g(s->gpu_mu);
+        KF_CK(cudaStreamSynchronize(s->stream));
+        KF_TRY(s->eng.reserve_work(*cfg, count));
+    }
+    // staging for up to `count` free slots that have none large enough
+    int staged = 0;
+    for (int i = 0; i < s->max_slots && staged < count; ++i) {
+        ServerSlot& h = s->hs[i];
+        {
+            std::lock_guard<std::mutex> q(s->q_mu);
+            if (h.id >= 0 || h.reserved) continue;
+            h.reserved = true;
+        }
+        kf_status r = KF_OK;
+        if (h.stage_cap < frame_bytes) {
+            for (int b = 0; b < 2; ++b) {
+                if (h.stage[b]) cudaFreeHost(h.stage[b]);
+                h.stage[b] = nullptr;
+            }
+            h.stage_cap = 0;
+            for (int b = 0; b < 2 && r == KF_OK; ++b)
+                if (cudaMallocHost(&h.stage[b], frame_bytes) != cudaSuccess) r = KF_ERR_CUDA;
+            if (r == KF_OK) h.stage_cap = frame_bytes;
+        }
+        {
+            std::lock_guard<std::mutex> q(s->q_mu);
+            h.reserved = false;
+        }
+        if (r != KF_OK) return r;
+        ++staged;
+    }
     return KF_OK;
 }
 
 kf_status kf_server_close(kf_server* s, int id) {
     if (!s) return KF_ERR_ARG;
-    std::lock_guard<std::mutex> g(s->gpu_mu);
     int slot;
     {
         std::lock_guard<std::mutex> q(s->q_mu);
@@ -1522,16 +1721,22 @@ kf_status kf_server_close(kf_server* s, int id) {
         if (slot < 0) return KF_ERR_ARG;
         s->hs[slot].id = -1;
         s->hs[slot].pending = -1;
+        s->hs[slot].reserved = true;   // not reusable until its memory is back
     }
-    KF_CK(cudaStreamSynchronize(s->stream));
-    ServerSlot& h = s->hs[slot];
-    s->in_use -= s->eng.slots[slot].bytes + 2 * h.stage_bytes;
-    s->eng.slots[slot].release();
-    for (int b = 0; b < 2; ++b) {
-        if (h.stage[b]) cudaFreeHost(h.stage[b]);
-        h.stage[b] = nullptr;
+    Slot tmp;
+    {
+        std::lock_guard<std::mutex> g(s->gpu_mu);   // no step is running while it is held
+        KF_CK(cudaStreamSynchronize(s->stream));
+        std::swap(s->eng.slots[slot], tmp);
+        s->eng.tables_dirty = true;
     }
-    s->eng.tables_dirty = true;
+    const size_t freed = tmp.bytes + 2 * s->hs[slot].stage_bytes;
+    tmp.release();   // the arena goes back to the pool; the staging stays with the slot
+    {
+        std::lock_guard<std::mutex> q(s->q_mu);
+        s->in_use -= freed;
+        s->hs[slot].reserved = false;
+    }
     return KF_OK;
 }
 
@@ -1621,6 +1826,18 @@ kf_status kf_server_get_session(kf_server* s, int id, kf_session** out) {
         s->views[slot] = v;
     }
     *out = s->views[slot];
+    return KF_OK;
+}
+
+kf_status kf_server_stats_reset(kf_server* s) {
+    if (!s) return KF_ERR_ARG;
+    std::lock_guard<std::mutex> q(s->q_mu);
+    s->lat.clear();
+    s->frames_done = s->admitted = s->refused = s->steps = 0;
+    int active = 0;
+    for (const ServerSlot& h : s->hs)
+        if (h.id >= 0) ++active;
+    s->max_active = active;
     return KF_OK;
 }
 

@@ -20,7 +20,7 @@
 namespace kf {
 
 constexpr int kMaxMarchSamples = 1 << 16;
-constexpr int kSerialBudget = 64;   // loop iterations a lane marches before queueing the ray
+constexpr int kSerialBudget = 40;   // loop iterations a lane marches before queueing the ray
 
 struct RayGeo {
     F3 o, dir;

@@ -569,6 +569,13 @@ class Server:
         check(lib.kf_server_stats_get(self._s, ctypes.byref(s)))
         return {f: getattr(s, f) for f, _ in KfServerStats._fields_}
 
+    def reserve(self, config, count):
+        """Pre-allocate device arenas (and pinned staging) for `count` sessions like config."""
+        check(lib.kf_server_reserve(self._s, ctypes.byref(config), int(count)), "kf_server_reserve")
+
+    def reset_stats(self):
+        check(lib.kf_server_stats_reset(self._s), "kf_server_stats_reset")
+
     @staticmethod
     def now_ms():
         return lib.kf_now_ms()

@@ -132,6 +132,8 @@ SIGNATURES = {
     "kf_server_result": (_I, [_P, _I, _FP, ctypes.POINTER(KfFrameStats)]),
     "kf_server_get_session": (_I, [_P, _I, ctypes.POINTER(_P)]),
     "kf_server_stats_get": (_I, [_P, ctypes.POINTER(KfServerStats)]),
+    "kf_server_stats_reset": (_I, [_P]),
+    "kf_server_reserve": (_I, [_P, _CFG, _I]),
     "kf_now_ms": (ctypes.c_double, []),
     "kf_session_set_profiling": (_I, [_P, _I]),
     "kf_session_stage_times": (_I, [_P, _FP]),
