@@ -251,6 +251,64 @@ kf_status kf_compute_pose(const float* const* vertex, const float* const* target
 kf_status kf_pose_error(const float pose_1[16], const float pose_2[16], float out[2]);
 
 /* ------------------------------------------------------------------------------------------ */
+/* files: TSDF in the reference's .bin layout, session checkpoints                            */
+/* ------------------------------------------------------------------------------------------ */
+/* VoxelGrid::saveVoxelGrid / loadVoxelGrid (project/src/voxel_grid.cpp:43-80): n^3 interleaved
+ * float {f, w}, x fastest, no header.  Loading a file of another size is KF_ERR_SHAPE.  F16U16
+ * sessions convert to and from float. */
+kf_status kf_save_tsdf_file(kf_session* s, const char* path);
+kf_status kf_load_tsdf_file(kf_session* s, const char* path);
+/* Checkpoint: the .bin TSDF at `path` plus `path`.pose (text: frame count and the
+ * column-major camera->world pose).  After a load the session resumes tracking as frame
+ * `frames` of its sequence.  No counterpart in the reference beyond the .bin file. */
+kf_status kf_session_checkpoint_save(kf_session* s, const char* path);
+kf_status kf_session_checkpoint_load(kf_session* s, const char* path);
+
+/* ------------------------------------------------------------------------------------------ */
+/* headless display: the reference's window-content kernels (project/src/display.cu:9-105)    */
+/* into RGBA8 images in device memory (row-major, bytes r, g, b, 255 per pixel)              */
+/* ------------------------------------------------------------------------------------------ */
+#define KF_RENDER_NORMALS 0   /* normalMapToWindowContent: rotated normal * 255 as r, g, b */
+#define KF_RENDER_SHADING 1   /* shadingToWindowContent: |normal . ray| * 255 as grey */
+/* kernel::normalMapToWindowContent (project/src/display.cu:143-154); normal: float4 map,
+ * inv_rot: the inverse sensor rotation (column-major 3x3). */
+kf_status kf_normal_map_to_rgba(const float* normal, int w, int h, const float inv_rot[9],
+                                uint8_t* rgba, void* stream, float* elapsed_ms);
+/* kernel::shadingToWindowContent (project/src/display.cu:156-167); pose: camera->world,
+ * inv_cam_k: level-0 inverse intrinsics. */
+kf_status kf_shading_to_rgba(const float* normal, int w, int h, const float pose[16],
+                             const float inv_cam_k[9], uint8_t* rgba, void* stream,
+                             float* elapsed_ms);
+/* kernel::oneFloatChannelToWindowContent (project/src/display.cu:117-128): value * scale. */
+kf_status kf_float_channel_to_rgba(const float* src, int w, int h, float scale, uint8_t* rgba,
+                                   void* stream, float* elapsed_ms);
+/* KinectFusion::visualizeCurrentModel (project/src/kinect_fusion.cpp:185-203), headless: raycast
+ * the session's volume at level 0 from `pose` (NULL: the current pose; the reference's static
+ * view passes the initial pose) into the session's own render maps, then the display kernel of
+ * `mode` into rgba (w * h * 4 bytes; host memory when to_host = 1).  Tracking maps are not
+ * touched.  Synchronizes `stream`. */
+kf_status kf_render(kf_session* s, int mode, const float pose[16], uint8_t* rgba, int to_host,
+                    void* stream);
+
+/* ------------------------------------------------------------------------------------------ */
+/* datasets: TUM RGB-D sequences (RgbdDataset, project/src/rgbd_dataset.h:12-27)              */
+/* ------------------------------------------------------------------------------------------ */
+typedef struct kf_tum kf_tum;
+/* RgbdDataset::load (project/src/rgbd_dataset.cpp:6-76): groundtruth.txt and depth.txt (three
+ * comment lines each); every depth image is paired with the nearest ground-truth pose. */
+kf_status kf_tum_open(const char* dir, kf_tum** out);
+kf_status kf_tum_close(kf_tum* d);
+kf_status kf_tum_count(const kf_tum* d, int* count);
+/* Frame `index`: the 16-bit depth PNG decoded into depth (w * h, KF_ERR_SHAPE if the image
+ * size differs; NULL to skip) and its ground-truth pose (column-major camera->world, the
+ * reference's mat4_cast(quaternion) with the translation; NULL to skip). */
+kf_status kf_tum_frame(const kf_tum* d, int index, uint16_t* depth, int w, int h, float pose[16]);
+/* RgbdDataset::getInitialPoseInverse (project/src/rgbd_dataset.cpp:89-92). */
+kf_status kf_tum_initial_pose_inverse(const kf_tum* d, float out[16]);
+/* DepthMap::update(path) (project/src/depth_map.cpp:17-28): a 16-bit greyscale PNG. */
+kf_status kf_png16_read(const char* path, uint16_t* dst, int w, int h);
+
+/* ------------------------------------------------------------------------------------------ */
 /* batch: many independent sessions of uneven sizes, one persistent launch per stage,        */
 /* replayed from a captured CUDA graph                                                        */
 /* ------------------------------------------------------------------------------------------ */

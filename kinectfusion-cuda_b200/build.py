@@ -17,7 +17,8 @@ LIB = os.path.join(HERE, "lib")
 OBJ = os.path.join(HERE, "_build")
 REPO = os.path.dirname(HERE)
 
-CU_SOURCES = ["k_preprocess.cu", "k_raycast.cu", "k_tsdf.cu", "k_icp.cu", "api.cu"]
+CU_SOURCES = ["k_preprocess.cu", "k_raycast.cu", "k_tsdf.cu", "k_icp.cu", "k_display.cu", "api.cu"]
+CXX_SOURCES = ["dataset.cpp"]   # host-only parts of the library (zlib for 16-bit PNG)
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",
     "-lineinfo", "-O3", "-std=c++17",
@@ -67,13 +68,19 @@ def build(verbose=False, ptxas_info=False):
         objs.append(o)
         if ptxas_info or _stale(o, [s] + headers):
             jobs.append([nvcc] + NVCC_FLAGS + extra + ["-c", s, "-o", o])
+    for src in CXX_SOURCES:
+        s = os.path.join(CSRC, src)
+        o = os.path.join(OBJ, src.replace(".cpp", ".o"))
+        objs.append(o)
+        if _stale(o, [s, os.path.join(REPO, "include", "kf_api.h")]):
+            jobs.append([_cxx(), "-O2", "-std=c++17", "-fPIC", "-I", os.path.join(REPO, "include"), "-c", s, "-o", o])
     logs = []
     with ThreadPoolExecutor(max_workers=min(8, max(1, len(jobs)))) as ex:
         for out in ex.map(lambda c: _run(c, verbose), jobs):
             logs.append(out)
     so = os.path.join(LIB, "libkfb200.so")
     if jobs or not os.path.exists(so):
-        _run([nvcc, "-shared", "-gencode", "arch=compute_100a,code=sm_100a", "-o", so] + objs, verbose)
+        _run([nvcc, "-shared", "-gencode", "arch=compute_100a,code=sm_100a", "-o", so] + objs + ["-lz"], verbose)
     synth = os.path.join(LIB, "libkfsynth.so")
     ssrc = os.path.join(CSRC, "synth.cpp")
     if _stale(synth, [ssrc]):

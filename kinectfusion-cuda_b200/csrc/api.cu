@@ -176,6 +176,9 @@ struct Slot {
     kf_frame_stats stats{};
     float pose[16]{};
     bool external = false;   // maps supplied by the caller (kf_compute_pose)
+    float4* render_v = nullptr;          // kf_render's own level-0 maps and image (lazily)
+    float4* render_n = nullptr;
+    unsigned int* render_rgba = nullptr;
 
     // reserve (and zero, on st) one arena for buffers of `need` bytes in all
     cudaError_t begin_arena(size_t need, cudaStream_t st) {
@@ -215,6 +218,8 @@ struct Slot {
         }
         arena = nullptr;
         arena_cap = arena_used = 0;
+        render_v = render_n = nullptr;
+        render_rgba = nullptr;
         bytes = 0;
         used = false;
         external = false;
@@ -1078,6 +1083,154 @@ kf_status kf_set_tsdf(kf_session* s, const void* src, size_t src_bytes, int layo
     // the raycaster's brick minima follow the new volume
     KF_CK(launch_rebuild_bricks(sl.d.tf, sl.d.fmt, sl.cfg.volume_n, sl.d.bmin, sl.d.bdil, sl.d.sdil, 0));
     KF_CK(cudaDeviceSynchronize());
+    return KF_OK;
+}
+
+// ---- files: the reference's .bin TSDF layout, and checkpoints (TSDF + pose + frame index) ----
+
+kf_status kf_save_tsdf_file(kf_session* s, const char* path) {
+    if (!s || !path) return KF_ERR_ARG;
+    const Slot& sl = s->sl();
+    const size_t n3 = size_t(sl.cfg.volume_n) * sl.cfg.volume_n * sl.cfg.volume_n;
+    std::vector<float> host(n3 * 2);
+    KF_TRY(kf_get_tsdf(s, host.data(), n3 * 8, 1, 1));
+    FILE* f = std::fopen(path, "wb");
+    if (!f) return KF_ERR_ARG;
+    const size_t wrote = std::fwrite(host.data(), 1, n3 * 8, f);
+    const int closed = std::fclose(f);
+    return wrote == n3 * 8 && closed == 0 ? KF_OK : KF_ERR_ARG;
+}
+
+kf_status kf_load_tsdf_file(kf_session* s, const char* path) {
+    if (!s || !path) return KF_ERR_ARG;
+    const Slot& sl = s->sl();
+    const size_t n3 = size_t(sl.cfg.volume_n) * sl.cfg.volume_n * sl.cfg.volume_n;
+    FILE* f = std::fopen(path, "rb");
+    if (!f) return KF_ERR_ARG;
+    std::vector<float> host(n3 * 2);
+    const size_t got = std::fread(host.data(), 1, n3 * 8, f);
+    const bool extra = std::fgetc(f) != EOF;
+    std::fclose(f);
+    if (got != n3 * 8 || extra) return KF_ERR_SHAPE;   // a .bin of another volume size
+    return kf_set_tsdf(s, host.data(), n3 * 8, 1, 1);
+}
+
+kf_status kf_session_checkpoint_save(kf_session* s, const char* path) {
+    if (!s || !path) return KF_ERR_ARG;
+    KF_TRY(kf_save_tsdf_file(s, path));
+    float pose[16];
+    KF_TRY(kf_get_pose(s, pose));
+    const std::string side = std::string(path) + ".pose";
+    FILE* f = std::fopen(side.c_str(), "w");
+    if (!f) return KF_ERR_ARG;
+    std::fprintf(f, "kinectfusion-b200 checkpoint 1\nframes %d\npose", s->sl().frames);
+    for (int i = 0; i < 16; ++i) std::fprintf(f, " %.9g", double(pose[i]));
+    std::fprintf(f, "\n");
+    return std::fclose(f) == 0 ? KF_OK : KF_ERR_ARG;
+}
+
+kf_status kf_session_checkpoint_load(kf_session* s, const char* path) {
+    if (!s || !path) return KF_ERR_ARG;
+    const std::string side = std::string(path) + ".pose";
+    FILE* f = std::fopen(side.c_str(), "r");
+    if (!f) return KF_ERR_ARG;
+    int frames = -1;
+    float pose[16];
+    char head[64] = {0};
+    bool ok = std::fscanf(f, "%63[^\n]\nframes %d\npose", head, &frames) == 2 &&
+              std::strcmp(head, "kinectfusion-b200 checkpoint 1") == 0 && frames >= 0;
+    for (int i = 0; ok && i < 16; ++i) ok = std::fscanf(f, " %f", &pose[i]) == 1;
+    std::fclose(f);
+    if (!ok) return KF_ERR_ARG;
+    KF_TRY(kf_load_tsdf_file(s, path));
+    KF_TRY(kf_set_pose(s, pose));
+    // resume: the next frame is frame `frames` (tracking, not the first-frame fusion only)
+    Slot& sl = s->sl();
+    sl.frames = frames;
+    std::memcpy(sl.pose, pose, sizeof(pose));
+    PoseDev P;
+    KF_CK(cudaMemcpy(&P, sl.d.pose, sizeof(P), cudaMemcpyDeviceToHost));
+    P.frame = frames;
+    KF_CK(cudaMemcpy(sl.d.pose, &P, sizeof(P), cudaMemcpyHostToDevice));
+    return KF_OK;
+}
+
+// ---- headless display (project/src/display.cu) ----
+
+static kf_status display(int mode, const void* src, int w, int h, const DispMats& m, float scale, uint8_t* rgba,
+                         void* stream, float* elapsed_ms) {
+    if (!src || !rgba || w <= 0 || h <= 0) return KF_ERR_ARG;
+    StageTimer t(elapsed_ms, as_stream(stream));
+    return t.finish(stage_display(mode, src, w, h, m, scale, reinterpret_cast<unsigned int*>(rgba), as_stream(stream)));
+}
+
+kf_status kf_normal_map_to_rgba(const float* normal, int w, int h, const float inv_rot[9], uint8_t* rgba, void* stream,
+                                float* elapsed_ms) {
+    if (!inv_rot) return KF_ERR_ARG;
+    DispMats m{};
+    std::memcpy(m.r, inv_rot, sizeof(m.r));
+    return display(kDisplayNormals, normal, w, h, m, 0.f, rgba, stream, elapsed_ms);
+}
+
+kf_status kf_shading_to_rgba(const float* normal, int w, int h, const float pose[16], const float inv_cam_k[9],
+                             uint8_t* rgba, void* stream, float* elapsed_ms) {
+    if (!pose || !inv_cam_k) return KF_ERR_ARG;
+    DispMats m{};
+    for (int c = 0; c < 3; ++c)
+        for (int r = 0; r < 3; ++r) m.r[c * 3 + r] = pose[c * 4 + r];
+    std::memcpy(m.ik, inv_cam_k, sizeof(m.ik));
+    return display(kDisplayShading, normal, w, h, m, 0.f, rgba, stream, elapsed_ms);
+}
+
+kf_status kf_float_channel_to_rgba(const float* src, int w, int h, float scale, uint8_t* rgba, void* stream,
+                                   float* elapsed_ms) {
+    DispMats m{};
+    return display(kDisplayFloat, src, w, h, m, scale, rgba, stream, elapsed_ms);
+}
+
+kf_status kf_render(kf_session* s, int mode, const float pose_in[16], uint8_t* rgba, int to_host, void* stream) {
+    if (!s || !rgba || (mode != KF_RENDER_NORMALS && mode != KF_RENDER_SHADING)) return KF_ERR_ARG;
+    Slot& sl = s->sl();
+    if (sl.external) return KF_ERR_STATE;
+    const kf_config& c = sl.cfg;
+    const int w = c.width, h = c.height;
+    cudaStream_t st = as_stream(stream);
+    if (!sl.render_v) {
+        cudaError_t err = cudaSuccess;
+        sl.render_v = static_cast<float4*>(sl.alloc(size_t(w) * h * 16, err));
+        if (err == cudaSuccess) sl.render_n = static_cast<float4*>(sl.alloc(size_t(w) * h * 16, err));
+        if (err == cudaSuccess) sl.render_rgba = static_cast<unsigned int*>(sl.alloc(size_t(w) * h * 4, err));
+        if (err != cudaSuccess) { g_last_cuda = err; sl.render_v = sl.render_n = nullptr; return KF_ERR_CUDA; }
+    }
+    float pose[16];
+    if (pose_in) std::memcpy(pose, pose_in, sizeof(pose));
+    else KF_TRY(kf_get_pose(s, pose));
+    float k[9], ik[9];
+    level_intrinsics(c, 0, k, ik);
+    kf_volume vol;
+    KF_TRY(kf_get_volume(s, &vol));
+    // the reference raycasts the model at level 0 into the predicted maps, then displays
+    // (KinectFusion::visualizeCurrentModel, project/src/kinect_fusion.cpp:185-203); the
+    // tracking maps are left alone here
+    KF_CK(cudaStreamSynchronize(st));
+    KF_CK(cudaMemsetAsync(sl.render_v, 0, size_t(w) * h * 16, st));
+    KF_CK(cudaMemsetAsync(sl.render_n, 0, size_t(w) * h * 16, st));
+    KF_CK(stage_raycast(&vol, pose, ik, sl.render_v, sl.render_n, w, h, c.min_depth, c.max_depth, c.step_large,
+                        c.step_small, st, &sl.d));
+    DispMats m{};
+    if (mode == KF_RENDER_NORMALS) {
+        for (int cc = 0; cc < 3; ++cc)
+            for (int r = 0; r < 3; ++r) m.r[cc * 3 + r] = pose[r * 4 + cc];   // inverse rotation R^T
+    } else {
+        for (int cc = 0; cc < 3; ++cc)
+            for (int r = 0; r < 3; ++r) m.r[cc * 3 + r] = pose[cc * 4 + r];
+        std::memcpy(m.ik, ik, sizeof(ik));
+    }
+    KF_CK(stage_display(mode == KF_RENDER_NORMALS ? kDisplayNormals : kDisplayShading, sl.render_n, w, h, m, 0.f,
+                        sl.render_rgba, st));
+    KF_CK(cudaMemcpyAsync(rgba, sl.render_rgba, size_t(w) * h * 4,
+                          to_host ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice, st));
+    KF_CK(cudaStreamSynchronize(st));
     return KF_OK;
 }
 

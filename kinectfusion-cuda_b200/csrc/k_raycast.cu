@@ -420,8 +420,15 @@ __global__ void raycast_stage_kernel(SessionDev S, RayStage rs, int w, int h) {
 }
 
 cudaError_t stage_raycast(const kf_volume* vol, const float* pose, const float* ik, float4* vtx, float4* nrm, int w,
-                          int h, float min_d, float max_d, float step_l, float step_s, cudaStream_t st) {
+                          int h, float min_d, float max_d, float step_l, float step_s, cudaStream_t st,
+                          const SessionDev* bounds) {
     SessionDev S{};
+    if (bounds) {   // a session's brick bounds: the same samples, skipping exactly as the pipeline
+        S.bdil = bounds->bdil;
+        S.sdil = bounds->sdil;
+        S.nb = bounds->nb;
+        S.ns = bounds->ns;
+    }
     S.n = vol->n;
     S.fmt = vol->format;
     S.vol_w = vol->width;

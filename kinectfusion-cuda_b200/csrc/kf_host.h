@@ -85,8 +85,18 @@ cudaError_t stage_bilateral(const float* in, float* out, int w, int h, float ss,
 cudaError_t stage_down_sample(const float* in, float* out, int wo, int ho, float sr, cudaStream_t st);
 cudaError_t stage_vertex(const float* d, float4* v, int w, int h, const float* ik, cudaStream_t st);
 cudaError_t stage_normal(const float4* v, float4* n, int w, int h, cudaStream_t st);
+// bounds (optional): a session whose brick bounds the march may use to skip
 cudaError_t stage_raycast(const kf_volume* vol, const float* pose, const float* ik, float4* vtx, float4* nrm, int w,
-                          int h, float min_d, float max_d, float step_l, float step_s, cudaStream_t st);
+                          int h, float min_d, float max_d, float step_l, float step_s, cudaStream_t st,
+                          const SessionDev* bounds = nullptr);
+// headless display (project/src/display.cu): RGBA8 images
+constexpr int kDisplayNormals = 0, kDisplayShading = 1, kDisplayFloat = 2;
+struct DispMats {
+    float r[9];    // normals: inverse sensor rotation; shading: sensor rotation (column-major)
+    float ik[9];   // shading: inverse intrinsics (column-major)
+};
+cudaError_t stage_display(int mode, const void* src, int w, int h, const DispMats& m, float scale, unsigned int* out,
+                          cudaStream_t st);
 cudaError_t stage_fuse(const float* depth, int w, int h, const float* k, const kf_volume* vol, const float* pose,
                        float min_d, float max_d, const float* xs, const float* zs, cudaStream_t st);
 cudaError_t stage_icp_residuals(const float4* vmap, const float4* tv, const float4* tn, int w, int h,

@@ -14,17 +14,20 @@ indexed [row, col]; they are converted to the column-major layout of the C ABI a
 boundary.  Every call goes through the CUDA library; there is no CPU path.
 """
 import ctypes
+import os
 
 import numpy as np
 
 from . import _lib
 from ._lib import (KF_ERR_ARG, KF_ERR_CAPACITY, KF_ERR_CUDA, KF_ERR_NONFINITE, KF_ERR_OOM_BUDGET, KF_ERR_SHAPE,
-                   KF_ERR_STATE, KF_ERR_TIMEOUT, KF_MAX_LEVELS, KF_OK, KF_TSDF_F16U16, KF_TSDF_F32F32, KF_WEIGHT_SCALE,
-                   KfConfig, KfError, KfFrameStats, KfServerStats, KfVolume, check, lib)
+                   KF_ERR_STATE, KF_ERR_TIMEOUT, KF_MAX_LEVELS, KF_OK, KF_RENDER_NORMALS, KF_RENDER_SHADING,
+                   KF_TSDF_F16U16, KF_TSDF_F32F32, KF_WEIGHT_SCALE, KfConfig, KfError, KfFrameStats, KfServerStats,
+                   KfVolume, check, lib)
 
 __all__ = [
     "KfConfig", "KfError", "default_config", "config_small", "config_full", "KinectFusion", "kernel", "ICP",
-    "LinearLeastSquares", "poseError", "Batch", "Server", "lib", "to_colmajor", "from_colmajor",
+    "LinearLeastSquares", "poseError", "Batch", "Server", "RgbdDataset", "read_png16", "lib", "to_colmajor",
+    "from_colmajor",
 ]
 
 
@@ -247,18 +250,29 @@ class KinectFusion:
         check(lib.kf_set_tsdf(self._s, _np_ptr(inter), inter.nbytes, 1, 1))
 
     def saveTSDF(self, path):
-        """Reference .bin layout: n^3 float2 {f, w}, x fastest (project/src/voxel_grid.cpp:43-62)."""
-        n = self.config.volume_n
-        inter = np.empty((n, n, n, 2), np.float32)
-        check(lib.kf_get_tsdf(self._s, _np_ptr(inter), inter.nbytes, 1, 1))
-        inter.tofile(path)
+        """VoxelGrid::saveVoxelGrid (project/src/voxel_grid.cpp:43-62): n^3 float2 {f, w}, x fastest."""
+        check(lib.kf_save_tsdf_file(self._s, os.fsencode(path)), "kf_save_tsdf_file")
 
     def loadTSDF(self, path):
-        n = self.config.volume_n
-        inter = np.fromfile(path, dtype=np.float32, count=n * n * n * 2)
-        if inter.size != n * n * n * 2:
-            raise ValueError("TSDF file is too short")
-        check(lib.kf_set_tsdf(self._s, _np_ptr(inter), inter.nbytes, 1, 1))
+        """VoxelGrid::loadVoxelGrid (project/src/voxel_grid.cpp:64-80)."""
+        check(lib.kf_load_tsdf_file(self._s, os.fsencode(path)), "kf_load_tsdf_file")
+
+    def saveCheckpoint(self, path):
+        """TSDF (.bin at path) + pose and frame count (path + '.pose')."""
+        check(lib.kf_session_checkpoint_save(self._s, os.fsencode(path)), "kf_session_checkpoint_save")
+
+    def loadCheckpoint(self, path):
+        """Resume a saved session: the next frame tracks against the loaded model."""
+        check(lib.kf_session_checkpoint_load(self._s, os.fsencode(path)), "kf_session_checkpoint_load")
+
+    def render(self, mode=KF_RENDER_NORMALS, pose=None, stream=None):
+        """KinectFusion::visualizeCurrentModel, headless: (h, w, 4) uint8 RGBA image of the model
+        raycast from `pose` (default: the current pose)."""
+        c = self.config
+        img = np.empty((c.height, c.width, 4), np.uint8)
+        pp = to_colmajor(pose) if pose is not None else None
+        check(lib.kf_render(self._s, int(mode), pp, _np_ptr(img), 1, _stream(stream)), "kf_render")
+        return img
 
     def volume(self):
         v = KfVolume()
@@ -360,6 +374,27 @@ class kernel:  # noqa: N801 -- mirrors the reference's C++ namespace
                           step_small, _stream(stream))
 
     @staticmethod
+    def normalMapToWindowContent(normal, inverse_rotation, rgba, stream=None):
+        """project/src/display.cu:143-154, into an (h, w, 4) uint8 device image."""
+        h, w = normal.shape[:2]
+        return kernel._ms(lib.kf_normal_map_to_rgba, _dev_ptr(normal), w, h, to_colmajor(inverse_rotation),
+                          _dev_ptr(rgba), _stream(stream))
+
+    @staticmethod
+    def shadingToWindowContent(normal, pose, inv_cam_k, rgba, stream=None):
+        """project/src/display.cu:156-167."""
+        h, w = normal.shape[:2]
+        return kernel._ms(lib.kf_shading_to_rgba, _dev_ptr(normal), w, h, to_colmajor(pose), to_colmajor(inv_cam_k),
+                          _dev_ptr(rgba), _stream(stream))
+
+    @staticmethod
+    def oneFloatChannelToWindowContent(src, scale, rgba, stream=None):
+        """project/src/display.cu:117-128."""
+        h, w = src.shape[:2]
+        return kernel._ms(lib.kf_float_channel_to_rgba, _dev_ptr(src), w, h, float(scale), _dev_ptr(rgba),
+                          _stream(stream))
+
+    @staticmethod
     def constructIcpResiduals(vertex, target_vertex, target_normal, prev_rot, prev_transl, cur_rot, cur_transl,
                               cam_k, distance_thresh, angle_thresh, mat_a, vec_b, stream=None):
         h, w = vertex.shape[:2]
@@ -410,6 +445,76 @@ def poseError(pose_1, pose_2):
     out = (ctypes.c_float * 2)()
     check(lib.kf_pose_error(to_colmajor(pose_1), to_colmajor(pose_2), out))
     return float(out[0]), float(out[1])
+
+
+# ------------------------------------------------------------------------------------------
+# datasets
+# ------------------------------------------------------------------------------------------
+class RgbdDataset:
+    """RgbdDataset (project/src/rgbd_dataset.h:12-27): a TUM RGB-D sequence directory, read by
+    the library (kf_tum_*).  Frames come back as (h, w) uint16 depth and a 4x4 ground-truth
+    camera->world pose."""
+
+    def __init__(self, path=None):
+        self._d = None
+        self.m_current_index = 0
+        if path is not None:
+            self.load(path)
+
+    def load(self, path):
+        self.close()
+        h = ctypes.c_void_p()
+        check(lib.kf_tum_open(os.fsencode(path), ctypes.byref(h)), "kf_tum_open")
+        self._d = h
+        self.m_current_index = 0
+
+    def close(self):
+        if self._d:
+            lib.kf_tum_close(self._d)
+        self._d = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __len__(self):
+        n = ctypes.c_int()
+        check(lib.kf_tum_count(self._d, ctypes.byref(n)))
+        return n.value
+
+    def frame(self, index, width=640, height=480):
+        depth = np.empty((height, width), np.uint16)
+        pose = (ctypes.c_float * 16)()
+        check(lib.kf_tum_frame(self._d, int(index), _np_ptr(depth), width, height, pose), "kf_tum_frame")
+        return depth, from_colmajor(pose, 4)
+
+    def getCurrentPose(self):
+        pose = (ctypes.c_float * 16)()
+        check(lib.kf_tum_frame(self._d, self.m_current_index, None, 0, 0, pose), "kf_tum_frame")
+        return from_colmajor(pose, 4)
+
+    def getInitialPoseInverse(self):
+        out = (ctypes.c_float * 16)()
+        check(lib.kf_tum_initial_pose_inverse(self._d, out), "kf_tum_initial_pose_inverse")
+        return from_colmajor(out, 4)
+
+    def nextFrame(self, width=640, height=480):
+        """The next depth image and its pose (getNextDepthImagePath + DepthMap::update)."""
+        out = self.frame(self.m_current_index, width, height)
+        self.m_current_index += 1
+        return out
+
+    def isFinished(self):
+        return self.m_current_index >= len(self)
+
+
+def read_png16(path, width, height):
+    """A 16-bit greyscale PNG (DepthMap::update(path)) as an (h, w) uint16 array."""
+    depth = np.empty((height, width), np.uint16)
+    check(lib.kf_png16_read(os.fsencode(path), _np_ptr(depth), width, height), "kf_png16_read")
+    return depth
 
 
 # ------------------------------------------------------------------------------------------

@@ -24,6 +24,8 @@ KF_ERR_STATE = 7
 KF_ERR_CAPACITY = 8
 KF_ERR_TOO_LARGE = 9
 KF_LLS_NOALLOC_MAX_ROWS = 1048576   # row limit of kf_solve_linear_least_squares_noalloc
+KF_RENDER_NORMALS = 0
+KF_RENDER_SHADING = 1
 
 KF_TSDF_F32F32 = 0
 KF_TSDF_F16U16 = 1
@@ -134,6 +136,20 @@ SIGNATURES = {
     "kf_server_stats_get": (_I, [_P, ctypes.POINTER(KfServerStats)]),
     "kf_server_stats_reset": (_I, [_P]),
     "kf_server_reserve": (_I, [_P, _CFG, _I]),
+    "kf_save_tsdf_file": (_I, [_P, ctypes.c_char_p]),
+    "kf_load_tsdf_file": (_I, [_P, ctypes.c_char_p]),
+    "kf_session_checkpoint_save": (_I, [_P, ctypes.c_char_p]),
+    "kf_session_checkpoint_load": (_I, [_P, ctypes.c_char_p]),
+    "kf_normal_map_to_rgba": (_I, [_P, _I, _I, _FP, _P, _P, _FP]),
+    "kf_shading_to_rgba": (_I, [_P, _I, _I, _FP, _FP, _P, _P, _FP]),
+    "kf_float_channel_to_rgba": (_I, [_P, _I, _I, _F, _P, _P, _FP]),
+    "kf_render": (_I, [_P, _I, _FP, _P, _I, _P]),
+    "kf_tum_open": (_I, [ctypes.c_char_p, ctypes.POINTER(_P)]),
+    "kf_tum_close": (_I, [_P]),
+    "kf_tum_count": (_I, [_P, _IP]),
+    "kf_tum_frame": (_I, [_P, _I, _P, _I, _I, _FP]),
+    "kf_tum_initial_pose_inverse": (_I, [_P, _FP]),
+    "kf_png16_read": (_I, [ctypes.c_char_p, _P, _I, _I]),
     "kf_now_ms": (ctypes.c_double, []),
     "kf_session_set_profiling": (_I, [_P, _I]),
     "kf_session_stage_times": (_I, [_P, _FP]),

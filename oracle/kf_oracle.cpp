@@ -1139,4 +1139,44 @@ long long kfo_pipeline_last_fused(void* h) {
     return s;
 }
 
+// ---- display kernels (project/src/display.cu:63-105), RGBA8 out ----
+
+// static_cast<unsigned char>(x) on the device: truncation, saturated to [0, 255], NaN -> 0
+static unsigned to_u8(float x) {
+    if (!(x > 0.0f)) return 0u;
+    if (x >= 255.0f) return 255u;
+    return unsigned(x);
+}
+
+// normalMapToWindowContentKernel (display.cu:63-81): normalize(Rinv * n) * 255 as r, g, b
+void kfo_display_normals(const float* nm, int w, int h, const float rinv[9], unsigned char* rgba) {
+    for (int j = 0; j < h; ++j)
+        for (int i = 0; i < w; ++i) {
+            const float* n = nm + (size_t(j) * w + i) * 4;
+            float v[3];
+            for (int r = 0; r < 3; ++r) v[r] = rinv[r] * n[0] + rinv[3 + r] * n[1] + rinv[6 + r] * n[2];
+            const float s = 1.0f / std::sqrt(v[0] * v[0] + v[1] * v[1] + v[2] * v[2]);
+            unsigned char* o = rgba + (size_t(j) * w + i) * 4;
+            for (int r = 0; r < 3; ++r) o[r] = (unsigned char)to_u8(v[r] * s * 255.0f);
+            o[3] = 255;
+        }
+}
+
+// shadingToWindowContentKernel (display.cu:83-105): min(|n . normalize(R K^-1 (i+.5, j+.5, 1))|, 1)
+void kfo_display_shading(const float* nm, int w, int h, const float pose[16], const float ik[9], unsigned char* rgba) {
+    for (int j = 0; j < h; ++j)
+        for (int i = 0; i < w; ++i) {
+            const float p[3] = {float(i) + 0.5f, float(j) + 0.5f, 1.0f};
+            float q[3], d[3];
+            for (int r = 0; r < 3; ++r) q[r] = ik[r] * p[0] + ik[3 + r] * p[1] + ik[6 + r] * p[2];
+            for (int r = 0; r < 3; ++r) d[r] = pose[r] * q[0] + pose[4 + r] * q[1] + pose[8 + r] * q[2];
+            const float s = 1.0f / std::sqrt(d[0] * d[0] + d[1] * d[1] + d[2] * d[2]);
+            const float* n = nm + (size_t(j) * w + i) * 4;
+            const float rad = std::min(std::fabs((n[0] * d[0] + n[1] * d[1] + n[2] * d[2]) * s), 1.0f);
+            unsigned char* o = rgba + (size_t(j) * w + i) * 4;
+            o[0] = o[1] = o[2] = (unsigned char)to_u8(rad * 255.0f);
+            o[3] = 255;
+        }
+}
+
 }  // extern "C"

@@ -62,6 +62,8 @@ _SIG = {
     "kfo_pipeline_set_tsdf": (_I, [_P, _P, _P]),
     "kfo_pipeline_last_samples": (_LL, [_P, _I]),
     "kfo_pipeline_last_fused": (_LL, [_P]),
+    "kfo_display_normals": (None, [_P, _I, _I, _P, _P]),
+    "kfo_display_shading": (None, [_P, _I, _I, _P, _P, _P]),
 }
 for _n, (_r, _a) in _SIG.items():
     _f = getattr(_lib, _n)
@@ -322,3 +324,21 @@ class Pipeline:
 
     def last_fused(self):
         return _lib.kfo_pipeline_last_fused(self._h)
+
+
+def display_normals(nmap, inv_rot):
+    """normalMapToWindowContentKernel (project/src/display.cu:63-81) -> (h, w, 4) uint8."""
+    n = np.ascontiguousarray(nmap, np.float32)
+    h, w = n.shape[:2]
+    out = np.zeros((h, w, 4), np.uint8)
+    _lib.kfo_display_normals(_p(n), w, h, _p(_cm(inv_rot)), _p(out))
+    return out
+
+
+def display_shading(nmap, pose, inv_k):
+    """shadingToWindowContentKernel (project/src/display.cu:83-105) -> (h, w, 4) uint8."""
+    n = np.ascontiguousarray(nmap, np.float32)
+    h, w = n.shape[:2]
+    out = np.zeros((h, w, 4), np.uint8)
+    _lib.kfo_display_shading(_p(n), w, h, _p(_cm(pose)), _p(_cm(inv_k)), _p(out))
+    return out
