@@ -63,45 +63,78 @@ def ncu_traffic():
 
 
 class ClockSampler:
-    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+    """SM clocks and throttle reasons sampled during the timed region (NVML every 10 ms; the
+    nvidia-smi query of the same fields when NVML is not importable)."""
 
     QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    NAMES = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
 
     def __init__(self, index):
         self.index = index
-        self.rows = []
+        self.sm = []
+        self.max_sm = None
+        self.reasons = set()
         self._stop = threading.Event()
         self._t = None
 
+    def _nvml_loop(self, nv):
+        h = nv.nvmlDeviceGetHandleByIndex(self.index)
+        self.max_sm = float(nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM))
+        bits = {"hw_slowdown": 0x8, "hw_thermal_slowdown": 0x40, "sw_thermal_slowdown": 0x20, "sw_power_cap": 0x4}
+        while not self._stop.is_set():
+            self.sm.append(float(nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM)))
+            r = nv.nvmlDeviceGetCurrentClocksEventReasons(h) if hasattr(nv, "nvmlDeviceGetCurrentClocksEventReasons") \
+                else nv.nvmlDeviceGetCurrentClocksThrottleReasons(h)
+            for name, bit in bits.items():
+                if r & bit:
+                    self.reasons.add(name)
+            self._stop.wait(0.01)
+
+    def _smi_loop(self):
+        while not self._stop.is_set():
+            try:
+                out = subprocess.run(["nvidia-smi", "-i", str(self.index), "--query-gpu=" + self.QUERY,
+                                      "--format=csv,noheader,nounits"], capture_output=True, text=True,
+                                     timeout=5).stdout.strip()
+            except Exception:
+                return
+            r = [x.strip() for x in out.split(",")]
+            if len(r) >= 9:
+                if r[1].replace(".", "").isdigit():
+                    self.sm.append(float(r[1]))
+                if r[2].replace(".", "").isdigit():
+                    self.max_sm = float(r[2])
+                for i, name in enumerate(self.NAMES):
+                    if r[5 + i] == "Active":
+                        self.reasons.add(name)
+            self._stop.wait(0.2)
+
     def start(self):
         def run():
-            while not self._stop.is_set():
+            try:
+                import pynvml as nv
+                nv.nvmlInit()
                 try:
-                    out = subprocess.run(["nvidia-smi", "-i", str(self.index), "--query-gpu=" + self.QUERY,
-                                          "--format=csv,noheader,nounits"], capture_output=True, text=True,
-                                         timeout=5).stdout.strip()
-                    if out:
-                        self.rows.append([x.strip() for x in out.split(",")])
-                except Exception:
-                    return
-                self._stop.wait(0.2)
+                    self._nvml_loop(nv)
+                finally:
+                    nv.nvmlShutdown()
+            except Exception:
+                if not self.sm:
+                    self._smi_loop()
         self._t = threading.Thread(target=run, daemon=True)
         self._t.start()
+        time.sleep(0.02)
 
     def stop(self):
         self._stop.set()
         if self._t:
             self._t.join(timeout=10)
-        if not self.rows:
+        if not self.sm:
             return None
-        sm = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
-        mx = [float(r[2]) for r in self.rows if r[2].replace(".", "").isdigit()]
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        reasons = sorted({names[i] for r in self.rows for i in range(4) if len(r) > 5 + i and r[5 + i] == "Active"})
-        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
-                "reasons": reasons, "samples": len(self.rows)}
+        return {"sm_mhz": float(np.median(self.sm)), "sm_max_mhz": self.max_sm, "reasons": sorted(self.reasons),
+                "samples": len(self.sm)}
 
 
 def dist_setup():
@@ -485,6 +518,85 @@ def run_served(kf, torch, seconds, seed=11):
             "latency": "arrival of the frame (client queueing included) to result ready"}
 
 
+# ---------------------------------------------------------------------------------------------
+# accuracy against the FP64 oracle (rank 0, N = 1)
+# ---------------------------------------------------------------------------------------------
+def synced_errors(kf, orc, cfg, imgs):
+    """Per frame, the oracle (FP64) starts from the device's TSDF and pose, then both process
+    the frame.  Returns max pose error, TSDF RMS (truncation units, voxels both observed),
+    raycast depth error (mm, pixels where both hit) and ICP-mask agreement."""
+    s = kf.KinectFusion(kf.KfConfig.from_buffer_copy(cfg))
+    P = orc.Pipeline(cfg, prec=1)
+    worst_a = worst_d = same_a = same_d = 0.0
+    rms, ray_mm, ray_hit = [], [], []
+    flips = 0
+    for k, img in enumerate(imgs):
+        f, w = s.tsdf()
+        P.set_tsdf(f, w)
+        P.set_pose(s.pose())
+        cam = s.pose()[:3, 3].astype(np.float64)
+        P.process_frame(img)
+        s.process_frame(img)
+        a, d = kf.poseError(P.pose(), s.pose())
+        worst_a, worst_d = max(worst_a, a), max(worst_d, d)
+        if list(P.iters()) == list(s.frame_stats()["icp_iters"]):
+            same_a, same_d = max(same_a, a), max(same_d, d)
+        else:
+            flips += 1   # the 0.1 deg / 1 cm early stop decided differently: one more or fewer pass
+        if k == 0:
+            continue
+        gf, gw = s.tsdf()
+        of, ow = P.tsdf()
+        both = (gw > 0) & (ow > 0)
+        rms.append(float(np.sqrt(np.mean((gf[both].astype(np.float64) - of[both]) ** 2))))
+        gv, _ = s.raycast_maps(0)
+        ov, _ = P.raycast_maps(0)
+        gh, oh = gv[..., 3] == -1, ov[..., 3] == -1
+        ray_hit.append(float(np.mean(gh == oh)))
+        m = gh & oh
+        if m.any():
+            dz = np.abs(np.linalg.norm(gv[m][:, :3] - cam, axis=1) - np.linalg.norm(ov[m][:, :3] - cam, axis=1))
+            ray_mm.append(dz * 1000.0)
+    s.close()
+    P.close()
+    mm = np.concatenate(ray_mm) if ray_mm else np.zeros(1)
+    return {"frames": len(imgs), "pose_rad_max": float(worst_a), "pose_m_max": float(worst_d),
+            "frames_icp_iterations_differ": flips,
+            "pose_rad_max_same_iterations": float(same_a), "pose_m_max_same_iterations": float(same_d),
+            "tsdf_rms_trunc_max": float(max(rms)) if rms else None,
+            "raycast_mm_max": round(float(mm.max()), 4), "raycast_mm_p999": round(float(np.quantile(mm, 0.999)), 4),
+            "raycast_hit_agreement_min": round(float(min(ray_hit)), 5) if ray_hit else None}
+
+
+def drift(kf, orc, cfg, imgs):
+    """Free-running: device and FP64 oracle each track the whole sequence; final pose error."""
+    s = kf.KinectFusion(kf.KfConfig.from_buffer_copy(cfg))
+    P = orc.Pipeline(cfg, prec=1)
+    for img in imgs:
+        s.process_frame(img)
+        P.process_frame(img)
+    a, d = kf.poseError(P.pose(), s.pose())
+    s.close()
+    P.close()
+    return {"frames": len(imgs), "pose_rad": float(a), "pose_m": float(d)}
+
+
+def run_accuracy(kf, full_frames=6, small_frames=30, drift_frames=150):
+    import oracle as orc
+    from kfb200 import synth
+    out = {"reference": "FP64 CPU restatement (oracle/kf_oracle.cpp), synced per frame from the device state"}
+    small = kf.config_small()
+    imgs, _ = synth.sequence(small, max(small_frames, drift_frames), seed=61)
+    out["small_f32"] = synced_errors(kf, orc, small, imgs[:small_frames])
+    s16 = kf.config_small(tsdf_format=kf.KF_TSDF_F16U16)
+    out["small_f16u16"] = synced_errors(kf, orc, s16, imgs[:small_frames])
+    out["small_f16u16_drift"] = drift(kf, orc, s16, imgs[:drift_frames])
+    full = kf.config_full(tsdf_format=kf.KF_TSDF_F16U16)
+    fimgs, _ = synth.sequence(full, full_frames, seed=63, kind=synth.LOOP)
+    out["full_f16u16"] = synced_errors(kf, orc, full, fimgs)
+    return out
+
+
 def run_ours(args, world, rank, local):
     import torch
     import kfb200 as kf
@@ -638,6 +750,10 @@ def run_ours(args, world, rank, local):
             out["batched"] = run_batched(kf, torch, min(steps, 150), value)
         if not args.no_served:
             out["served"] = run_served(kf, torch, args.served_seconds)
+        if not args.no_accuracy:
+            progress("accuracy: start")
+            out["accuracy"] = run_accuracy(kf)
+            progress("accuracy: done")
     if dist is not None:
         dist.barrier()
         dist.destroy_process_group()
@@ -669,6 +785,7 @@ def main():
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
     ap.add_argument("--no-batched", action="store_true", help="skip the batched-form measurement")
     ap.add_argument("--no-served", action="store_true", help="skip the served-form measurement")
+    ap.add_argument("--no-accuracy", action="store_true", help="skip the error report against the FP64 oracle")
     ap.add_argument("--served-seconds", type=float, default=20.0,
                     help="length of the served run (the 64-session schedule is scaled to it)")
     ap.add_argument("--profile-frames", type=int, default=0,
