@@ -1,7 +1,7 @@
 // kf_oracle.cpp -- TEST INFRASTRUCTURE ONLY.
 //
 // CPU restatement of the per-frame KinectFusion path of isikmustafa/kinectfusion-cuda
-// (project/src).  It is the checker for the CUDA library in kinectfusion-cuda_b200/ and the
+// (project/src).  It is the reference the tests compare the CUDA library in kinectfusion-cuda_b200/ with, and the
 // timed CPU baseline of bench.py; the product never links, loads or calls it.  Only tests/,
 // __graft_entry__.smoke() and bench.py's CPU legs load it.
 //

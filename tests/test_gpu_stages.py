@@ -3,7 +3,7 @@ inputs, plus the reference's own known answers on the device.
 
 Tolerances (floating point, stated per test): values from the fused/fast-exp kernels agree
 with the float oracle to ~1e-6 relative; masks and integer decisions agree exactly except
-where stated; raycast depths agree within 1 mm where both hit (the north-star bound)."""
+where stated; raycast depths agree within 1 mm where both hit."""
 import json
 import os
 
