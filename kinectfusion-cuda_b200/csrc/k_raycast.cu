@@ -7,15 +7,20 @@
 // it, and the march does its own trilinear interpolation with the reference's texel mapping
 // (uvw * n - 0.5, clamp).  Every sample the reference takes is taken at the same float
 // position, in the same order; three things make that fast:
-//   - Skipping: a sample whose eight taps lie in cells (32^3 super-bricks during large steps,
-//     then 8^3 bricks) whose distance lower bound proves it cannot change the march (>= 0.991
-//     during large steps, >= 0.001 during small steps) is not evaluated, nor is any later
-//     sample in the same cell; t still advances by the reference's repeated float additions.
+//   - Skipping: a sample whose eight taps lie in cells (32^3 super-bricks, then 8^3 bricks)
+//     whose distance lower bound proves it cannot change the march (>= 0.991 during large
+//     steps, >= 0.001 during small steps) is not evaluated, nor is any later sample in the
+//     same cell; t still lands on the reference's repeated float additions (the first eight
+//     one by one, longer runs in closed form within each binade, kf_march.h).  Rays that pass
+//     within mu of a surface without crossing it keep 0.1 mu steps to the far plane (the
+//     reference never returns to large steps); super-bricks let them cross free space 94 steps
+//     at a time.
 //   - Load balance: each warp pulls 8 x 4-ray tiles from an atomic counter, and a lane marches
 //     at most 64 iterations; longer rays are queued with their exact march state.
 //   - Long rays: a second kernel marches each queued ray with a whole warp, 32 consecutive
 //     samples per round, taking the first sample (in order) that changes the state.
 #include "kf_host.h"
+#include "kf_march.h"
 
 namespace kf {
 
@@ -124,60 +129,60 @@ __device__ __forceinline__ float box_exit(const RayGeo& g, int n, int lox, int h
 // The reference's march loop for one lane (project/src/raycast.cu:75-117).  Returns 1 when
 // the ray is finished (precise = refined hit distance, 0 for none) and 0 when `budget`
 // iterations ran out with the ray still marching (state kept in st).
+// Samples whose base voxel lies in a cell whose distance lower bound is at or above the
+// current threshold (0.991 during large steps, 0.001 during small steps) cannot change the
+// march.  If the sample at st.t is such a sample, advance st past every following sample in the
+// same cell -- its 32^3 super-brick when that one qualifies, else its 8^3 brick -- by the
+// reference's own float additions, and return true.
+__device__ __forceinline__ bool skip_cell(const SessionDev* S, const RayGeo& g, RayState& st, float x, float y, float z,
+                                          float inc) {
+    const int n = S->n;
+    const int vx = min(max(int(floorf(x)), 0), n - 1);
+    const int vy = min(max(int(floorf(y)), 0), n - 1);
+    const int vz = min(max(int(floorf(z)), 0), n - 1);
+    // order-preserving int keys of the two thresholds
+    const int thr = st.small ? __float_as_int(0.001f) : __float_as_int(0.991f);
+    int lo[3], hi[3];
+    const int sx = vx >> 5, sy = vy >> 5, sz = vz >> 5;
+    if (__ldg(S->sdil + (size_t(sz) * S->ns + sy) * S->ns + sx) >= thr) {
+        lo[0] = sx * 32; lo[1] = sy * 32; lo[2] = sz * 32;
+        hi[0] = lo[0] + 32; hi[1] = lo[1] + 32; hi[2] = lo[2] + 32;
+    } else {
+        const int bx = vx >> 3, by = vy >> 3, bz = vz >> 3;
+        if (__ldg(S->bdil + (size_t(bz) * S->nb + by) * S->nb + bx) < thr) return false;
+        lo[0] = bx * 8; lo[1] = by * 8; lo[2] = bz * 8;
+        hi[0] = lo[0] + 8; hi[1] = lo[1] + 8; hi[2] = lo[2] + 8;
+    }
+    // skip this sample and every later one whose base voxel stays in the box
+    const float t_safe = box_exit(g, n, lo[0], hi[0], lo[1], hi[1], lo[2], hi[2], st.far_d);
+    // first steps one by one (most skips are short), the rest in closed form
+    const float lim = fminf(t_safe, st.far_d);
+    int k = 0;
+    do {
+        st.prev_t = st.t;
+        st.t += inc;
+        ++st.guard;
+        ++k;
+    } while (st.t < lim && st.guard < kMaxMarchSamples && k < 8);
+    if (st.t < lim && st.guard < kMaxMarchSamples)
+        st.guard += advance_steps(st.t, st.prev_t, inc, lim, kMaxMarchSamples - st.guard);
+    st.prev_known = 0;
+    return true;
+}
+
 template <class TF>
 __device__ int march_serial(const SessionDev* S, const RayGeo& g, const TF* f, RayState& st, int budget,
                             float& precise) {
     const int n = S->n;
     const float mu = S->mu, large = mu * S->step_l, small = mu * S->step_s;
     const int* __restrict__ bdil = S->bdil;
-    const int* __restrict__ sdil = S->sdil;
-    const int nb = S->nb, ns = S->ns;
-    // order-preserving int keys of the two skip thresholds
-    const int k_large = __float_as_int(0.991f), k_small = __float_as_int(0.001f);
     int iters = 0;
     while (st.t < st.far_d && st.guard < kMaxMarchSamples) {
         if (iters++ >= budget) return 0;
         const float inc = st.small ? small : large;
         float x, y, z;
         texel(g, st.t, x, y, z);
-        if (bdil) {
-            const int vx = min(max(int(floorf(x)), 0), n - 1);
-            const int vy = min(max(int(floorf(y)), 0), n - 1);
-            const int vz = min(max(int(floorf(z)), 0), n - 1);
-            // the skippable box around the sample's base voxel, in voxels: its super-brick
-            // (large steps), else its brick
-            int lox = 0, hix = 0, loy = 0, hiy = 0, loz = 0, hiz = 0;
-            bool skip = false;
-            if (!st.small) {
-                const int sx = vx >> 5, sy = vy >> 5, sz = vz >> 5;
-                if (__ldg(sdil + (size_t(sz) * ns + sy) * ns + sx) >= k_large) {
-                    lox = sx * 32; hix = lox + 32;
-                    loy = sy * 32; hiy = loy + 32;
-                    loz = sz * 32; hiz = loz + 32;
-                    skip = true;
-                }
-            }
-            if (!skip) {
-                const int bx = vx >> 3, by = vy >> 3, bz = vz >> 3;
-                if (__ldg(bdil + (size_t(bz) * nb + by) * nb + bx) >= (st.small ? k_small : k_large)) {
-                    lox = bx * 8; hix = lox + 8;
-                    loy = by * 8; hiy = loy + 8;
-                    loz = bz * 8; hiz = loz + 8;
-                    skip = true;
-                }
-            }
-            if (skip) {
-                // skip this sample and every later one whose base voxel stays in the box
-                const float t_safe = box_exit(g, n, lox, hix, loy, hiy, loz, hiz, st.far_d);
-                do {
-                    st.prev_t = st.t;
-                    st.t += inc;
-                    ++st.guard;
-                } while (st.t < t_safe && st.t < st.far_d && st.guard < kMaxMarchSamples);
-                st.prev_known = 0;
-                continue;
-            }
-        }
+        if (bdil && skip_cell(S, g, st, x, y, z, inc)) continue;
         const float tsdf = trilinear(f, n, x, y, z);
         ++st.guard;
         if (tsdf < 0.0f) {
@@ -218,6 +223,11 @@ __device__ void march_coop(const SessionDev* S, const RayGeo& g, const TF* f, Ra
     const unsigned int full = 0xffffffffu;
     while (st.t < st.far_d && st.guard < kMaxMarchSamples) {
         const float inc = st.small ? small : large;
+        if (S->bdil) {
+            float x, y, z;
+            texel(g, st.t, x, y, z);
+            if (skip_cell(S, g, st, x, y, z, inc)) continue;   // every lane takes the same steps
+        }
         float tk = st.t;
         for (int q = 0; q < lane; ++q) tk += inc;
         const bool valid = tk < st.far_d && st.guard + lane < kMaxMarchSamples;
