@@ -381,7 +381,8 @@ double kf_now_ms(void);
 /* ------------------------------------------------------------------------------------------ */
 /* Record events between the stages of every step (re-captures the step graph). */
 kf_status kf_session_set_profiling(kf_session* s, int on);
-/* Device durations (ms) of the last completed step: preprocess, raycast, ICP, fusion. */
+/* Device durations (ms) of the last completed step: preprocess, raycast, ICP, fusion.  The
+ * preprocess runs on a graph branch beside the raycast, so the raycast figure spans both. */
 kf_status kf_session_stage_times(kf_session* s, float ms[4]);
 kf_status kf_batch_set_profiling(kf_batch* b, int on);
 kf_status kf_batch_stage_times(kf_batch* b, float ms[4]);

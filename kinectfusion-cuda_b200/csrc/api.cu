@@ -416,6 +416,10 @@ struct Engine {
     bool graph_dirty = true;
     cudaGraphExec_t gexec = nullptr;
     cudaStream_t cap_stream = nullptr;
+    // the preprocess of a frame runs on a branch beside its raycast (which reads the previous
+    // frame's volume and pose only): fork and join events and the branch's stream
+    cudaStream_t aux_stream = nullptr;
+    cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
     bool stages[4] = {true, true, true, true};
     // per-stage timing: events between the launches (also inside the captured graph)
     bool profile = false;
@@ -453,6 +457,9 @@ struct Engine {
         std::memset(h_out, 0, sizeof(OutDev) * capacity);
         std::memset(h_sync, 0, sizeof(GridSync));
         KF_CK(cudaStreamCreateWithFlags(&cap_stream, cudaStreamNonBlocking));
+        KF_CK(cudaStreamCreateWithFlags(&aux_stream, cudaStreamNonBlocking));
+        KF_CK(cudaEventCreateWithFlags(&ev_fork, cudaEventDisableTiming));
+        KF_CK(cudaEventCreateWithFlags(&ev_join, cudaEventDisableTiming));
         // persistent grids (kf_batch_autotune may replace the first, second and fourth)
         grid_pre = sms * 4;
         grid_ray = sms * 6;
@@ -471,10 +478,14 @@ struct Engine {
         return KF_OK;
     }
 
-    // durations of the four stages of the last completed step (ms)
+    // durations of the four stages of the last completed step (ms); the preprocess runs beside
+    // the raycast, so the raycast's figure spans both branches (from the fork to the join)
     kf_status stage_times(float* ms) {
         if (!profile) return KF_ERR_STATE;
-        for (int i = 0; i < 4; ++i) KF_CK(cudaEventElapsedTime(&ms[i], ev[i], ev[i + 1]));
+        KF_CK(cudaEventElapsedTime(&ms[0], ev[0], ev[1]));
+        KF_CK(cudaEventElapsedTime(&ms[1], ev[0], ev[2]));
+        KF_CK(cudaEventElapsedTime(&ms[2], ev[2], ev[3]));
+        KF_CK(cudaEventElapsedTime(&ms[3], ev[3], ev[4]));
         return KF_OK;
     }
 
@@ -495,6 +506,9 @@ struct Engine {
         cudaFree(d_ctr);
         cudaFreeHost(h_step); cudaFreeHost(h_out); cudaFreeHost(h_sync);
         if (cap_stream) cudaStreamDestroy(cap_stream);
+        if (aux_stream) cudaStreamDestroy(aux_stream);
+        if (ev_fork) cudaEventDestroy(ev_fork);
+        if (ev_join) cudaEventDestroy(ev_join);
     }
 
     EngineView view() const {
@@ -658,9 +672,20 @@ struct Engine {
         KF_CK(cudaMemsetAsync(d_ctr, 0, sizeof(unsigned int) * kCounters, st));
         KF_CK(cudaMemsetAsync(d_sync, 0, sizeof(GridSync), st));
         if (profile) KF_CK(cudaEventRecordWithFlags(ev[0], st, cudaEventRecordExternal));
-        if (stages[0]) KF_CK(launch_preprocess(v, grid_pre, st));
-        if (profile) KF_CK(cudaEventRecordWithFlags(ev[1], st, cudaEventRecordExternal));
+        const bool fork = stages[0] && stages[1];
+        if (fork) {
+            // preprocess on a branch beside the raycast; ICP waits for both
+            KF_CK(cudaEventRecord(ev_fork, st));
+            KF_CK(cudaStreamWaitEvent(aux_stream, ev_fork, 0));
+            KF_CK(launch_preprocess(v, grid_pre, aux_stream));
+            if (profile) KF_CK(cudaEventRecordWithFlags(ev[1], aux_stream, cudaEventRecordExternal));
+            KF_CK(cudaEventRecord(ev_join, aux_stream));
+        } else {
+            if (stages[0]) KF_CK(launch_preprocess(v, grid_pre, st));
+            if (profile) KF_CK(cudaEventRecordWithFlags(ev[1], st, cudaEventRecordExternal));
+        }
         if (stages[1]) KF_CK(launch_raycast(v, grid_ray, st));
+        if (fork) KF_CK(cudaStreamWaitEvent(st, ev_join, 0));
         if (profile) KF_CK(cudaEventRecordWithFlags(ev[2], st, cudaEventRecordExternal));
         if (stages[2]) KF_CK(launch_icp(v, grid_icp, st));
         if (profile) KF_CK(cudaEventRecordWithFlags(ev[3], st, cudaEventRecordExternal));
