@@ -144,12 +144,13 @@ __device__ __forceinline__ bool skip_cell(const SessionDev* S, const RayGeo& g, 
     const int thr = st.small ? __float_as_int(0.001f) : __float_as_int(0.991f);
     int lo[3], hi[3];
     const int sx = vx >> 5, sy = vy >> 5, sz = vz >> 5;
-    if (__ldg(S->sdil + (size_t(sz) * S->ns + sy) * S->ns + sx) >= thr) {
+    const int ns = S->ns, nb = S->nb;   // (n / 8)^3 bricks: 32-bit indices
+    if (__ldg(S->sdil + (sz * ns + sy) * ns + sx) >= thr) {
         lo[0] = sx * 32; lo[1] = sy * 32; lo[2] = sz * 32;
         hi[0] = lo[0] + 32; hi[1] = lo[1] + 32; hi[2] = lo[2] + 32;
     } else {
         const int bx = vx >> 3, by = vy >> 3, bz = vz >> 3;
-        if (__ldg(S->bdil + (size_t(bz) * S->nb + by) * S->nb + bx) < thr) return false;
+        if (__ldg(S->bdil + (bz * nb + by) * nb + bx) < thr) return false;
         lo[0] = bx * 8; lo[1] = by * 8; lo[2] = bz * 8;
         hi[0] = lo[0] + 8; hi[1] = lo[1] + 8; hi[2] = lo[2] + 8;
     }

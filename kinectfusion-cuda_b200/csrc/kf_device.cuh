@@ -176,16 +176,20 @@ __device__ __forceinline__ float trilinear(const TF* f, int n, float x, float y,
     const float fx = floorf(x), fy = floorf(y), fz = floorf(z);
     const float ax = x - fx, ay = y - fy, az = z - fz;
     const int ix = int(fx), iy = int(fy), iz = int(fz);
-    const int x0 = min(max(ix, 0), n - 1), x1 = min(max(ix + 1, 0), n - 1);
-    const int y0 = min(max(iy, 0), n - 1), y1 = min(max(iy + 1, 0), n - 1);
-    const int z0 = min(max(iz, 0), n - 1), z1 = min(max(iz + 1, 0), n - 1);
-    const size_t nn = size_t(n);
-    const size_t r00 = (size_t(z0) * nn + y0) * nn, r10 = (size_t(z0) * nn + y1) * nn;
-    const size_t r01 = (size_t(z1) * nn + y0) * nn, r11 = (size_t(z1) * nn + y1) * nn;
-    const float v000 = load_f(f, r00 + x0), v100 = load_f(f, r00 + x1);
-    const float v010 = load_f(f, r10 + x0), v110 = load_f(f, r10 + x1);
-    const float v001 = load_f(f, r01 + x0), v101 = load_f(f, r01 + x1);
-    const float v011 = load_f(f, r11 + x0), v111 = load_f(f, r11 + x1);
+    // the low tap clamps to [0, n-1]; the high tap is the next voxel, or the same one where
+    // clamping makes both taps equal (index below 0 or at n-1 and above)
+    const int x0 = min(max(ix, 0), n - 1), y0 = min(max(iy, 0), n - 1), z0 = min(max(iz, 0), n - 1);
+    const int dx = unsigned(ix) < unsigned(n - 1) ? 1 : 0;
+    const int dy = unsigned(iy) < unsigned(n - 1) ? n : 0;
+    const int dz = unsigned(iz) < unsigned(n - 1) ? n * n : 0;
+    const TF* p00 = f + ((size_t(z0) * unsigned(n) + unsigned(y0)) * unsigned(n) + unsigned(x0));
+    const TF* p10 = p00 + dy;
+    const TF* p01 = p00 + dz;
+    const TF* p11 = p01 + dy;
+    const float v000 = load_f(p00, 0), v100 = load_f(p00, dx);
+    const float v010 = load_f(p10, 0), v110 = load_f(p10, dx);
+    const float v001 = load_f(p01, 0), v101 = load_f(p01, dx);
+    const float v011 = load_f(p11, 0), v111 = load_f(p11, dx);
     const float c00 = v000 * (1.f - ax) + v100 * ax;
     const float c10 = v010 * (1.f - ax) + v110 * ax;
     const float c01 = v001 * (1.f - ax) + v101 * ax;
