@@ -229,8 +229,11 @@ __device__ void march_coop(const SessionDev* S, const RayGeo& g, const TF* f, Ra
             texel(g, st.t, x, y, z);
             if (skip_cell(S, g, st, x, y, z, inc)) continue;   // every lane takes the same steps
         }
-        float tk = st.t;
-        for (int q = 0; q < lane; ++q) tk += inc;
+        float tk;
+        if (!add_k_times(st.t, inc, lane, tk)) {   // the same float as lane sequential additions
+            tk = st.t;
+            for (int q = 0; q < lane; ++q) tk += inc;
+        }
         const bool valid = tk < st.far_d && st.guard + lane < kMaxMarchSamples;
         const float fk = valid ? sample_at(S, g, f, tk) : 0.0f;
         const bool event = valid && (fk < 0.0f || (!st.small && fk < 0.99f));
@@ -276,35 +279,75 @@ __device__ void march_coop(const SessionDev* S, const RayGeo& g, const TF* f, Ra
     }
 }
 
-// computeGradient (project/src/raycast.cu:29-42) at the hit and the map writes (:120-144)
+// computeGradient (project/src/raycast.cu:29-42) at the hit: texel coordinates of the hit
+// and the offset of the six central-difference samples (mu / 2 apart, in uvw units)
+struct HitGeo {
+    F3 vtx;
+    float x, y, z, rt, r;
+};
+
+__device__ __forceinline__ HitGeo hit_geo(const SessionDev* S, const RayGeo& g, float precise) {
+    HitGeo h;
+    h.vtx = F3{g.o.x + g.dir.x * precise, g.o.y + g.dir.y * precise, g.o.z + g.dir.z * precise};
+    h.r = S->mu * 0.5f / S->vol_w;
+    h.rt = h.r * float(S->n);
+    h.x = h.vtx.x * g.sc + g.off;
+    h.y = h.vtx.y * g.sc + g.off;
+    h.z = h.vtx.z * g.sc + g.off;
+    return h;
+}
+
+// gradient sample q of computeGradient: q = 0, 1, 2 at +rt along x, y, z; 3, 4, 5 at -rt
 template <class TF>
-__device__ void finish_ray(const SessionDev* S, const RayGeo& g, const TF* f, int level, int i, int j, float precise) {
+__device__ __forceinline__ float grad_sample(const TF* f, int n, const HitGeo& h, int q) {
+    const float d = q < 3 ? h.rt : -h.rt;
+    const int a = q < 3 ? q : q - 3;
+    return trilinear(f, n, a == 0 ? h.x + d : h.x, a == 1 ? h.y + d : h.y, a == 2 ? h.z + d : h.z);
+}
+
+// the normal from the six samples and the map writes (project/src/raycast.cu:120-144)
+__device__ __forceinline__ void write_hit(const SessionDev* S, int level, int i, int j, bool hit, const HitGeo& h,
+                                          const float (&v)[6]) {
     const int w = S->lv[level].w;
     float4* ov = S->pv[level] + size_t(j) * w + i;
     float4* on = S->pn[level] + size_t(j) * w + i;
-    if (precise != 0.0f) {
-        const int n = S->n;
-        const float mu = S->mu, width = S->vol_w;
-        const F3 vtx{g.o.x + g.dir.x * precise, g.o.y + g.dir.y * precise, g.o.z + g.dir.z * precise};
-        // central differences mu / 2 apart, in uvw units
-        const float r = mu * 0.5f / width;
-        const float rt = r * float(n);
-        const float x = vtx.x * g.sc + g.off, y = vtx.y * g.sc + g.off, z = vtx.z * g.sc + g.off;
-        const float fx0 = trilinear(f, n, x + rt, y, z), fy0 = trilinear(f, n, x, y + rt, z);
-        const float fz0 = trilinear(f, n, x, y, z + rt);
-        const float fx = trilinear(f, n, x - rt, y, z), fy = trilinear(f, n, x, y - rt, z);
-        const float fz = trilinear(f, n, x, y, z - rt);
-        F3 gr{(fx - fx0) / r, (fy - fy0) / r, (fz - fz0) / r};
+    if (hit) {
+        F3 gr{(v[3] - v[0]) / h.r, (v[4] - v[1]) / h.r, (v[5] - v[2]) / h.r};
         const float gn = sqrtf(dot3(gr, gr));
         if (depth_valid(gn)) {
             gr = F3{gr.x / gn, gr.y / gn, gr.z / gn};
-            *ov = make_float4(vtx.x, vtx.y, vtx.z, kValid);
+            *ov = make_float4(h.vtx.x, h.vtx.y, h.vtx.z, kValid);
             *on = make_float4(gr.x, gr.y, gr.z, kValid);
             return;
         }
     }
     *ov = make_float4(0.f, 0.f, 0.f, kInvalid);
     *on = make_float4(0.f, 0.f, 0.f, kInvalid);
+}
+
+template <class TF>
+__device__ void finish_ray(const SessionDev* S, const RayGeo& g, const TF* f, int level, int i, int j, float precise) {
+    const HitGeo h = hit_geo(S, g, precise);
+    float v[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+    if (precise != 0.0f) {
+#pragma unroll
+        for (int q = 0; q < 6; ++q) v[q] = grad_sample(f, S->n, h, q);
+    }
+    write_hit(S, level, i, j, precise != 0.0f, h, v);
+}
+
+// the same for a ray carried by a whole warp: lanes 0-5 take one gradient sample each, lane 0
+// writes
+template <class TF>
+__device__ void finish_ray_warp(const SessionDev* S, const RayGeo& g, const TF* f, int level, int i, int j,
+                                float precise, int lane) {
+    const HitGeo h = hit_geo(S, g, precise);
+    float mine = 0.f;
+    if (precise != 0.0f && lane < 6) mine = grad_sample(f, S->n, h, lane);
+    float v[6];
+#pragma unroll
+    for (int q = 0; q < 6; ++q) v[q] = __shfl_sync(0xffffffffu, mine, q);
+    if (lane == 0) write_hit(S, level, i, j, precise != 0.0f, h, v);
 }
 
 __device__ __forceinline__ void write_miss(const SessionDev* S, int level, int i, int j) {
@@ -375,7 +418,7 @@ __device__ void coop_ray(const SessionDev* S, const LongRay& L, int lane) {
     RayState st = L.st;
     float precise = 0.0f;
     march_coop(S, g, f, st, lane, precise);
-    if (lane == 0) finish_ray(S, g, f, L.level, L.i, L.j, precise);
+    finish_ray_warp(S, g, f, L.level, L.i, L.j, precise, lane);
 }
 
 // the queued long rays, one warp each

@@ -42,6 +42,30 @@ KF_HD float u2f(uint32_t u) {
 #endif
 }
 
+// t after k >= 0 repeated additions t <- fl(t + inc), in closed form.  True (out set) when t
+// and inc are positive normal floats, inc is not a rounding tie in t's binade and the k
+// additions stay inside t's binade; false otherwise, and the caller adds one by one.
+KF_HD bool add_k_times(float t, float inc, int k, float& out) {
+    const uint32_t tb = f2u(t), ib = f2u(inc);
+    const int e = int(tb >> 23), ei = int(ib >> 23);   // a set sign bit makes these >= 256
+    if (e <= 0 || e >= 255 || ei <= 0 || ei > e) return false;
+    const int sh = e - ei;
+    if (sh > 24) return false;
+    const int32_t m = int32_t((tb & 0x7fffffu) | 0x800000u);
+    const int32_t mi = int32_t((ib & 0x7fffffu) | 0x800000u);
+    int32_t D = mi >> sh;                                  // ulps of t's binade per addition
+    if (sh > 0) {
+        const int32_t r = mi & ((int32_t(1) << sh) - 1), half = int32_t(1) << (sh - 1);
+        if (r == half) return false;                       // tie: round-to-even alternates
+        if (r > half) ++D;
+    }
+    if (k < 0 || k > 127) return false;                    // k * D stays below 2^31
+    const int32_t m1 = m + k * D;
+    if (m1 > 0xffffff) return false;
+    out = u2f((uint32_t(e) << 23) | (uint32_t(m1) & 0x7fffffu));
+    return true;
+}
+
 // Repeats { prev = t; t = fl(t + inc); } at least once and until t >= limit or max_steps
 // additions were made; returns the number of additions.  Equal, bit for bit, to the plain
 // loop for any t, inc, limit (the closed form is used only for positive normal t, inc and

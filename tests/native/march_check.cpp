@@ -1,5 +1,5 @@
-// Host check of kf::advance_steps (kinectfusion-cuda_b200/csrc/kf_march.h) against the plain
-// repeated float additions.  Built and run by tests/test_march_fastforward.py.
+// Host check of kf::advance_steps and kf::add_k_times (kinectfusion-cuda_b200/csrc/kf_march.h)
+// against the plain repeated float additions.  Built and run by tests/test_march_fastforward.py.
 #include <cstdio>
 #include <cstdint>
 #include <cstdlib>
@@ -65,6 +65,28 @@ int main(int argc, char** argv) {
             ++bad;
         }
     }
-    printf("cases %d steps %lld mismatches %lld\n", cases, steps, bad);
-    return bad ? 1 : 0;
+    // add_k_times: lane k of a cooperative march forms t + k increments in closed form
+    long long kbad = 0, kused = 0;
+    for (int c = 0; c < cases; ++c) {
+        const float t0 = (c & 1) ? uni(0.4f, 6.0f) : float(1 << int(next_u64() % 3)) - uni(0.0f, 0.05f);
+        float inc = incs[next_u64() % 6];
+        if (c % 5 == 0) {   // random increments, ties included
+            const uint32_t ib = (uint32_t(117 + next_u64() % 10) << 23) | uint32_t(next_u64() & 0x7fffffu);
+            memcpy(&inc, &ib, 4);
+        }
+        const int k = int(next_u64() % 32);
+        float seq = t0;
+        for (int q = 0; q < k; ++q) seq = seq + inc;
+        float fast = 0.f;
+        if (kf::add_k_times(t0, inc, k, fast)) {
+            ++kused;
+            if (memcmp(&seq, &fast, 4)) {
+                if (kbad < 5) printf("add_k_times mismatch t0=%.9g inc=%.9g k=%d: %.9g vs %.9g\n", t0, inc, k, seq, fast);
+                ++kbad;
+            }
+        }
+    }
+    printf("cases %d steps %lld mismatches %lld; add_k_times closed form %lld of %d, mismatches %lld\n", cases,
+           steps, bad, kused, cases, kbad);
+    return (bad || kbad || kused < cases / 4) ? 1 : 0;
 }
