@@ -603,12 +603,14 @@ struct Engine {
             for (int l = 0; l < c.levels; ++l) {
                 const LevelDev& Lv = sl.d.lv[l];
                 const int np = Lv.icw * Lv.ich;
-                // a few tiles per ICP block per session-level (the grid's blocks take them
-                // round robin, which evens out tiles of mostly invalid pixels), at least a
-                // block's worth of pixels each
-                const int ntiles = grid_icp * kIcpTilesPerBlock;
+                // up to a few tiles per ICP block per session-level (the grid's blocks take them
+                // round robin, which evens out tiles of mostly invalid pixels), each at least
+                // one pipelined step of the block (kIcpMinTile pixels): small levels get few
+                // tiles, so a pass over many sessions stores few partials
+                const int per_block = std::max(1, std::min(kIcpTilesPerBlock, np / (grid_icp * kIcpMinTile)));
+                const int ntiles = grid_icp * per_block;
                 int tile = (np + ntiles - 1) / ntiles;
-                tile = std::max(kIcpThreads, (tile + 31) / 32 * 32);
+                tile = std::max(kIcpMinTile, (tile + 31) / 32 * 32);
                 IcpRange rg;
                 rg.begin = int(it[l].size());
                 for (int p0 = 0; p0 < np; p0 += tile) it[l].push_back(IcpTile{s, p0, std::min(tile, np - p0)});

@@ -70,10 +70,13 @@ __device__ __forceinline__ void make_geo(const SessionDev* S, const float* m, F3
     g.itdx = 1.0f / g.tdx; g.itdy = 1.0f / g.tdy; g.itdz = 1.0f / g.tdz;
 }
 
+// texel coordinate of the sample at t, (o + dir t) * sc + off, with its roundings spelled out
+// (two fused multiply-adds): a sample's value must not depend on which kernel, or which
+// branch of the march, evaluates it, since its comparison with 0.99 or 0 decides the march
 __device__ __forceinline__ void texel(const RayGeo& g, float t, float& x, float& y, float& z) {
-    x = (g.o.x + g.dir.x * t) * g.sc + g.off;
-    y = (g.o.y + g.dir.y * t) * g.sc + g.off;
-    z = (g.o.z + g.dir.z * t) * g.sc + g.off;
+    x = __fmaf_rn(__fmaf_rn(g.dir.x, t, g.o.x), g.sc, g.off);
+    y = __fmaf_rn(__fmaf_rn(g.dir.y, t, g.o.y), g.sc, g.off);
+    z = __fmaf_rn(__fmaf_rn(g.dir.z, t, g.o.z), g.sc, g.off);
 }
 
 template <class TF>
@@ -288,12 +291,13 @@ struct HitGeo {
 
 __device__ __forceinline__ HitGeo hit_geo(const SessionDev* S, const RayGeo& g, float precise) {
     HitGeo h;
-    h.vtx = F3{g.o.x + g.dir.x * precise, g.o.y + g.dir.y * precise, g.o.z + g.dir.z * precise};
+    h.vtx = F3{__fmaf_rn(g.dir.x, precise, g.o.x), __fmaf_rn(g.dir.y, precise, g.o.y),
+               __fmaf_rn(g.dir.z, precise, g.o.z)};
     h.r = S->mu * 0.5f / S->vol_w;
     h.rt = h.r * float(S->n);
-    h.x = h.vtx.x * g.sc + g.off;
-    h.y = h.vtx.y * g.sc + g.off;
-    h.z = h.vtx.z * g.sc + g.off;
+    h.x = __fmaf_rn(h.vtx.x, g.sc, g.off);
+    h.y = __fmaf_rn(h.vtx.y, g.sc, g.off);
+    h.z = __fmaf_rn(h.vtx.z, g.sc, g.off);
     return h;
 }
 
@@ -302,7 +306,8 @@ template <class TF>
 __device__ __forceinline__ float grad_sample(const TF* f, int n, const HitGeo& h, int q) {
     const float d = q < 3 ? h.rt : -h.rt;
     const int a = q < 3 ? q : q - 3;
-    return trilinear(f, n, a == 0 ? h.x + d : h.x, a == 1 ? h.y + d : h.y, a == 2 ? h.z + d : h.z);
+    return trilinear(f, n, a == 0 ? __fadd_rn(h.x, d) : h.x, a == 1 ? __fadd_rn(h.y, d) : h.y,
+                     a == 2 ? __fadd_rn(h.z, d) : h.z);
 }
 
 // the normal from the six samples and the map writes (project/src/raycast.cu:120-144)

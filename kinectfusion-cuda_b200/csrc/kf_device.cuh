@@ -190,13 +190,16 @@ __device__ __forceinline__ float trilinear(const TF* f, int n, float x, float y,
     const float v010 = load_f(p10, 0), v110 = load_f(p10, dx);
     const float v001 = load_f(p01, 0), v101 = load_f(p01, dx);
     const float v011 = load_f(p11, 0), v111 = load_f(p11, dx);
-    const float c00 = v000 * (1.f - ax) + v100 * ax;
-    const float c10 = v010 * (1.f - ax) + v110 * ax;
-    const float c01 = v001 * (1.f - ax) + v101 * ax;
-    const float c11 = v011 * (1.f - ax) + v111 * ax;
-    const float c0 = c00 * (1.f - ay) + c10 * ay;
-    const float c1 = c01 * (1.f - ay) + c11 * ay;
-    return c0 * (1.f - az) + c1 * az;
+    // each lerp a (1 - w) + b w as one rounded product and one fused multiply-add, spelled
+    // out so every kernel that samples the volume rounds identically
+    const float bx = __fsub_rn(1.f, ax), by = __fsub_rn(1.f, ay), bz = __fsub_rn(1.f, az);
+    const float c00 = __fmaf_rn(v100, ax, __fmul_rn(v000, bx));
+    const float c10 = __fmaf_rn(v110, ax, __fmul_rn(v010, bx));
+    const float c01 = __fmaf_rn(v101, ax, __fmul_rn(v001, bx));
+    const float c11 = __fmaf_rn(v111, ax, __fmul_rn(v011, bx));
+    const float c0 = __fmaf_rn(c10, ay, __fmul_rn(c00, by));
+    const float c1 = __fmaf_rn(c11, ay, __fmul_rn(c01, by));
+    return __fmaf_rn(c1, az, __fmul_rn(c0, bz));
 }
 
 // globaltimer (ns) for bounded waits

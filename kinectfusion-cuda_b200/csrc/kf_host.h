@@ -56,6 +56,7 @@ constexpr int kIcpThreads = 256;
 constexpr int kIcpPxPerThread = 8;
 constexpr int kIcpTilePx = kIcpThreads * kIcpPxPerThread;   // rows per block of the LLS stage
 constexpr int kIcpTilesPerBlock = 4;  // ICP tiles per session-level per block of the grid
+constexpr int kIcpMinTile = kIcpThreads * 4;   // smallest ICP tile: 4 pixels per thread
 constexpr int kIcpPartialStride = 56; // floats per ICP tile partial: 27 (sum, compensation) pairs + pad
 constexpr int kIcpMaxPasses = 64;     // hard cap on ICP passes per frame
 
