@@ -251,6 +251,7 @@ void fill_levels(SessionDev& d, const kf_config& c) {
     for (int l = 0; l < c.levels; ++l) d.iters[l] = c.iters[l];
     d.dist_th = c.dist_thresh;
     d.angle_th = c.angle_thresh;
+    d.angle_cos = float(std::cos(double(c.angle_thresh)));
     d.stop_a = c.stop_angle;
     d.stop_d = c.stop_dist;
 }

@@ -16,6 +16,8 @@
 // separated by bounded grid barriers.  Nothing returns to the host until the frame is done.
 #include <mutex>
 
+#include <cmath>
+
 #include "kf_host.h"
 
 namespace kf {
@@ -25,33 +27,45 @@ __device__ __forceinline__ float ldcg(const float* p) { return __ldcg(p); }
 __device__ __forceinline__ double ldcg(const double* p) { return __ldcg(p); }
 __device__ __forceinline__ int ldcg(const int* p) { return __ldcg(p); }
 
+// ---- the reference's correspondence and rejection tests (project/src/icp.cuh:40-48, 72-85),
+// in the forms its -use_fast_math build evaluates or cheaper equivalents ----
+// floor(x / z) of computeCorrespondence with the approximate division of that build
+__device__ __forceinline__ int corr_coord(float x, float z) {
+    return int(floorf(__fdividef(x, z)));   // cvt.rzi: NaN -> 0, as in the reference
+}
+// areVerticesTooFarAway: |e| > d  <=>  e.e > d^2 (NaN compares false either way)
+__device__ __forceinline__ bool too_far(F3 e, float dist_th) { return dot3(e, e) > dist_th * dist_th; }
+// areNormalsTooDifferent: acos(c) > a  <=>  c < cos(a) for c in [-1, 1]; outside [-1, 1] and
+// for NaN acos is NaN, the comparison is false and the pair passes, as in the reference
+__device__ __forceinline__ bool too_different(float c, float cos_th) { return c < cos_th && c >= -1.0f; }
+
 // ---- per-pixel residual: constructIcpResidualsKernel body with computeCorrespondence,
 // areVerticesTooFarAway, areNormalsTooDifferent and computeAndFillA/B
 // (project/src/icp.cu:20-81, project/src/icp.cuh:40-95) ----
 __device__ __forceinline__ bool icp_pixel(const float4* __restrict__ vm, const float4* __restrict__ tv,
                                           const float4* __restrict__ tn, int w, int h, int u, int v, const float* R,
                                           const float* t, const float* M, const float* tp, float dist_th,
-                                          float ang_th, float a[6], float& b) {
+                                          float cos_th, float a[6], float& b) {
     const float4 vc = __ldg(vm + size_t(v) * w + u);
     if (vc.w != kValid) return false;
     const F3 s = mv3(R, f3(vc)) + F3{t[0], t[1], t[2]};
     // (K * R_prev^T) * (s - t_prev), then floor(x / z), floor(y / z)
     const F3 pt = mv3(M, s - F3{tp[0], tp[1], tp[2]});
-    const int uc = int(floorf(pt.x / pt.z));   // cvt.rzi: NaN -> 0, as in the reference
-    const int vcor = int(floorf(pt.y / pt.z));
+    const int uc = corr_coord(pt.x, pt.z);
+    const int vcor = corr_coord(pt.y, pt.z);
     if (uc < 0 || vcor < 0 || uc >= w || vcor >= h) return false;
     const float4 d4 = __ldg(tv + size_t(vcor) * w + uc);
     const float4 n4 = __ldg(tn + size_t(vcor) * w + uc);
     if (d4.w != kValid || n4.w != kValid) return false;
     const F3 d = f3(d4);
     const F3 e = s - d;
-    if (sqrtf(dot3(e, e)) > dist_th) return false;
+    if (too_far(e, dist_th)) return false;
     const float4 ns = compute_normal(vm, w, h, u, v);
     if (ns.w == kInvalid) return false;
     F3 nr = mv3(R, f3(ns));
     nr = nr * rsqrtf(dot3(nr, nr));
     const F3 n = f3(n4);
-    if (acosf(dot3(nr, n)) > ang_th) return false;   // NaN passes, as in the reference
+    if (too_different(dot3(nr, n), cos_th)) return false;
     a[0] = n.y * s.z - n.z * s.y;
     a[1] = n.z * s.x - n.x * s.z;
     a[2] = n.x * s.y - n.y * s.x;
@@ -73,7 +87,7 @@ struct IcpMats { const float* R; const float* t; const float* M; const float* tp
 template <int U, class Acc>
 __device__ __forceinline__ void icp_multi(const float4* __restrict__ vm, const float4* __restrict__ tv,
                                         const float4* __restrict__ tn, int w, int h, int icw, int p0, int pend,
-                                        const IcpMats& m, float dist_th, float ang_th, uint8_t* mask, Acc&& accumulate) {
+                                        const IcpMats& m, float dist_th, float cos_th, uint8_t* mask, Acc&& accumulate) {
     int u[U], vv[U];
     bool in[U];
     float4 vc[U], vr[U], vd[U];
@@ -99,8 +113,8 @@ __device__ __forceinline__ void icp_multi(const float4* __restrict__ vm, const f
         if (ok[q]) {
             s[q] = mv3(m.R, f3(vc[q])) + F3{m.t[0], m.t[1], m.t[2]};
             const F3 pt = mv3(m.M, s[q] - F3{m.tp[0], m.tp[1], m.tp[2]});
-            uc[q] = int(floorf(pt.x / pt.z));   // cvt.rzi: NaN -> 0, as in the reference
-            vcor[q] = int(floorf(pt.y / pt.z));
+            uc[q] = corr_coord(pt.x, pt.z);
+            vcor[q] = corr_coord(pt.y, pt.z);
             ok[q] = !(uc[q] < 0 || vcor[q] < 0 || uc[q] >= w || vcor[q] >= h);
         }
     }
@@ -117,7 +131,7 @@ __device__ __forceinline__ void icp_multi(const float4* __restrict__ vm, const f
         if (good) {
             const F3 d = f3(d4[q]);
             const F3 e = s[q] - d;
-            good = !(sqrtf(dot3(e, e)) > dist_th);
+            good = !too_far(e, dist_th);
             // computeNormal: the vertex, its right and its lower neighbour valid
             good = good && vr[q].w == kValid && vd[q].w == kValid;
             if (good) {
@@ -127,7 +141,7 @@ __device__ __forceinline__ void icp_multi(const float4* __restrict__ vm, const f
                 F3 nr = mv3(m.R, nn);
                 nr = nr * rsqrtf(dot3(nr, nr));
                 const F3 n = f3(n4[q]);
-                good = !(acosf(dot3(nr, n)) > ang_th);   // NaN passes, as in the reference
+                good = !too_different(dot3(nr, n), cos_th);
                 if (good) {
                     const F3 sv = s[q];
                     a[0] = n.y * sv.z - n.z * sv.y;
@@ -605,7 +619,7 @@ __global__ void __launch_bounds__(kIcpThreads, 1) icp_kernel(EngineView v) {
                 const float4* tv = S->pv[lvl];
                 const float4* tn = S->pn[lvl];
                 uint8_t* mask = S->mask[lvl];
-                const float dist = S->dist_th, ang = S->angle_th;
+                const float dist = S->dist_th, ang = S->angle_cos;
                 const IcpMats m{mats, mats + 9, mats + 12, mats + 21};
                 const int pend = T.p0 + T.np;
 #pragma unroll 1
@@ -659,11 +673,11 @@ cudaError_t launch_icp(const EngineView& v, int grid, cudaStream_t st) {
 struct IcpStageMats { float R[9], t[3], M[9], tp[3]; };
 
 __global__ void icp_rows_kernel(const float4* vm, const float4* tv, const float4* tn, int w, int h, IcpStageMats m,
-                                float dist, float angle, float* A, float* b) {
+                                float dist, float cos_th, float* A, float* b) {
     const int u = blockIdx.x * blockDim.x + threadIdx.x, vv = blockIdx.y * blockDim.y + threadIdx.y;
     if (u >= w || vv >= h) return;
     float a[6], bb;
-    const bool ok = icp_pixel(vm, tv, tn, w, h, u, vv, m.R, m.t, m.M, m.tp, dist, angle, a, bb);
+    const bool ok = icp_pixel(vm, tv, tn, w, h, u, vv, m.R, m.t, m.M, m.tp, dist, cos_th, a, bb);
     const size_t idx = size_t(vv) * w + u;
     for (int q = 0; q < 6; ++q) A[idx * 6 + q] = ok ? a[q] : 0.f;
     b[idx] = ok ? bb : 0.f;
@@ -683,7 +697,8 @@ cudaError_t stage_icp_residuals(const float4* vmap, const float4* tv, const floa
             m.M[col * 3 + row] = acc;
         }
     dim3 blk(16, 16), grd((w + 15) / 16, (h + 15) / 16);
-    icp_rows_kernel<<<grd, blk, 0, st>>>(vmap, tv, tn, w, h, m, dist, angle, A, b);
+    const float cos_th = float(std::cos(double(angle)));
+    icp_rows_kernel<<<grd, blk, 0, st>>>(vmap, tv, tn, w, h, m, dist, cos_th, A, b);
     return cudaGetLastError();
 }
 

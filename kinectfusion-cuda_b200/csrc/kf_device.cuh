@@ -78,6 +78,7 @@ struct SessionDev {
     // ICP
     int iters[kMaxLevels];
     float dist_th, angle_th, stop_a, stop_d;
+    float angle_cos;       // cos(angle_th): the normal test compares cosines
     PoseDev* pose;
 };
 

@@ -135,6 +135,30 @@ def level_intrinsics(cfg, level):
     return k
 
 
+def level_inverse_intrinsics(cfg, level):
+    """K_l^-1 exactly as the library forms it (adjugate over determinant in float32, the
+    glm::inverse the reference applies to its 3x3), so a caller's stage raycast from this
+    matrix takes the same rays as the session's own (kf_render)."""
+    k = level_intrinsics(cfg, level)
+    f = np.float32
+    a, b, cc = k[0, 0], k[0, 1], k[0, 2]
+    d, e, ff = k[1, 0], k[1, 1], k[1, 2]
+    g, h, i = k[2, 0], k[2, 1], k[2, 2]
+    det = f(f(a * f(f(e * i) - f(ff * h))) - f(b * f(f(d * i) - f(ff * g)))) + f(cc * f(f(d * h) - f(e * g)))
+    od = f(f(1.0) / det)
+    ik = np.zeros((3, 3), dtype=np.float32)
+    ik[0, 0] = f(f(e * i) - f(ff * h)) * od
+    ik[0, 1] = -f(f(b * i) - f(cc * h)) * od
+    ik[0, 2] = f(f(b * ff) - f(cc * e)) * od
+    ik[1, 0] = -f(f(d * i) - f(ff * g)) * od
+    ik[1, 1] = f(f(a * i) - f(cc * g)) * od
+    ik[1, 2] = -f(f(a * ff) - f(cc * d)) * od
+    ik[2, 0] = f(f(d * h) - f(e * g)) * od
+    ik[2, 1] = -f(f(a * h) - f(b * g)) * od
+    ik[2, 2] = f(f(a * e) - f(b * d)) * od
+    return ik
+
+
 # ------------------------------------------------------------------------------------------
 # the per-frame pipeline
 # ------------------------------------------------------------------------------------------

@@ -55,7 +55,9 @@ def test_display_kernels_vs_oracle(kf, orc, cuda, tracked):
 def test_render_matches_raycast_and_display(kf, orc, cuda, tracked):
     cfg, imgs, s = tracked
     pose = s.pose()
-    ik = np.linalg.inv(kf.level_intrinsics(cfg, 0).astype(np.float64)).astype(np.float32)
+    # the library's own K^-1: a ray direction one ulp apart moves a sample by ~1e-5 of a
+    # voxel, enough to flip a 0.99 or 0 test near a surface
+    ik = kf.level_inverse_intrinsics(cfg, 0)
     vt = cuda.zeros((cfg.height, cfg.width, 4), dtype=cuda.float32, device="cuda")
     nt = cuda.zeros_like(vt)
     kf.kernel.raycast(s.volume(), pose, ik, vt, nt, cfg.min_depth, cfg.max_depth, cfg.step_large, cfg.step_small)

@@ -111,3 +111,14 @@ def test_pose_error_host(kf, orc):
     got = kf.poseError(a, b)
     want = orc.pose_error(a, b)
     assert abs(got[0] - want[0]) < 1e-7 and abs(got[1] - 0.5) < 1e-6
+
+
+@pytest.mark.parametrize("level", [0, 1, 2])
+def test_level_inverse_intrinsics(kf, level):
+    """The Python mirror of the library's K_l^-1 (float32 adjugate over determinant) inverts
+    K_l to float rounding, for the full-size and small configurations."""
+    for cfg in (kf.config_full(), kf.config_small()):
+        k = kf.level_intrinsics(cfg, level).astype(np.float64)
+        ik = kf.level_inverse_intrinsics(cfg, level)
+        assert ik.dtype == np.float32
+        np.testing.assert_allclose(ik.astype(np.float64) @ k, np.eye(3), atol=2e-6)
