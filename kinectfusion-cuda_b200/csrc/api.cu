@@ -656,6 +656,7 @@ struct Engine {
         tb.S = cap;
         tb.n_pre = int(pre.size());
         tb.n_ray = int(ray.size());
+        tb.ray_budget = serial_budget(tb.n_ray);
         for (int l = 0; l < KF_MAX_LEVELS; ++l) {
             tb.n_itiles[l] = int(it[l].size());
             tb.icp_off[l] = off[l];

@@ -16,7 +16,8 @@
 //     reference never returns to large steps); super-bricks let them cross free space 94 steps
 //     at a time.
 //   - Load balance: each warp pulls 8 x 4-ray tiles from an atomic counter, and a lane marches
-//     at most 64 iterations; longer rays are queued with their exact march state.
+//     at most 40 iterations (64 in steps of many sessions); longer rays are queued with their
+//     exact march state.
 //   - Long rays: a second kernel marches each queued ray with a whole warp, 32 consecutive
 //     samples per round, taking the first sample (in order) that changes the state.
 #include "kf_host.h"
@@ -25,7 +26,13 @@
 namespace kf {
 
 constexpr int kMaxMarchSamples = 1 << 16;
-constexpr int kSerialBudget = 40;   // loop iterations a lane marches before queueing the ray
+// loop iterations a lane marches before queueing the ray: a short budget keeps the tail of a
+// single session's frame short; steps of many sessions hand off fewer rays with a longer one
+constexpr int kSerialBudgetSingle = 40;
+constexpr int kSerialBudgetMany = 64;
+constexpr int kManyRayTiles = 25000;   // more ray tiles than this in a step: kSerialBudgetMany
+
+int serial_budget(int ray_tiles) { return ray_tiles > kManyRayTiles ? kSerialBudgetMany : kSerialBudgetSingle; }
 
 struct RayGeo {
     F3 o, dir;
@@ -364,7 +371,7 @@ __device__ __forceinline__ void write_miss(const SessionDev* S, int level, int i
 
 template <class TF>
 __device__ void serial_ray(const EngineView& v, const SessionDev* S, int s, const float* m, F3 o, int level, int i,
-                           int j) {
+                           int j, int budget) {
     const TF* f = static_cast<const TF*>(S->tf);
     RayGeo g;
     make_geo(S, m, o, i, j, g);
@@ -374,7 +381,7 @@ __device__ void serial_ray(const EngineView& v, const SessionDev* S, int s, cons
         return;
     }
     float precise = 0.0f;
-    if (!march_serial(S, g, f, st, kSerialBudget, precise)) {
+    if (!march_serial(S, g, f, st, budget, precise)) {
         const unsigned int slot = atomicAdd(&v.counters[6], 1u);
         if (slot < unsigned(v.longq_cap)) {
             v.longq[slot] = LongRay{s, level, i, j, st};
@@ -389,6 +396,7 @@ __device__ void serial_ray(const EngineView& v, const SessionDev* S, int s, cons
 __global__ void __launch_bounds__(256, 3) raycast_kernel(EngineView v) {
     const int lane = threadIdx.x & 31;
     const int ntiles = v.tb->n_ray;
+    const int budget = v.tb->ray_budget;
     const int lx = lane & 7, ly = lane >> 3;
     while (true) {
         int t = 0;
@@ -406,9 +414,9 @@ __global__ void __launch_bounds__(256, 3) raycast_kernel(EngineView v) {
         F3 o;
         ray_matrix(S, Lv, m, o);
         if (S->fmt == KF_TSDF_F16U16)
-            serial_ray<__half>(v, S, T.s, m, o, T.level, i, j);
+            serial_ray<__half>(v, S, T.s, m, o, T.level, i, j, budget);
         else
-            serial_ray<float>(v, S, T.s, m, o, T.level, i, j);
+            serial_ray<float>(v, S, T.s, m, o, T.level, i, j, budget);
     }
 }
 

@@ -17,13 +17,14 @@ struct Tables {
     int n_itiles[kMaxLevels];// ICP tiles per level
     int icp_off[kMaxLevels]; // offset of each level's tiles in the ICP tile array
     int max_levels;
-    int pad;
+    int ray_budget;          // march iterations a lane takes before handing its ray to a warp
     long long fuse_total;    // fusion segments over all slots
     long long brick_total;   // bricks over all slots
     long long super_total;   // super-bricks over all slots
 };
 
 struct LongRay;   // march state of a ray handed from a lane to a warp (k_raycast.cu)
+int serial_budget(int ray_tiles);   // ray_budget for a step with this many ray tiles
 
 // raw pointers the kernels take
 struct EngineView {

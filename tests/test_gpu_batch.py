@@ -52,6 +52,32 @@ def test_batch_equals_alone(kf, mix):
     b.close()
 
 
+def test_long_lane_budget_batch_equals_alone(kf):
+    """Two 640x480 sessions make 2 x 12,600 ray tiles, past the 25,000 at which a step's lanes
+    march 64 iterations before handing a ray to a warp (40 alone): the hand-off point moves,
+    the samples and results do not."""
+    from kfb200 import synth
+    cfgs = [kf.config_full(volume_n=256), kf.config_full(volume_n=256, tsdf_format=kf.KF_TSDF_F16U16)]
+    seqs = [synth.sequence(c, 5, seed=150 + i, kind=synth.LOOP)[0] for i, c in enumerate(cfgs)]
+    alone = []
+    for c, seq in zip(cfgs, seqs):
+        s = kf.KinectFusion(c)
+        poses = [s.process_frame(img)[1] for img in seq]
+        alone.append((poses, s.raycast_maps(0)))
+        s.close()
+    b = kf.Batch(cfgs)
+    for f in range(5):
+        st, poses = b.step([seq[f] for seq in seqs])
+        assert st == kf.KF_OK
+        for i in range(2):
+            np.testing.assert_array_equal(poses[i], alone[i][0][f])
+    for i in range(2):
+        v, n = b.session(i).raycast_maps(0)
+        np.testing.assert_array_equal(v, alone[i][1][0])
+        np.testing.assert_array_equal(n, alone[i][1][1])
+    b.close()
+
+
 def test_batch_skipped_session_is_untouched(kf, mix):
     cfgs, seqs, alone = mix
     b = kf.Batch(cfgs[:2])
