@@ -140,9 +140,12 @@ __device__ __forceinline__ void fuse_block(const FuseCtx& c, int x0, int j0, int
             const float by = c.iR[4] * y + c.iR[7] * z + c.it[1];
             const float bz = c.iR[5] * y + c.iR[8] * z + c.it[2];
             const float ex = c.iR[0] * xv + bx, ey = c.iR[1] * xv + by, ez = c.iR[2] * xv + bz;
-            // pixel /= pixel.z in the reference's -use_fast_math build: the approximate division
-            const float px = __fdividef(c.fx * ex + c.cx * ez, ez);
-            const float py = __fdividef(c.fy * ey + c.cy * ez, ez);
+            // pixel /= pixel.z: the reference's build divides approximately, but rounded
+            // division here keeps the per-frame pose within 2e-6 rad of the FP64 oracle (1e-4
+            // with the approximate one: voxels near a pixel edge change pixel)
+            const float iz = 1.0f / ez;
+            const float px = (c.fx * ex + c.cx * ez) * iz;
+            const float py = (c.fy * ey + c.cy * ez) * iz;
             pz[q] = ez;
             if (ez >= c.min_d && ez < c.max_d && px >= 0.0f && px < float(c.w) && py >= 0.0f && py < float(c.h)) {
                 pix[q] = int(py) * c.w + int(px);
@@ -161,7 +164,7 @@ __device__ __forceinline__ void fuse_block(const FuseCtx& c, int x0, int j0, int
             const float diff = d[q] - pz[q];
             if (diff >= -c.mu) {   // step 4 (the reference divides with -use_fast_math)
                 fn[q] = fminf(1.0f, __fdividef(diff, c.mu));
-                wn[q] = __fdividef(1.0f, d[q]);   // 1 / depth, approximate as in the reference's build
+                wn[q] = 1.0f / d[q];
                 upd |= 1u << q;
             }
         }
