@@ -110,46 +110,71 @@ __device__ __forceinline__ void unit_origin(int n, int u, int& x0, int& j0, int&
     k0 = (u / (ux * uy)) * 8;
 }
 
+// four consecutive voxels of a row as one vector: 16 bytes of f32, 8 bytes of f16 or u16
+__device__ __forceinline__ float4 ld4(const float* p) { return *reinterpret_cast<const float4*>(p); }
+__device__ __forceinline__ uint2 ld4(const __half* p) { return *reinterpret_cast<const uint2*>(p); }
+__device__ __forceinline__ uint2 ld4(const uint16_t* p) { return *reinterpret_cast<const uint2*>(p); }
+__device__ __forceinline__ void st4(float* p, float4 v) { *reinterpret_cast<float4*>(p) = v; }
+__device__ __forceinline__ void st4(__half* p, uint2 v) { *reinterpret_cast<uint2*>(p) = v; }
+__device__ __forceinline__ void st4(uint16_t* p, uint2 v) { *reinterpret_cast<uint2*>(p) = v; }
+// component q of a 4-vector (q a compile-time constant after unrolling)
+__device__ __forceinline__ float& comp(float4& v, int q) { return q == 0 ? v.x : q == 1 ? v.y : q == 2 ? v.z : v.w; }
+__device__ __forceinline__ uint16_t get16(uint2 v, int q) {
+    const unsigned int w = q < 2 ? v.x : v.y;
+    return uint16_t((q & 1) ? (w >> 16) : (w & 0xffffu));
+}
+__device__ __forceinline__ void set16(uint2& v, int q, uint16_t b) {
+    unsigned int& w = q < 2 ? v.x : v.y;
+    w = (q & 1) ? ((w & 0xffffu) | (unsigned(b) << 16)) : ((w & 0xffff0000u) | b);
+}
+
 // fuseKernel (project/src/tsdf.cu:28-74) for rows [r_begin, r_end) of one block (row r is
-// y = j0 + r % 8, z = k0 + r / 8; n is a multiple of 8, so every block has 64 rows), lanes
-// along x
+// y = j0 + r % 8, z = k0 + r / 8; n is a multiple of 8, so every block has 64 rows).  A warp
+// takes four rows per step: lanes 8 q .. 8 q + 7 row r0 + q, each lane four consecutive voxels
+// along x, so the warp reads and writes the volume as four 128-byte rows of 16-byte (f32) or
+// 8-byte (f16, u16) vectors.  A vector whose voxels all stay unchanged is not touched; voxels
+// that stay unchanged inside a written vector are written back with their own bits.
 template <class TF, class TW>
 __device__ __forceinline__ void fuse_block(const FuseCtx& c, int x0, int j0, int k0, int r_begin, int r_end, int lane) {
     const int n = c.n;
-    const int x = x0 + lane;
-    const bool lane_in = x < n;
-    const float xv = __ldg(c.xs + min(x, n - 1));
+    const int sub = lane >> 3;
+    const int x = x0 + 4 * (lane & 7);   // the first of this lane's four voxels
+    const bool lane_in = x < n;            // n % 8 == 0: all four voxels or none
+    float xv[4];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) xv[q] = __ldg(c.xs + min(x + q, n - 1));
     const int rows = min(r_end, 64);
     int kmin = 0x7fffffff;   // key of the smallest distance this lane stores
     TF* F = static_cast<TF*>(c.F);
     TW* Wa = static_cast<TW*>(c.W);
     for (int r0 = r_begin; r0 < rows; r0 += 4) {
+        const int r = r0 + sub;
+        const bool row_in = lane_in && r < rows;
+        const int j = j0 + (r & 7), k = k0 + (r >> 3);
         int pix[4];
         float pz[4], d[4];
         unsigned int cand = 0;
         // project (steps 1-2)
-#pragma unroll
-        for (int q = 0; q < 4; ++q) {
-            pix[q] = 0;
-            pz[q] = 0.f;
-            const int r = r0 + q;
-            if (r >= rows || !lane_in) continue;
-            const int j = j0 + (r & 7), k = k0 + (r >> 3);
+        if (row_in) {
             const float y = __ldg(c.xs + j), z = __ldg(c.zs + k);
             const float bx = c.iR[3] * y + c.iR[6] * z + c.it[0];
             const float by = c.iR[4] * y + c.iR[7] * z + c.it[1];
             const float bz = c.iR[5] * y + c.iR[8] * z + c.it[2];
-            const float ex = c.iR[0] * xv + bx, ey = c.iR[1] * xv + by, ez = c.iR[2] * xv + bz;
-            // pixel /= pixel.z: the reference's build divides approximately, but rounded
-            // division here keeps the per-frame pose within 2e-6 rad of the FP64 oracle (1e-4
-            // with the approximate one: voxels near a pixel edge change pixel)
-            const float iz = 1.0f / ez;
-            const float px = (c.fx * ex + c.cx * ez) * iz;
-            const float py = (c.fy * ey + c.cy * ez) * iz;
-            pz[q] = ez;
-            if (ez >= c.min_d && ez < c.max_d && px >= 0.0f && px < float(c.w) && py >= 0.0f && py < float(c.h)) {
-                pix[q] = int(py) * c.w + int(px);
-                cand |= 1u << q;
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                const float ex = c.iR[0] * xv[q] + bx, ey = c.iR[1] * xv[q] + by, ez = c.iR[2] * xv[q] + bz;
+                // pixel /= pixel.z: the reference's build divides approximately, but rounded
+                // division here keeps the per-frame pose within 2e-6 rad of the FP64 oracle
+                // (1e-4 with the approximate one: voxels near a pixel edge change pixel)
+                const float iz = 1.0f / ez;
+                const float px = (c.fx * ex + c.cx * ez) * iz;
+                const float py = (c.fy * ey + c.cy * ez) * iz;
+                pz[q] = ez;
+                pix[q] = 0;
+                if (ez >= c.min_d && ez < c.max_d && px >= 0.0f && px < float(c.w) && py >= 0.0f && py < float(c.h)) {
+                    pix[q] = int(py) * c.w + int(px);
+                    cand |= 1u << q;
+                }
             }
         }
         // nearest-pixel depth (step 3), four gathers in flight
@@ -169,46 +194,46 @@ __device__ __forceinline__ void fuse_block(const FuseCtx& c, int x0, int j0, int
             }
         }
         if (!__any_sync(0xffffffffu, upd != 0)) continue;
-        // step 5: read-modify-write, four rows' loads in flight
-        size_t idx[4];
-        float f0[4], w0[4];
+        if (!upd) continue;
+        // step 5: one vector read-modify-write of the lane's four voxels
+        const size_t idx = (size_t(k) * n + j) * n + x;
+        if constexpr (sizeof(TF) == 4) {
+            float4 fv = ld4(F + idx), wv = ld4(Wa + idx);
 #pragma unroll
-        for (int q = 0; q < 4; ++q) {
-            const int r = r0 + q;
-            idx[q] = (size_t(k0 + (r >> 3)) * n + (j0 + (r & 7))) * n + x;
-            f0[q] = w0[q] = 0.f;
-            if (upd & (1u << q)) {
-                if constexpr (sizeof(TF) == 4) {
-                    f0[q] = F[idx[q]];
-                    w0[q] = Wa[idx[q]];
-                } else {
-                    f0[q] = __half2float(F[idx[q]]);
-                    w0[q] = float(Wa[idx[q]]) * (1.0f / KF_WEIGHT_SCALE);
-                }
+            for (int q = 0; q < 4; ++q) {
+                if (!(upd & (1u << q))) continue;
+                float f0 = comp(fv, q), w0 = comp(wv, q);
+                fuse_update(f0, w0, fn[q], wn[q], c.max_w);
+                comp(fv, q) = f0;
+                comp(wv, q) = w0;
+                kmin = min(kmin, fkey(f0));
             }
-        }
+            st4(F + idx, fv);
+            st4(Wa + idx, wv);
+        } else {
+            uint2 fv = ld4(F + idx), wv = ld4(Wa + idx);
 #pragma unroll
-        for (int q = 0; q < 4; ++q) {
-            if (!(upd & (1u << q))) continue;
-            fuse_update(f0[q], w0[q], fn[q], wn[q], c.max_w);
-            if constexpr (sizeof(TF) == 4) {
-                F[idx[q]] = f0[q];
-                Wa[idx[q]] = w0[q];
-                kmin = min(kmin, fkey(f0[q]));
-            } else {
-                const __half hf = __float2half_rn(f0[q]);
-                F[idx[q]] = hf;
-                Wa[idx[q]] = uint16_t(fminf(rintf(w0[q] * KF_WEIGHT_SCALE), 65535.0f));
+            for (int q = 0; q < 4; ++q) {
+                if (!(upd & (1u << q))) continue;
+                float f0 = __half2float(__ushort_as_half(get16(fv, q)));
+                float w0 = float(get16(wv, q)) * (1.0f / KF_WEIGHT_SCALE);
+                fuse_update(f0, w0, fn[q], wn[q], c.max_w);
+                const __half hf = __float2half_rn(f0);
+                set16(fv, q, __half_as_ushort(hf));
+                set16(wv, q, uint16_t(fminf(rintf(w0 * KF_WEIGHT_SCALE), 65535.0f)));
                 kmin = min(kmin, fkey(__half2float(hf)));
             }
+            st4(F + idx, fv);
+            st4(Wa + idx, wv);
         }
     }
     if (c.bmin) {
-        // all of a lane's voxels in this block sit in brick (x >> 3, j0 >> 3, k0 >> 3):
-        // reduce over the brick's 8 lanes, one atomic per brick
-#pragma unroll
-        for (int off = 4; off >= 1; off >>= 1) kmin = min(kmin, __shfl_xor_sync(0xffffffffu, kmin, off));
-        if ((lane & 7) == 0 && kmin != 0x7fffffff && lane_in)
+        // a lane's voxels sit in brick (x >> 3, j0 >> 3, k0 >> 3): reduce over the lanes of the
+        // same brick (lane pairs along x, the four row groups), one atomic per brick
+        kmin = min(kmin, __shfl_xor_sync(0xffffffffu, kmin, 1));
+        kmin = min(kmin, __shfl_xor_sync(0xffffffffu, kmin, 8));
+        kmin = min(kmin, __shfl_xor_sync(0xffffffffu, kmin, 16));
+        if ((lane & 0x19) == 0 && kmin != 0x7fffffff && lane_in)
             atomicMin(c.bmin + (size_t(k0 >> 3) * c.nb + (j0 >> 3)) * c.nb + (x >> 3), kmin);
     }
 }
