@@ -336,7 +336,8 @@ __device__ void icp_begin(const EngineView& v, int s) {
     P->level = level;
     P->cont = level >= 0 ? 1 : 0;
     v.icp_sched[s] = sched_entry(v, s, level);
-    __threadfence();
+    // no fence here: thread 0 writes all of this, and the grid barrier that follows fences
+    // thread 0's writes before it arrives
 }
 
 // phase B for one session: FP64 combine of the tile pairs, solve, update, stop test
@@ -372,20 +373,21 @@ __device__ void icp_solve(const EngineView& v, int s, int level, int begin, int 
         for (int l = 0; l < kMaxLevels; ++l) rng[l] = v.iranges[l * S_cap + s];
     }
     // partial pairs as float4 (two entries each): thread (g, q) adds, in FP64 and in tile
-    // order, entries 2q and 2q + 1 of tiles g, g + 18, g + 36, ...; 8 tiles' loads in flight
+    // order, entries 2q and 2q + 1 of tiles g, g + 18, g + 36, ...; 9 tiles' loads in flight,
+    // so up to 162 partials (a grid of one block per SM) arrive in one round trip
     constexpr int kGroups = kIcpThreads / 14;   // 18
     const int q = tid % 14, g = tid / 14;
     if (g < kGroups) {
         const float4* src = reinterpret_cast<const float4*>(v.partials + size_t(begin) * kIcpPartialStride) + q;
         double a0 = 0.0, a1 = 0.0;
-        for (int t = g; t < cnt; t += 8 * kGroups) {
-            float4 p[8];
+        for (int t = g; t < cnt; t += 9 * kGroups) {
+            float4 p[9];
 #pragma unroll
-            for (int u = 0; u < 8; ++u)
+            for (int u = 0; u < 9; ++u)
                 p[u] = t + kGroups * u < cnt ? __ldcg(src + size_t(t + kGroups * u) * (kIcpPartialStride / 4))
                                              : make_float4(0.f, 0.f, 0.f, 0.f);
 #pragma unroll
-            for (int u = 0; u < 8; ++u)
+            for (int u = 0; u < 9; ++u)
                 if (t + kGroups * u < cnt) {
                     a0 += double(p[u].x) + double(p[u].y);
                     a1 += double(p[u].z) + double(p[u].w);
@@ -421,8 +423,7 @@ __device__ void icp_solve(const EngineView& v, int s, int level, int begin, int 
             P->status = KF_ERR_NONFINITE;
             P->level = -1;
             P->cont = 0;
-            v.icp_sched[s] = make_int4(-1, 0, 0, 0);
-            __threadfence();
+            v.icp_sched[s] = make_int4(-1, 0, 0, 0);   // published by the barrier's fence
         }
         return;
     }
@@ -491,7 +492,7 @@ __device__ void icp_solve(const EngineView& v, int s, int level, int begin, int 
     } else {
         v.icp_sched[s] = make_int4(-1, 0, 0, 0);
     }
-    __threadfence();
+    // lane 0 of warp 0 is thread 0, whose writes the grid barrier after phase B fences
 }
 
 // phase C for one session (one thread): the frame's pose becomes the previous pose; the
