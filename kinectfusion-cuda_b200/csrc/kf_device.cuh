@@ -5,6 +5,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <cuda/atomic>
+
 #include "../../include/kf_api.h"
 
 namespace kf {
@@ -222,12 +224,14 @@ __device__ __forceinline__ bool grid_barrier(GridSync* g, unsigned int nblocks, 
     if (threadIdx.x == 0) {
         ++epoch;
         const unsigned int target = epoch * nblocks;
-        __threadfence();
-        atomicAdd(&g->count, 1u);
+        // arrival releases the block's writes (the __syncthreads above orders them before
+        // thread 0's), the acquiring load that sees every arrival makes the others' visible
+        cuda::atomic_ref<unsigned int, cuda::thread_scope_device> cnt(g->count);
+        cnt.fetch_add(1u, cuda::memory_order_release);
         const unsigned long long t0 = global_ns();
         unsigned int spins = 0;
         while (true) {
-            const unsigned int c = *((volatile unsigned int*)&g->count);
+            const unsigned int c = cnt.load(cuda::memory_order_acquire);
             if (c >= target) break;
             if (*((volatile unsigned int*)&g->abort)) { ok = 0; break; }
             if ((++spins & 255u) == 0u && global_ns() - t0 > timeout_ns) {
@@ -238,7 +242,6 @@ __device__ __forceinline__ bool grid_barrier(GridSync* g, unsigned int nblocks, 
             }
             __nanosleep(32);
         }
-        __threadfence();
     }
     return __syncthreads_and(threadIdx.x == 0 ? ok : 1) != 0;
 }
