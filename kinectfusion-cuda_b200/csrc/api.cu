@@ -421,6 +421,12 @@ struct Engine {
     // frame's volume and pose only): fork and join events and the branch's stream
     cudaStream_t aux_stream = nullptr;
     cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+    // a single session's frame from host memory: its copy runs on h2d_stream while the frame's
+    // raycast (which needs only the previous frame) runs; the preprocess branch of the graph
+    // waits for ev_input (an external event wait node), recorded after every frame's copy
+    bool input_wait = false;
+    cudaStream_t h2d_stream = nullptr;
+    cudaEvent_t ev_input = nullptr, ev_prev = nullptr;
     bool stages[4] = {true, true, true, true};
     // per-stage timing: events between the launches (also inside the captured graph)
     bool profile = false;
@@ -461,6 +467,9 @@ struct Engine {
         KF_CK(cudaStreamCreateWithFlags(&aux_stream, cudaStreamNonBlocking));
         KF_CK(cudaEventCreateWithFlags(&ev_fork, cudaEventDisableTiming));
         KF_CK(cudaEventCreateWithFlags(&ev_join, cudaEventDisableTiming));
+        KF_CK(cudaStreamCreateWithFlags(&h2d_stream, cudaStreamNonBlocking));
+        KF_CK(cudaEventCreateWithFlags(&ev_input, cudaEventDisableTiming));
+        KF_CK(cudaEventCreateWithFlags(&ev_prev, cudaEventDisableTiming));
         // persistent grids (kf_batch_autotune may replace the first, second and fourth)
         grid_pre = sms * 4;
         grid_ray = sms * 6;
@@ -510,6 +519,9 @@ struct Engine {
         if (aux_stream) cudaStreamDestroy(aux_stream);
         if (ev_fork) cudaEventDestroy(ev_fork);
         if (ev_join) cudaEventDestroy(ev_join);
+        if (h2d_stream) cudaStreamDestroy(h2d_stream);
+        if (ev_input) cudaEventDestroy(ev_input);
+        if (ev_prev) cudaEventDestroy(ev_prev);
     }
 
     EngineView view() const {
@@ -681,10 +693,12 @@ struct Engine {
             // preprocess on a branch beside the raycast; ICP waits for both
             KF_CK(cudaEventRecord(ev_fork, st));
             KF_CK(cudaStreamWaitEvent(aux_stream, ev_fork, 0));
+            if (input_wait) KF_CK(cudaStreamWaitEvent(aux_stream, ev_input, cudaEventWaitExternal));
             KF_CK(launch_preprocess(v, grid_pre, aux_stream));
             if (profile) KF_CK(cudaEventRecordWithFlags(ev[1], aux_stream, cudaEventRecordExternal));
             KF_CK(cudaEventRecord(ev_join, aux_stream));
         } else {
+            if (stages[0] && input_wait) KF_CK(cudaStreamWaitEvent(st, ev_input, cudaEventWaitExternal));
             if (stages[0]) KF_CK(launch_preprocess(v, grid_pre, st));
             if (profile) KF_CK(cudaEventRecordWithFlags(ev[1], st, cudaEventRecordExternal));
         }
@@ -934,6 +948,7 @@ kf_status kf_session_create(const kf_config* cfg, kf_session** out) {
     if (!s->eng) { delete s; return KF_ERR_ARG; }
     s->owns = true;
     kf_status st = s->eng->init(1);
+    s->eng->input_wait = true;   // one session: its host frames copy beside the raycast
     if (st == KF_OK) st = slot_create(s->eng->slots[0], *cfg);
     if (st != KF_OK) { s->eng->destroy(); delete s->eng; delete s; return st; }
     s->eng->tables_dirty = true;
@@ -963,9 +978,20 @@ static kf_status session_enqueue(kf_session* s, const uint16_t* depth, int is_de
     std::vector<StepDev> want(s->eng->cap, StepDev{0, 0});
     want[s->slot] = StepDev{1, sl.frames == 0 ? 1 : 0};
     KF_TRY(s->eng->set_step(want, st));
-    KF_CK(cudaMemcpyAsync(const_cast<uint16_t*>(sl.d.raw), depth, bytes,
-                          is_dev ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, st));
-    return s->eng->enqueue(st);
+    Engine& e = *s->eng;
+    if (e.input_wait && !is_dev) {
+        // the copy waits for the work already on st (the previous frame reads this buffer), then
+        // runs beside the new frame's raycast
+        KF_CK(cudaEventRecord(e.ev_prev, st));
+        KF_CK(cudaStreamWaitEvent(e.h2d_stream, e.ev_prev, 0));
+        KF_CK(cudaMemcpyAsync(const_cast<uint16_t*>(sl.d.raw), depth, bytes, cudaMemcpyHostToDevice, e.h2d_stream));
+        KF_CK(cudaEventRecord(e.ev_input, e.h2d_stream));
+    } else {
+        KF_CK(cudaMemcpyAsync(const_cast<uint16_t*>(sl.d.raw), depth, bytes,
+                              is_dev ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, st));
+        if (e.input_wait) KF_CK(cudaEventRecord(e.ev_input, st));
+    }
+    return e.enqueue(st);
 }
 
 kf_status kf_process_frame(kf_session* s, const uint16_t* depth, int is_device_ptr, void* stream, float pose_out[16]) {
