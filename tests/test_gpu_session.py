@@ -192,6 +192,26 @@ def test_device_input_path(kf, cuda, run_small):
     s2.close()
 
 
+def test_mixed_host_device_and_async_frames(kf, cuda, run_small):
+    """A host frame's copy runs on a stream of its own beside the raycast; device frames
+    (synchronous and queued) go through the session's stream.  Mixing them frame by frame
+    gives the same poses and volume as host frames alone."""
+    cfg, imgs, s, P, rows = run_small
+    s2 = kf.KinectFusion(cfg)
+    for i in range(6):
+        if i % 3 == 0:
+            st, pose = s2.process_frame(imgs[i])
+        elif i % 3 == 1:
+            st, pose = s2.process_frame(cuda.from_numpy(imgs[i].view(np.int16)).cuda())
+        else:
+            d = cuda.from_numpy(imgs[i].view(np.int16)).cuda()
+            s2.process_frame_async(d)
+            cuda.cuda.synchronize()
+            pose = s2.pose()
+        np.testing.assert_array_equal(pose, rows[i][2])
+    s2.close()
+
+
 def test_trunc8_compat_mode(kf, orc):
     from kfb200 import synth
     cfg = kf.config_small(compat_trunc8=1)
