@@ -530,6 +530,7 @@ struct Engine {
         v.itiles = d_itiles; v.iranges = d_iranges; v.fuse_prefix = d_fprefix; v.brick_prefix = d_bprefix;
         v.super_prefix = d_sprefix;
         v.partials = d_partials;
+        v.partials2 = d_partials ? d_partials + cap_part / 2 : nullptr;   // two equal halves
         v.icp_sched = d_icp_sched;
         v.icp_mats = d_icp_mats;
         v.sync = d_sync; v.counters = d_ctr;
@@ -572,7 +573,7 @@ struct Engine {
         KF_TRY(grow(d_pre, cap_pre, int(need_pre)));
         KF_TRY(grow(d_ray, cap_ray, int(need_ray)));
         KF_TRY(grow(d_itiles, cap_it, int(need_it)));
-        KF_TRY(grow(d_partials, cap_part, int(need_it) * kIcpPartialStride));
+        KF_TRY(grow(d_partials, cap_part, 2 * int(need_it) * kIcpPartialStride));
         KF_TRY(grow(d_longq, cap_longq, std::max<int>(1024, int(need_ray) * 32 / 4) * long_ray_bytes()));
         KF_TRY(grow(d_fuseq, cap_fuseq, int(need_fq)));
         if (old_pre != cap_pre || old_ray != cap_ray || old_it != cap_it || old_part != cap_part || old_lq != cap_longq ||
@@ -651,7 +652,7 @@ struct Engine {
         KF_TRY(grow(d_pre, cap_pre, std::max<int>(1, int(pre.size()))));
         KF_TRY(grow(d_ray, cap_ray, std::max<int>(1, int(ray.size()))));
         KF_TRY(grow(d_itiles, cap_it, std::max<int>(1, int(all.size()))));
-        KF_TRY(grow(d_partials, cap_part, std::max<int>(1, int(all.size())) * kIcpPartialStride));
+        KF_TRY(grow(d_partials, cap_part, 2 * std::max<int>(1, int(all.size())) * kIcpPartialStride));
         // room for a quarter of all rays to take the long-ray path (more fall back to the lane)
         KF_TRY(grow(d_longq, cap_longq, std::max<int>(1024, int(ray.size()) * 32 / 4) * long_ray_bytes()));
         if (old_pre != cap_pre || old_ray != cap_ray || old_it != cap_it || old_part != cap_part || old_lq != cap_longq ||
@@ -705,7 +706,7 @@ struct Engine {
         if (stages[1]) KF_CK(launch_raycast(v, grid_ray, st));
         if (fork) KF_CK(cudaStreamWaitEvent(st, ev_join, 0));
         if (profile) KF_CK(cudaEventRecordWithFlags(ev[2], st, cudaEventRecordExternal));
-        if (stages[2]) KF_CK(launch_icp(v, grid_icp, st));
+        if (stages[2]) KF_CK(launch_icp(v, grid_icp, st, cap == 1));
         if (profile) KF_CK(cudaEventRecordWithFlags(ev[3], st, cudaEventRecordExternal));
         if (stages[3]) KF_CK(launch_fuse(v, grid_fuse, st));
         if (stages[3]) KF_CK(launch_bricks(v, grid_brick, st));
@@ -1489,7 +1490,7 @@ kf_status kf_compute_pose(const float* const* vertex, const float* const* target
     StepDev step{1, 0};
     e = cudaMemcpy(eng.d_step, &step, sizeof(step), cudaMemcpyHostToDevice);
     if (e == cudaSuccess) e = cudaMemsetAsync(eng.d_sync, 0, sizeof(GridSync), s);
-    if (e == cudaSuccess) e = launch_icp(eng.view(), eng.grid_icp, s);
+    if (e == cudaSuccess) e = launch_icp(eng.view(), eng.grid_icp, s, eng.cap == 1);
     if (e == cudaSuccess) e = cudaMemcpyAsync(eng.h_out, eng.d_out, sizeof(OutDev), cudaMemcpyDeviceToHost, s);
     if (e == cudaSuccess) e = cudaMemcpyAsync(eng.h_sync, eng.d_sync, sizeof(GridSync), cudaMemcpyDeviceToHost, s);
     if (e == cudaSuccess) e = cudaStreamSynchronize(s);

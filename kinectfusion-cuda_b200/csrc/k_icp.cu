@@ -314,28 +314,61 @@ __device__ __forceinline__ int4 sched_entry(const EngineView& v, int s, int leve
     return make_int4(level, rg.begin, rg.end - rg.begin, 0);
 }
 
+// Where a session's ICP iteration state lives: in the session's pose block and the engine's
+// schedule and matrix arrays (one owner block updates them and a grid barrier publishes
+// them), or in a block's shared memory (every block updates its own copy, identically).
+struct IcpStateRef {
+    double* R;
+    double* t;
+    int* it;
+    int* iters;
+    int* level;
+    int* cont;
+    int* status;
+    float* mats;   // the 24 floats phase A reads
+    int4* sched;   // the schedule entry of the next pass
+};
+
+__device__ __forceinline__ IcpStateRef global_state(const EngineView& v, int s) {
+    PoseDev* P = v.sess[s].pose;
+    return IcpStateRef{P->R, P->t, &P->it, P->iters, &P->level, &P->cont, &P->status,
+                       v.icp_mats + size_t(s) * 24, v.icp_sched + s};
+}
+
+struct IcpLocal {
+    double R[9], t[3];
+    int it, level, cont, status;
+    int iters[kMaxLevels];
+    float mats[24];
+    int4 sched;
+};
+
+__device__ __forceinline__ IcpStateRef local_state(IcpLocal& L) {
+    return IcpStateRef{L.R, L.t, &L.it, L.iters, &L.level, &L.cont, &L.status, L.mats, &L.sched};
+}
+
 // phase 0 for one session (one thread); every slot gets a schedule entry
-__device__ void icp_begin(const EngineView& v, int s) {
+__device__ void icp_begin(const EngineView& v, int s, const IcpStateRef& ref) {
     const SessionDev* S = &v.sess[s];
     const StepDev st = v.step[s];
     if (!st.active) {   // empty or idle slot: its state is not touched
-        v.icp_sched[s] = make_int4(-1, 0, 0, 0);
+        *ref.sched = make_int4(-1, 0, 0, 0);
         return;
     }
-    PoseDev* P = S->pose;
-    P->status = KF_OK;
-    for (int l = 0; l < kMaxLevels; ++l) P->iters[l] = 0;
-    P->it = 0;
+    const PoseDev* P = S->pose;
+    *ref.status = KF_OK;
+    for (int l = 0; l < kMaxLevels; ++l) ref.iters[l] = 0;
+    *ref.it = 0;
     int level = -1;
     if (!st.first) {
-        for (int q = 0; q < 9; ++q) P->R[q] = P->Rp[q];
-        for (int q = 0; q < 3; ++q) P->t[q] = P->tp[q];
+        for (int q = 0; q < 9; ++q) ref.R[q] = P->Rp[q];
+        for (int q = 0; q < 3; ++q) ref.t[q] = P->tp[q];
         level = next_level(S, S->L - 1);
-        if (level >= 0) publish_mats(v.icp_mats + size_t(s) * 24, P->Rp, P->tp, P->Rp, P->tpf, S->lv[level]);
+        if (level >= 0) publish_mats(ref.mats, P->Rp, P->tp, P->Rp, P->tpf, S->lv[level]);
     }
-    P->level = level;
-    P->cont = level >= 0 ? 1 : 0;
-    v.icp_sched[s] = sched_entry(v, s, level);
+    *ref.level = level;
+    *ref.cont = level >= 0 ? 1 : 0;
+    *ref.sched = sched_entry(v, s, level);
     // no fence here: thread 0 writes all of this, and the grid barrier that follows fences
     // thread 0's writes before it arrives
 }
@@ -345,9 +378,12 @@ __device__ void icp_begin(const EngineView& v, int s) {
 // sm: 19 * 28 doubles of shared scratch.  Warp 0 runs the solve redundantly on every lane
 // (identical values), so the three sines and cosines are computed on three lanes at once and
 // no lane waits on another through memory; lane 0 stores the results.
-__device__ void icp_solve(const EngineView& v, int s, int level, int begin, int cnt, double* sm) {
+template <bool kLocal>
+__device__ void icp_solve(const EngineView& v, int s, int level, int begin, int cnt, double* sm,
+                          const float* parts, IcpLocal* loc) {
+    const IcpStateRef ref = kLocal ? local_state(*loc) : global_state(v, s);
     const SessionDev* S = &v.sess[s];
-    PoseDev* P = S->pose;
+    const PoseDev* P = S->pose;
     const int tid = threadIdx.x, lane = tid & 31;
     // warp 0 fetches everything the update needs while the block sums the tiles
     double R0[9], t0[3], Rp[9];
@@ -356,11 +392,12 @@ __device__ void icp_solve(const EngineView& v, int s, int level, int begin, int 
     IcpRange rng[kMaxLevels];
     if (tid < 32) {
 #pragma unroll
-        for (int q = 0; q < 9; ++q) { R0[q] = ldcg(&P->R[q]); Rp[q] = ldcg(&P->Rp[q]); }
+        // the state was written by this block's thread 0 (ordered by the block barriers)
+        for (int q = 0; q < 9; ++q) { R0[q] = ref.R[q]; Rp[q] = ldcg(&P->Rp[q]); }
 #pragma unroll
-        for (int q = 0; q < 3; ++q) { t0[q] = ldcg(&P->t[q]); tpf[q] = ldcg(&P->tpf[q]); }
-        it0 = ldcg(&P->it);
-        done0 = ldcg(&P->iters[level]);
+        for (int q = 0; q < 3; ++q) { t0[q] = ref.t[q]; tpf[q] = ldcg(&P->tpf[q]); }
+        it0 = *ref.it;
+        done0 = ref.iters[level];
         S_cap = v.tb->S;
         stop_a = S->stop_a;
         stop_d = S->stop_d;
@@ -378,7 +415,7 @@ __device__ void icp_solve(const EngineView& v, int s, int level, int begin, int 
     constexpr int kGroups = kIcpThreads / 14;   // 18
     const int q = tid % 14, g = tid / 14;
     if (g < kGroups) {
-        const float4* src = reinterpret_cast<const float4*>(v.partials + size_t(begin) * kIcpPartialStride) + q;
+        const float4* src = reinterpret_cast<const float4*>(parts + size_t(begin) * kIcpPartialStride) + q;
         double a0 = 0.0, a1 = 0.0;
         for (int t = g; t < cnt; t += 9 * kGroups) {
             float4 p[9];
@@ -420,10 +457,10 @@ __device__ void icp_solve(const EngineView& v, int s, int level, int begin, int 
     if (!solved) {
         if (lane == 0) {
             // the reference throws (project/src/icp.cpp:67-73): keep the previous pose, no fusion
-            P->status = KF_ERR_NONFINITE;
-            P->level = -1;
-            P->cont = 0;
-            v.icp_sched[s] = make_int4(-1, 0, 0, 0);   // published by the barrier's fence
+            *ref.status = KF_ERR_NONFINITE;
+            *ref.level = -1;
+            *ref.cont = 0;
+            *ref.sched = make_int4(-1, 0, 0, 0);   // published by the barrier's fence
         }
         return;
     }
@@ -465,15 +502,15 @@ __device__ void icp_solve(const EngineView& v, int s, int level, int begin, int 
     }
     if (lane != 0) return;
 #pragma unroll
-    for (int r = 0; r < 9; ++r) P->R[r] = R1[r];
+    for (int r = 0; r < 9; ++r) ref.R[r] = R1[r];
 #pragma unroll
-    for (int r = 0; r < 3; ++r) P->t[r] = t1[r];
-    P->iters[level] = done0 + 1;
-    P->it = it;
-    P->level = lvl;
-    P->cont = lvl >= 0 ? 1 : 0;
+    for (int r = 0; r < 3; ++r) ref.t[r] = t1[r];
+    ref.iters[level] = done0 + 1;
+    *ref.it = it;
+    *ref.level = lvl;
+    *ref.cont = lvl >= 0 ? 1 : 0;
     if (lvl >= 0) {
-        float* m = v.icp_mats + size_t(s) * 24;
+        float* m = ref.mats;
 #pragma unroll
         for (int r = 0; r < 9; ++r) m[r] = float(R1[r]);
 #pragma unroll
@@ -488,9 +525,9 @@ __device__ void icp_solve(const EngineView& v, int s, int level, int begin, int 
         }
 #pragma unroll
         for (int r = 0; r < 3; ++r) m[21 + r] = tpf[r];
-        v.icp_sched[s] = make_int4(lvl, rng[lvl].begin, rng[lvl].end - rng[lvl].begin, 0);
+        *ref.sched = make_int4(lvl, rng[lvl].begin, rng[lvl].end - rng[lvl].begin, 0);
     } else {
-        v.icp_sched[s] = make_int4(-1, 0, 0, 0);
+        *ref.sched = make_int4(-1, 0, 0, 0);
     }
     // lane 0 of warp 0 is thread 0, whose writes the grid barrier after phase B fences
 }
@@ -555,6 +592,7 @@ __device__ void block_inclusive_scan(int* a, int n, int* warp_tot) {
 constexpr int kIcpMaxSessionsSmem = 1024;
 constexpr int kIcpPixelsPerStep = 4;   // pixels a thread carries through one pipelined step
 
+template <bool local>
 __global__ void __launch_bounds__(kIcpThreads, 1) icp_kernel(EngineView v) {
     __shared__ float red[8 * 32 * 2];
     __shared__ double dsm[(kIcpThreads / 14 + 1) * 28];
@@ -563,19 +601,32 @@ __global__ void __launch_bounds__(kIcpThreads, 1) icp_kernel(EngineView v) {
     __shared__ short s_lvl[kIcpMaxSessionsSmem];
     __shared__ int s_beg[kIcpMaxSessionsSmem];
     __shared__ int s_wtot[kIcpThreads / 32];
+    __shared__ IcpLocal loc;
     const int tid = threadIdx.x;
     const unsigned int nb = gridDim.x;
     unsigned int epoch = 0;
     const int S_cap = v.tb->S;
+    // local (an engine of one session): every block runs the session's solve itself (the same arithmetic on the
+    // same partials, so every block's copy of the state is identical) and goes straight on to
+    // the next pass -- one grid barrier per pass instead of two.  The partials of consecutive
+    // passes go to alternate buffers, since a block may start writing the next pass's
+    // partials while another still sums this pass's; a block two passes on has passed a
+    // barrier that every block reaches only after its solve.
 
-    for (int s = blockIdx.x; s < S_cap; s += gridDim.x)
-        if (tid == 0) icp_begin(v, s);
-    if (!grid_barrier(v.sync, nb, epoch)) return;
+    if (local) {
+        if (tid == 0) icp_begin(v, 0, local_state(loc));
+        __syncthreads();
+    } else {
+        for (int s = blockIdx.x; s < S_cap; s += gridDim.x)
+            if (tid == 0) icp_begin(v, s, global_state(v, s));
+        if (!grid_barrier(v.sync, nb, epoch)) return;
+    }
 
     for (int pass = 0; pass < kIcpMaxPasses; ++pass) {
+        float* const parts = (local && (pass & 1)) ? v.partials2 : v.partials;
         // which sessions iterate in this pass, at which level, with which tiles
         for (int s = tid; s < S_cap; s += blockDim.x) {
-            const int4 e = __ldcg(v.icp_sched + s);
+            const int4 e = local ? loc.sched : __ldcg(v.icp_sched + s);
             s_lvl[s] = short(e.x);
             s_beg[s] = e.y;
             s_pre[s + 1] = e.x >= 0 ? e.z : 0;
@@ -604,13 +655,13 @@ __global__ void __launch_bounds__(kIcpThreads, 1) icp_kernel(EngineView v) {
                 const int s = lo, lvl = s_lvl[s];
                 if (s != run_s) {
                     if (run_s >= 0) {
-                        block_reduce_store(acc, red, v.partials + size_t(s_beg[run_s] + run_slot) * kIcpPartialStride);
+                        block_reduce_store(acc, red, parts + size_t(s_beg[run_s] + run_slot) * kIcpPartialStride);
 #pragma unroll
                         for (int q = 0; q < 32; ++q) acc[q] = 0.f;
                     }
                     run_s = s;
                     run_slot = vt - s_pre[s];
-                    if (tid < 24) mats[tid] = ldcg(v.icp_mats + size_t(s) * 24 + tid);
+                    if (tid < 24) mats[tid] = local ? loc.mats[tid] : ldcg(v.icp_mats + size_t(s) * 24 + tid);
                     __syncthreads();
                 }
                 const IcpTile T = v.itiles[s_beg[s] + (vt - s_pre[s])];
@@ -629,17 +680,43 @@ __global__ void __launch_bounds__(kIcpThreads, 1) icp_kernel(EngineView v) {
                                                  [&](const float (&a)[6], float b) { accumulate_products(acc, a, b); });
             }
             if (run_s >= 0)
-                block_reduce_store(acc, red, v.partials + size_t(s_beg[run_s] + run_slot) * kIcpPartialStride);
+                block_reduce_store(acc, red, parts + size_t(s_beg[run_s] + run_slot) * kIcpPartialStride);
         }
         if (!grid_barrier(v.sync, nb, epoch)) return;
 
+        if (local) {
+            // phase B in every block, on its own copy of the state
+            if (s_lvl[0] >= 0)
+                icp_solve<true>(v, 0, s_lvl[0], s_beg[0], min(s_pre[1] - s_pre[0], int(gridDim.x)), dsm, parts, &loc);
+            __syncthreads();
+            continue;
+        }
         // phase B: the block that owns a session solves it
         for (int s = blockIdx.x; s < S_cap; s += gridDim.x) {
             if (s_lvl[s] < 0) continue;
-            icp_solve(v, s, s_lvl[s], s_beg[s], min(s_pre[s + 1] - s_pre[s], int(gridDim.x)), dsm);
+            icp_solve<false>(v, s, s_lvl[s], s_beg[s], min(s_pre[s + 1] - s_pre[s], int(gridDim.x)), dsm, parts,
+                             nullptr);
             __syncthreads();
         }
         if (!grid_barrier(v.sync, nb, epoch)) return;
+    }
+
+    if (local) {
+        // block 0 stores the state the rest of the frame and the host read
+        if (blockIdx.x == 0 && tid == 0 && v.step[0].active) {
+            PoseDev* P = v.sess[0].pose;
+            if (!v.step[0].first) {   // a first frame has no estimate (fusion only)
+                for (int q = 0; q < 9; ++q) P->R[q] = loc.R[q];
+                for (int q = 0; q < 3; ++q) P->t[q] = loc.t[q];
+            }
+            for (int l = 0; l < kMaxLevels; ++l) P->iters[l] = loc.iters[l];
+            P->it = loc.it;
+            P->level = loc.level;
+            P->cont = loc.cont;
+            P->status = loc.status;
+            icp_finish(&v.sess[0], v.step[0], v.out);
+        }
+        return;
     }
 
     for (int s = blockIdx.x; s < S_cap; s += gridDim.x)
@@ -664,9 +741,10 @@ cudaError_t launch_barrier_selftest(GridSync* g, unsigned long long timeout_ns, 
     return cudaLaunchCooperativeKernel((const void*)barrier_selftest_kernel, dim3(2), dim3(32), args, 0, st);
 }
 
-cudaError_t launch_icp(const EngineView& v, int grid, cudaStream_t st) {
+cudaError_t launch_icp(const EngineView& v, int grid, cudaStream_t st, bool single) {
     void* args[] = {const_cast<EngineView*>(&v)};
-    return cudaLaunchCooperativeKernel((const void*)icp_kernel, dim3(grid), dim3(kIcpThreads), args, 0, st);
+    const void* k = single ? (const void*)icp_kernel<true> : (const void*)icp_kernel<false>;
+    return cudaLaunchCooperativeKernel(k, dim3(grid), dim3(kIcpThreads), args, 0, st);
 }
 
 // ---- stage: kernel::constructIcpResiduals (A rows and b to HBM, as the reference) ----

@@ -40,6 +40,7 @@ struct EngineView {
     const long long* brick_prefix;// S + 1 entries, in bricks
     const long long* super_prefix;// S + 1 entries, in super-bricks
     float* partials;             // ICP tile partials, kIcpPartialStride floats per tile
+    float* partials2;            // a second set: a single session's odd passes (see icp_kernel)
     int4* icp_sched;             // per slot: {level of the next ICP pass or -1, first tile, tiles, 0}
     float* icp_mats;             // per slot: 24 floats phase A reads (R, t, K_l R_prev^T, t_prev)
     GridSync* sync;
@@ -64,7 +65,8 @@ constexpr int kIcpMaxPasses = 64;     // hard cap on ICP passes per frame
 // launch helpers (each returns the CUDA error of its launch)
 cudaError_t launch_preprocess(const EngineView& v, int grid, cudaStream_t st);
 cudaError_t launch_raycast(const EngineView& v, int grid, cudaStream_t st);
-cudaError_t launch_icp(const EngineView& v, int grid, cudaStream_t st);
+// single: an engine of one slot (the kernel keeps that session's state per block)
+cudaError_t launch_icp(const EngineView& v, int grid, cudaStream_t st, bool single);
 cudaError_t launch_fuse(const EngineView& v, int grid, cudaStream_t st);
 // widen the brick lower bounds to the 2 x 2 x 2 bricks the raycaster reads, and bound the
 // super-bricks (one launch)
