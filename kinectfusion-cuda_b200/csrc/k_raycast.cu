@@ -49,9 +49,12 @@ struct RayState {
     int guard;        // samples taken (hard bound)
 };
 
-struct LongRay {
+// a ray handed from a lane to a warp: where it is, its exact march state and its geometry (so
+// the warp neither reloads the pose nor divides again)
+struct __align__(16) LongRay {
     int s, level, i, j;
     RayState st;
+    RayGeo g;
 };
 
 __device__ __forceinline__ void ray_matrix(const SessionDev* S, const LevelDev& Lv, float* m, F3& o) {
@@ -384,7 +387,7 @@ __device__ void serial_ray(const EngineView& v, const SessionDev* S, int s, cons
     if (!march_serial(S, g, f, st, budget, precise)) {
         const unsigned int slot = atomicAdd(&v.counters[6], 1u);
         if (slot < unsigned(v.longq_cap)) {
-            v.longq[slot] = LongRay{s, level, i, j, st};
+            v.longq[slot] = LongRay{s, level, i, j, st, g};
             return;
         }
         march_serial(S, g, f, st, 0x7fffffff, precise);   // queue full: finish here
@@ -423,11 +426,7 @@ __global__ void __launch_bounds__(256, 3) raycast_kernel(EngineView v) {
 template <class TF>
 __device__ void coop_ray(const SessionDev* S, const LongRay& L, int lane) {
     const TF* f = static_cast<const TF*>(S->tf);
-    float m[9];
-    F3 o;
-    ray_matrix(S, S->lv[L.level], m, o);
-    RayGeo g;
-    make_geo(S, m, o, L.i, L.j, g);
+    const RayGeo g = L.g;
     RayState st = L.st;
     float precise = 0.0f;
     march_coop(S, g, f, st, lane, precise);
