@@ -82,7 +82,9 @@ __device__ __forceinline__ bool block_culled(const FuseCtx& c, int x0, int j0, i
     float pxmin = 3.0e38f, pxmax = -3.0e38f, pymin = 3.0e38f, pymax = -3.0e38f;
 #pragma unroll
     for (int q = 0; q < 8; ++q) {
-        const float px = (c.fx * ex[q] + c.cx * ez[q]) / ez[q], py = (c.fy * ey[q] + c.cy * ez[q]) / ez[q];
+        // approximate division (a few 1e-4 px at most): the bounds below keep 0.01 px margins
+        const float px = __fdividef(c.fx * ex[q] + c.cx * ez[q], ez[q]);
+        const float py = __fdividef(c.fy * ey[q] + c.cy * ez[q], ez[q]);
         pxmin = fminf(pxmin, px);
         pxmax = fmaxf(pxmax, px);
         pymin = fminf(pymin, py);
@@ -352,19 +354,13 @@ cudaError_t launch_fuse(const EngineView& v, int grid, cudaStream_t st) {
 
 __device__ __forceinline__ int large_key() { return __float_as_int(0.991f); }
 
-// bdil[b] = min of bmin over bricks {b, b+1}^3 (clamped)
-__device__ __forceinline__ void dilate_brick(const int* __restrict__ m, int* bdil, int nb, long long b) {
-    const int bx = int(b % nb), by = int((b / nb) % nb), bz = int(b / ((long long)nb * nb));
-    const int x1 = min(bx + 1, nb - 1), y1 = min(by + 1, nb - 1), z1 = min(bz + 1, nb - 1);
-    int k = 0x7fffffff;
-    k = min(k, __ldg(m + (size_t(bz) * nb + by) * nb + bx));
-    k = min(k, __ldg(m + (size_t(bz) * nb + by) * nb + x1));
-    k = min(k, __ldg(m + (size_t(bz) * nb + y1) * nb + bx));
-    k = min(k, __ldg(m + (size_t(bz) * nb + y1) * nb + x1));
-    k = min(k, __ldg(m + (size_t(z1) * nb + by) * nb + bx));
-    k = min(k, __ldg(m + (size_t(z1) * nb + by) * nb + x1));
-    k = min(k, __ldg(m + (size_t(z1) * nb + y1) * nb + bx));
-    k = min(k, __ldg(m + (size_t(z1) * nb + y1) * nb + x1));
+// bdil[b] = min of bmin over bricks {b, b+1}^3 (clamped); nb^3 < 2^31, so 32-bit indices
+__device__ __forceinline__ void dilate_brick(const int* __restrict__ m, int* bdil, int nb, int b) {
+    const int bx = b % nb, byz = b / nb, by = byz % nb, bz = byz / nb;
+    const int dx = bx + 1 < nb ? 1 : 0, dy = by + 1 < nb ? nb : 0, dz = bz + 1 < nb ? nb * nb : 0;
+    const int* p = m + b;
+    int k = min(min(__ldg(p), __ldg(p + dx)), min(__ldg(p + dy), __ldg(p + dy + dx)));
+    k = min(k, min(min(__ldg(p + dz), __ldg(p + dz + dx)), min(__ldg(p + dz + dy), __ldg(p + dz + dy + dx))));
     bdil[b] = k;
 }
 
@@ -402,7 +398,7 @@ __global__ void __launch_bounds__(256) bricks_kernel(EngineView v) {
             const int s = slot_of(v.brick_prefix, g, S_cap);
             if (!v.step[s].active) continue;
             const SessionDev* S = &v.sess[s];
-            dilate_brick(S->bmin, S->bdil, S->nb, g - __ldg(v.brick_prefix + s));
+            dilate_brick(S->bmin, S->bdil, S->nb, int(g - __ldg(v.brick_prefix + s)));
         }
     } else {
         const long long total = v.tb->super_total;
@@ -465,7 +461,7 @@ __global__ void rebuild_bricks_kernel(const TF* f, int n, int* bmin) {
 __global__ void dilate_one_kernel(const int* bmin, int* bdil, int nb) {
     const long long total = (long long)nb * nb * nb;
     for (long long b = blockIdx.x * (long long)blockDim.x + threadIdx.x; b < total; b += (long long)gridDim.x * blockDim.x)
-        dilate_brick(bmin, bdil, nb, b);
+        dilate_brick(bmin, bdil, nb, int(b));
 }
 
 __global__ void superbrick_one_kernel(const int* bmin, int* sdil, int nb) {
