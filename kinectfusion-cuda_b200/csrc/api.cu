@@ -421,10 +421,11 @@ struct Engine {
     // frame's volume and pose only): fork and join events and the branch's stream
     cudaStream_t aux_stream = nullptr;
     cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
-    // a single session's frame from host memory: its copy runs on h2d_stream while the frame's
-    // raycast (which needs only the previous frame) runs; the preprocess branch of the graph
-    // waits for ev_input (an external event wait node), recorded after every frame's copy
-    bool input_wait = false;
+    // frames from host memory: their copies run on h2d_stream while the step's raycast (which
+    // needs only the previous frames) runs; the preprocess branch of the graph waits for
+    // ev_input (an external event wait node), recorded after every step's copies
+    bool input_wait = true;
+    bool capturing = false;   // record() runs inside a stream capture (the wait becomes a node)
     cudaStream_t h2d_stream = nullptr;
     cudaEvent_t ev_input = nullptr, ev_prev = nullptr;
     bool stages[4] = {true, true, true, true};
@@ -476,6 +477,20 @@ struct Engine {
         grid_fuse = sms * 4;
         grid_brick = sms * 4;
         grid_icp = icp_max_grid(sms);
+        return KF_OK;
+    }
+
+    // the stream a step's frame copies go on: h2d_stream for host frames, after the work already
+    // queued on st (earlier steps read the same input buffers); st itself for device frames
+    kf_status begin_inputs(bool host, cudaStream_t st, cudaStream_t* cs) {
+        if (!host) { *cs = st; return KF_OK; }
+        KF_CK(cudaEventRecord(ev_prev, st));
+        KF_CK(cudaStreamWaitEvent(h2d_stream, ev_prev, 0));
+        *cs = h2d_stream;
+        return KF_OK;
+    }
+    kf_status end_inputs(cudaStream_t cs) {
+        KF_CK(cudaEventRecord(ev_input, cs));
         return KF_OK;
     }
 
@@ -694,12 +709,12 @@ struct Engine {
             // preprocess on a branch beside the raycast; ICP waits for both
             KF_CK(cudaEventRecord(ev_fork, st));
             KF_CK(cudaStreamWaitEvent(aux_stream, ev_fork, 0));
-            if (input_wait) KF_CK(cudaStreamWaitEvent(aux_stream, ev_input, cudaEventWaitExternal));
+            if (input_wait) KF_CK(cudaStreamWaitEvent(aux_stream, ev_input, capturing ? cudaEventWaitExternal : 0));
             KF_CK(launch_preprocess(v, grid_pre, aux_stream));
             if (profile) KF_CK(cudaEventRecordWithFlags(ev[1], aux_stream, cudaEventRecordExternal));
             KF_CK(cudaEventRecord(ev_join, aux_stream));
         } else {
-            if (stages[0] && input_wait) KF_CK(cudaStreamWaitEvent(st, ev_input, cudaEventWaitExternal));
+            if (stages[0] && input_wait) KF_CK(cudaStreamWaitEvent(st, ev_input, capturing ? cudaEventWaitExternal : 0));
             if (stages[0]) KF_CK(launch_preprocess(v, grid_pre, st));
             if (profile) KF_CK(cudaEventRecordWithFlags(ev[1], st, cudaEventRecordExternal));
         }
@@ -720,7 +735,9 @@ struct Engine {
         if (gexec) { cudaGraphExecDestroy(gexec); gexec = nullptr; }
         cudaGraph_t g = nullptr;
         KF_CK(cudaStreamBeginCapture(cap_stream, cudaStreamCaptureModeThreadLocal));
+        capturing = true;
         kf_status rs = record(cap_stream);
+        capturing = false;
         cudaError_t e = cudaStreamEndCapture(cap_stream, &g);
         if (rs != KF_OK || e != cudaSuccess) {
             if (g) cudaGraphDestroy(g);
@@ -949,7 +966,6 @@ kf_status kf_session_create(const kf_config* cfg, kf_session** out) {
     if (!s->eng) { delete s; return KF_ERR_ARG; }
     s->owns = true;
     kf_status st = s->eng->init(1);
-    s->eng->input_wait = true;   // one session: its host frames copy beside the raycast
     if (st == KF_OK) st = slot_create(s->eng->slots[0], *cfg);
     if (st != KF_OK) { s->eng->destroy(); delete s->eng; delete s; return st; }
     s->eng->tables_dirty = true;
@@ -980,18 +996,11 @@ static kf_status session_enqueue(kf_session* s, const uint16_t* depth, int is_de
     want[s->slot] = StepDev{1, sl.frames == 0 ? 1 : 0};
     KF_TRY(s->eng->set_step(want, st));
     Engine& e = *s->eng;
-    if (e.input_wait && !is_dev) {
-        // the copy waits for the work already on st (the previous frame reads this buffer), then
-        // runs beside the new frame's raycast
-        KF_CK(cudaEventRecord(e.ev_prev, st));
-        KF_CK(cudaStreamWaitEvent(e.h2d_stream, e.ev_prev, 0));
-        KF_CK(cudaMemcpyAsync(const_cast<uint16_t*>(sl.d.raw), depth, bytes, cudaMemcpyHostToDevice, e.h2d_stream));
-        KF_CK(cudaEventRecord(e.ev_input, e.h2d_stream));
-    } else {
-        KF_CK(cudaMemcpyAsync(const_cast<uint16_t*>(sl.d.raw), depth, bytes,
-                              is_dev ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, st));
-        if (e.input_wait) KF_CK(cudaEventRecord(e.ev_input, st));
-    }
+    cudaStream_t cs = st;
+    KF_TRY(e.begin_inputs(!is_dev, st, &cs));
+    KF_CK(cudaMemcpyAsync(const_cast<uint16_t*>(sl.d.raw), depth, bytes,
+                          is_dev ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, cs));
+    KF_TRY(e.end_inputs(cs));
     return e.enqueue(st);
 }
 
@@ -1554,12 +1563,15 @@ kf_status kf_batch_step(kf_batch* b, const uint16_t* const* depth, int is_device
         want[i] = StepDev{depth[i] ? 1 : 0, sl.frames == 0 ? 1 : 0};
     }
     KF_TRY(b->eng.set_step(want, st));
+    cudaStream_t cs = st;
+    KF_TRY(b->eng.begin_inputs(!is_device_ptr, st, &cs));
     for (int i = 0; i < b->n; ++i) {
         if (!depth[i]) continue;
         Slot& sl = b->eng.slots[i];
         KF_CK(cudaMemcpyAsync(const_cast<uint16_t*>(sl.d.raw), depth[i], size_t(sl.cfg.width) * sl.cfg.height * 2,
-                              is_device_ptr ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, st));
+                              is_device_ptr ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, cs));
     }
+    KF_TRY(b->eng.end_inputs(cs));
     KF_TRY(b->eng.enqueue(st));
     KF_CK(cudaStreamSynchronize(st));
     kf_status r = b->eng.collect(want);
@@ -1984,12 +1996,15 @@ kf_status kf_server_step(kf_server* s, int* served) {
     if (n == 0) return KF_OK;
     cudaStream_t st = s->stream;
     KF_TRY(s->eng.set_step(want, st));
+    cudaStream_t cs = st;
+    KF_TRY(s->eng.begin_inputs(true, st, &cs));
     for (int i = 0; i < cap; ++i) {
         if (!want[i].active) continue;
         const ServerSlot& h = s->hs[i];
         KF_CK(cudaMemcpyAsync(const_cast<uint16_t*>(s->eng.slots[i].d.raw), h.stage[h.inflight], h.stage_bytes,
-                              cudaMemcpyHostToDevice, st));
+                              cudaMemcpyHostToDevice, cs));
     }
+    KF_TRY(s->eng.end_inputs(cs));
     KF_TRY(s->eng.enqueue(st));
     KF_CK(cudaStreamSynchronize(st));
     kf_status r = s->eng.collect(want);
