@@ -375,7 +375,7 @@ def run_batched(kf, torch, steps, plain_fps):
         h = torch.empty(seqs[q].shape, dtype=torch.int16, pin_memory=True)
         h.copy_(seqs[q].cpu())
         pins.append(h)
-    for K in (8, 16, 32):
+    for K in (8, 16, 32, 48):
         cfgs = [kf.config_full(tsdf_format=kf.KF_TSDF_F16U16) for _ in range(K)]
         host = [pins[i % 8] for i in range(K)]
         devs = [seqs[i % 8] for i in range(K)]
