@@ -426,6 +426,7 @@ struct Engine {
     // ev_input (an external event wait node), recorded after every step's copies
     bool input_wait = true;
     bool capturing = false;   // record() runs inside a stream capture (the wait becomes a node)
+    bool ray_many = false;    // the step has many ray tiles: the raycast kernel's 4-block form
     cudaStream_t h2d_stream = nullptr;
     cudaEvent_t ev_input = nullptr, ev_prev = nullptr;
     bool stages[4] = {true, true, true, true};
@@ -685,6 +686,8 @@ struct Engine {
         tb.n_pre = int(pre.size());
         tb.n_ray = int(ray.size());
         tb.ray_budget = serial_budget(tb.n_ray);
+        if (ray_many != many_ray_tiles(tb.n_ray)) graph_dirty = true;
+        ray_many = many_ray_tiles(tb.n_ray);
         for (int l = 0; l < KF_MAX_LEVELS; ++l) {
             tb.n_itiles[l] = int(it[l].size());
             tb.icp_off[l] = off[l];
@@ -718,7 +721,7 @@ struct Engine {
             if (stages[0]) KF_CK(launch_preprocess(v, grid_pre, st));
             if (profile) KF_CK(cudaEventRecordWithFlags(ev[1], st, cudaEventRecordExternal));
         }
-        if (stages[1]) KF_CK(launch_raycast(v, grid_ray, st));
+        if (stages[1]) KF_CK(launch_raycast(v, grid_ray, st, ray_many));
         if (fork) KF_CK(cudaStreamWaitEvent(st, ev_join, 0));
         if (profile) KF_CK(cudaEventRecordWithFlags(ev[2], st, cudaEventRecordExternal));
         if (stages[2]) KF_CK(launch_icp(v, grid_icp, st, cap == 1));

@@ -32,7 +32,8 @@ constexpr int kSerialBudgetSingle = 40;
 constexpr int kSerialBudgetMany = 64;
 constexpr int kManyRayTiles = 25000;   // more ray tiles than this in a step: kSerialBudgetMany
 
-int serial_budget(int ray_tiles) { return ray_tiles > kManyRayTiles ? kSerialBudgetMany : kSerialBudgetSingle; }
+bool many_ray_tiles(int ray_tiles) { return ray_tiles > kManyRayTiles; }
+int serial_budget(int ray_tiles) { return many_ray_tiles(ray_tiles) ? kSerialBudgetMany : kSerialBudgetSingle; }
 
 struct RayGeo {
     F3 o, dir;
@@ -395,8 +396,11 @@ __device__ void serial_ray(const EngineView& v, const SessionDev* S, int s, cons
     finish_ray(S, g, f, level, i, j, precise);
 }
 
-// Each warp pulls 8 x 4-ray tiles on its own (no block-wide barrier).
-__global__ void __launch_bounds__(256, 3) raycast_kernel(EngineView v) {
+// Each warp pulls 8 x 4-ray tiles on its own (no block-wide barrier).  Steps of many ray tiles
+// run four blocks per SM (64 registers: more warps to hide the gathers behind); a single
+// session's step runs three (80 registers: fewer instructions per sample, a shorter tail).
+template <int kBlocksPerSm>
+__global__ void __launch_bounds__(256, kBlocksPerSm) raycast_kernel(EngineView v) {
     const int lane = threadIdx.x & 31;
     const int ntiles = v.tb->n_ray;
     const int budget = v.tb->ray_budget;
@@ -453,8 +457,11 @@ __global__ void __launch_bounds__(256) raycast_long_kernel(EngineView v) {
 
 int long_ray_bytes() { return int(sizeof(LongRay)); }
 
-cudaError_t launch_raycast(const EngineView& v, int grid, cudaStream_t st) {
-    raycast_kernel<<<grid, 256, 0, st>>>(v);
+cudaError_t launch_raycast(const EngineView& v, int grid, cudaStream_t st, bool many) {
+    if (many)
+        raycast_kernel<4><<<grid, 256, 0, st>>>(v);
+    else
+        raycast_kernel<3><<<grid, 256, 0, st>>>(v);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
     raycast_long_kernel<<<grid, 256, 0, st>>>(v);

@@ -25,6 +25,7 @@ struct Tables {
 
 struct LongRay;   // march state of a ray handed from a lane to a warp (k_raycast.cu)
 int serial_budget(int ray_tiles);   // ray_budget for a step with this many ray tiles
+bool many_ray_tiles(int ray_tiles); // a step large enough for the raycast's long-budget, 4-block form
 
 // raw pointers the kernels take
 struct EngineView {
@@ -64,7 +65,8 @@ constexpr int kIcpMaxPasses = 64;     // hard cap on ICP passes per frame
 
 // launch helpers (each returns the CUDA error of its launch)
 cudaError_t launch_preprocess(const EngineView& v, int grid, cudaStream_t st);
-cudaError_t launch_raycast(const EngineView& v, int grid, cudaStream_t st);
+// many: a step of more than kManyRayTiles ray tiles (serial_budget's rule)
+cudaError_t launch_raycast(const EngineView& v, int grid, cudaStream_t st, bool many);
 // single: an engine of one slot (the kernel keeps that session's state per block)
 cudaError_t launch_icp(const EngineView& v, int grid, cudaStream_t st, bool single);
 cudaError_t launch_fuse(const EngineView& v, int grid, cudaStream_t st);
