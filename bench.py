@@ -259,6 +259,55 @@ def algorithmic_bytes(cfg, fused_voxels, samples, hits=0):
     }
 
 
+def stage_rooflines(cfg, ab, stage_ms, peak, icp_iters, traffic, fps):
+    """Per-stage algorithmic bytes, achieved GB/s and fraction of the HBM peak for one frame,
+    with the ncu DRAM bytes beside them.  The raycast's time runs from the fork of the frame
+    graph, so it also covers the preprocess that runs beside it."""
+    px = [(cfg.width >> l) * (cfg.height >> l) for l in range(cfg.levels)]
+    pre = px[0] * (2 + 4 + 4 + 16) + sum(p * (4 + 16) for p in px[1:])
+    icp = sum(px[l] * 48 * icp_iters[l] for l in range(cfg.levels))
+    n3 = cfg.volume_n ** 3
+    rows = {
+        "preprocess": (pre, "u16 in, metres, bilateral, dmax tiles, vertex maps of every level"),
+        "raycast": (ab["raycast_gather"], "reference-equivalent gather (8 taps per sample the reference takes)"),
+        "icp": (icp, "48 B per pixel per iteration (source vertex, target vertex and normal), %s iterations"
+                % "/".join(str(i) for i in icp_iters)),
+        "fuse": (ab["fuse_dense"], "dense-equivalent n^3 read + write + depth map"),
+    }
+    out = {}
+    for k, ms in zip(["preprocess", "raycast", "icp", "fuse"], stage_ms):
+        b, note = rows[k]
+        ms = float(ms)
+        gbs = b / (ms / 1000.0) / 1e9 if ms > 0 else None
+        out[k] = {"ms": round(float(ms), 5), "algorithmic_bytes": int(b), "achieved_gbs": round(gbs, 1) if gbs else None,
+                  "frac": round(gbs / peak, 4) if gbs else None, "dram_bytes_ncu": traffic.get(k), "bytes": note}
+    fuse_s = stage_ms[3] / 1000.0
+    out["fuse"]["updated_bytes"] = int(ab["fuse_updated"])
+    out["fuse"]["updated_gbs"] = round(ab["fuse_updated"] / fuse_s / 1e9, 1) if fuse_s > 0 else None
+    out["fuse"]["voxels_per_s_dense"] = round(n3 / fuse_s, 1) if fuse_s > 0 else None
+    out["frame"] = {"voxels_per_s": round(n3 * fps, 1), "unit_note": "volume voxels integrated per second "
+                                                                        "(n^3 x frames/s)"}
+    return out
+
+
+def l2_read_gbs(torch):
+    """Read bandwidth of an L2-resident buffer (64 MB, under the 126 MB L2) through torch's
+    sum, timed with events after warm-up: the on-box L2 figure beside the gather numbers."""
+    x = torch.rand(16 * 1024 * 1024, device="cuda")
+    for _ in range(5):
+        x.sum()
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    a.record()
+    reps = 50
+    for _ in range(reps):
+        x.sum()
+    b.record()
+    b.synchronize()
+    ms = a.elapsed_time(b)
+    return round(x.numel() * 4 * reps / (ms / 1000.0) / 1e9, 1)
+
+
 # ---------------------------------------------------------------------------------------------
 # batched and served forms (rank 0, N = 1)
 # ---------------------------------------------------------------------------------------------
@@ -737,6 +786,12 @@ def run_ours(args, world, rank, local):
                     "stage_ms": {k: round(float(v), 5) for k, v in zip(names, stage_ms)},
                     "fuse_updated_voxels": fused, "raycast_samples": samples,
                     "fuse_updated_bytes": ab["fuse_updated"]}
+        stages = stage_rooflines(cfg, ab, stage_ms, peak, P.iters(), traffic, value)
+        l2 = l2_read_gbs(torch)
+        stages["raycast"]["l2_read_gbs"] = l2
+        stages["raycast"]["frac_of_l2_read"] = (round(stages["raycast"]["achieved_gbs"] / l2, 4)
+                                                if stages["raycast"]["achieved_gbs"] else None)
+        roofline["stages"] = stages
         progress("plain: roofline sample done")
         cpu = None
         if world == 1 and not args.no_cpu:
