@@ -290,22 +290,13 @@ def stage_rooflines(cfg, ab, stage_ms, peak, icp_iters, traffic, fps):
     return out
 
 
-def l2_read_gbs(torch):
-    """Read bandwidth of an L2-resident buffer (64 MB, under the 126 MB L2) through torch's
-    sum, timed with events after warm-up: the on-box L2 figure beside the gather numbers."""
-    x = torch.rand(16 * 1024 * 1024, device="cuda")
-    for _ in range(5):
-        x.sum()
-    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    torch.cuda.synchronize()
-    a.record()
-    reps = 50
-    for _ in range(reps):
-        x.sum()
-    b.record()
-    b.synchronize()
-    ms = a.elapsed_time(b)
-    return round(x.numel() * 4 * reps / (ms / 1000.0) / 1e9, 1)
+def l2_read_gbs(kf):
+    """Read bandwidth of an L2-resident buffer (64 MiB, under the 126 MB L2), 200 rounds in one
+    launch (kf_measure_read_bandwidth): the on-box L2 figure beside the gather numbers."""
+    import ctypes
+    g = ctypes.c_double()
+    st = kf.lib.kf_measure_read_bandwidth(64 << 20, 200, ctypes.byref(g))
+    return round(g.value, 1) if st == 0 else None
 
 
 # ---------------------------------------------------------------------------------------------
@@ -787,10 +778,10 @@ def run_ours(args, world, rank, local):
                     "fuse_updated_voxels": fused, "raycast_samples": samples,
                     "fuse_updated_bytes": ab["fuse_updated"]}
         stages = stage_rooflines(cfg, ab, stage_ms, peak, P.iters(), traffic, value)
-        l2 = l2_read_gbs(torch)
+        l2 = l2_read_gbs(kf)
         stages["raycast"]["l2_read_gbs"] = l2
         stages["raycast"]["frac_of_l2_read"] = (round(stages["raycast"]["achieved_gbs"] / l2, 4)
-                                                if stages["raycast"]["achieved_gbs"] else None)
+                                                if stages["raycast"]["achieved_gbs"] and l2 else None)
         roofline["stages"] = stages
         progress("plain: roofline sample done")
         cpu = None

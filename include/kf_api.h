@@ -390,6 +390,11 @@ kf_status kf_batch_stage_times(kf_batch* b, float ms[4]);
  * completed must give up after timeout_ms and report KF_ERR_TIMEOUT, leaving the context
  * usable.  waited_ms (may be NULL) gets the wall time the launch took. */
 kf_status kf_selftest_bounded_wait(int timeout_ms, int* waited_ms);
+/* Read bandwidth of this device (GB/s) over a buffer of `bytes` (16 MiB .. 4 GiB, a multiple of
+ * 16), read `rounds` times (1 .. 1000) by a grid of 8 blocks per SM after one untimed round.  A
+ * buffer under the L2's size measures the L2; the raycaster's gather rate is read against it.
+ * Allocates and frees its buffer.  No counterpart in the reference (a measurement aid). */
+kf_status kf_measure_read_bandwidth(size_t bytes, int rounds, double* gbs);
 
 #ifdef __cplusplus
 }

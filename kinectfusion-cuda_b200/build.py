@@ -17,7 +17,7 @@ LIB = os.path.join(HERE, "lib")
 OBJ = os.path.join(HERE, "_build")
 REPO = os.path.dirname(HERE)
 
-CU_SOURCES = ["k_preprocess.cu", "k_raycast.cu", "k_tsdf.cu", "k_icp.cu", "k_display.cu", "api.cu"]
+CU_SOURCES = ["k_preprocess.cu", "k_raycast.cu", "k_tsdf.cu", "k_icp.cu", "k_display.cu", "k_probe.cu", "api.cu"]
 CXX_SOURCES = ["dataset.cpp"]   # host-only parts of the library (zlib for 16-bit PNG)
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",

@@ -2148,4 +2148,36 @@ kf_status kf_selftest_bounded_wait(int timeout_ms, int* waited_ms) {
     return h_res == 1 ? KF_OK : KF_ERR_STATE;
 }
 
+kf_status kf_measure_read_bandwidth(size_t bytes, int rounds, double* gbs) {
+    if (!gbs || bytes < (size_t(16) << 20) || bytes > (size_t(4) << 30) || bytes % 16 || rounds < 1 || rounds > 1000)
+        return KF_ERR_ARG;
+    int dev = 0, sms = 0;
+    KF_CK(cudaGetDevice(&dev));
+    KF_CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    const int grid = sms * 8;
+    float4* buf = nullptr;
+    float* sink = nullptr;
+    cudaEvent_t a = nullptr, b = nullptr;
+    cudaError_t e = cudaMalloc(&buf, bytes);
+    if (e == cudaSuccess) e = cudaMalloc(&sink, sizeof(float) * grid);
+    if (e == cudaSuccess) e = cudaMemset(buf, 0, bytes);
+    if (e == cudaSuccess) e = cudaEventCreate(&a);
+    if (e == cudaSuccess) e = cudaEventCreate(&b);
+    const long long n4 = (long long)(bytes / 16);
+    if (e == cudaSuccess) e = launch_read_probe(buf, n4, 1, sink, grid, 0);   // warm: the buffer into L2
+    if (e == cudaSuccess) e = cudaEventRecord(a, 0);
+    if (e == cudaSuccess) e = launch_read_probe(buf, n4, rounds, sink, grid, 0);
+    if (e == cudaSuccess) e = cudaEventRecord(b, 0);
+    if (e == cudaSuccess) e = cudaEventSynchronize(b);
+    float ms = 0.f;
+    if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, a, b);
+    if (a) cudaEventDestroy(a);
+    if (b) cudaEventDestroy(b);
+    cudaFree(buf);
+    cudaFree(sink);
+    KF_CK(e);
+    *gbs = ms > 0.f ? double(bytes) * rounds / (double(ms) * 1e-3) / 1e9 : 0.0;
+    return KF_OK;
+}
+
 }  // extern "C"

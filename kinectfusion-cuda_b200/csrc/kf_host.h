@@ -79,6 +79,7 @@ cudaError_t launch_rebuild_bricks(const void* f, int fmt, int n, int* bmin, int*
 int icp_max_grid(int num_sms);
 int long_ray_bytes();
 cudaError_t launch_barrier_selftest(GridSync* g, unsigned long long timeout_ns, int* result, cudaStream_t st);
+cudaError_t launch_read_probe(const float4* buf, long long n4, int rounds, float* sink, int grid, cudaStream_t st);
 __host__ __device__ int fuse_units(int n);   // 32 x 8 x 8 voxel blocks of an n^3 volume
 
 cudaError_t launch_init_volume(void* f, void* w, long long nvox, int fmt, cudaStream_t st);

@@ -156,6 +156,7 @@ SIGNATURES = {
     "kf_batch_set_profiling": (_I, [_P, _I]),
     "kf_batch_stage_times": (_I, [_P, _FP]),
     "kf_selftest_bounded_wait": (_I, [_I, _IP]),
+    "kf_measure_read_bandwidth": (_I, [ctypes.c_size_t, _I, ctypes.POINTER(ctypes.c_double)]),
 }
 
 

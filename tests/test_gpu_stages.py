@@ -298,3 +298,14 @@ def test_bounded_wait_times_out_and_context_survives(kf, cuda):
     # the context is still usable
     x = cuda.ones(16, device="cuda")
     assert float((x * 2).sum()) == 32.0
+
+
+def test_read_bandwidth_probe(kf):
+    """The read-bandwidth probe runs and reports an L2-resident read rate above the HBM copy
+    rate (64 MiB fits the L2), and rejects sizes outside its range."""
+    import ctypes
+    g = ctypes.c_double()
+    assert kf.lib.kf_measure_read_bandwidth(64 << 20, 20, ctypes.byref(g)) == kf.KF_OK
+    assert g.value > 3000.0, g.value
+    assert kf.lib.kf_measure_read_bandwidth(1 << 20, 20, ctypes.byref(g)) == kf.KF_ERR_ARG
+    assert kf.lib.kf_measure_read_bandwidth(64 << 20, 0, ctypes.byref(g)) == kf.KF_ERR_ARG
