@@ -633,7 +633,7 @@ __global__ void __launch_bounds__(kIcpThreads, 1) icp_kernel(EngineView v) {
         }
         if (tid == 0) s_pre[0] = 0;
         __syncthreads();
-        block_inclusive_scan(s_pre + 1, S_cap, s_wtot);
+        if (!local) block_inclusive_scan(s_pre + 1, S_cap, s_wtot);   // one slot: s_pre[1] is its own count
         const int total = s_pre[S_cap];
         if (total == 0) break;   // block-uniform: every block reads the same schedule
 
