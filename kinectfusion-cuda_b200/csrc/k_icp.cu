@@ -684,24 +684,24 @@ __global__ void __launch_bounds__(kIcpThreads, 1) icp_kernel(EngineView v) {
         }
         if (!grid_barrier(v.sync, nb, epoch)) return;
 
-        if (local) {
+        if constexpr (local) {
             // phase B in every block, on its own copy of the state
             if (s_lvl[0] >= 0)
                 icp_solve<true>(v, 0, s_lvl[0], s_beg[0], min(s_pre[1] - s_pre[0], int(gridDim.x)), dsm, parts, &loc);
             __syncthreads();
-            continue;
+        } else {
+            // phase B: the block that owns a session solves it
+            for (int s = blockIdx.x; s < S_cap; s += gridDim.x) {
+                if (s_lvl[s] < 0) continue;
+                icp_solve<false>(v, s, s_lvl[s], s_beg[s], min(s_pre[s + 1] - s_pre[s], int(gridDim.x)), dsm,
+                                 parts, nullptr);
+                __syncthreads();
+            }
+            if (!grid_barrier(v.sync, nb, epoch)) return;
         }
-        // phase B: the block that owns a session solves it
-        for (int s = blockIdx.x; s < S_cap; s += gridDim.x) {
-            if (s_lvl[s] < 0) continue;
-            icp_solve<false>(v, s, s_lvl[s], s_beg[s], min(s_pre[s + 1] - s_pre[s], int(gridDim.x)), dsm, parts,
-                             nullptr);
-            __syncthreads();
-        }
-        if (!grid_barrier(v.sync, nb, epoch)) return;
     }
 
-    if (local) {
+    if constexpr (local) {
         // block 0 stores the state the rest of the frame and the host read
         if (blockIdx.x == 0 && tid == 0 && v.step[0].active) {
             PoseDev* P = v.sess[0].pose;
@@ -716,11 +716,10 @@ __global__ void __launch_bounds__(kIcpThreads, 1) icp_kernel(EngineView v) {
             P->status = loc.status;
             icp_finish(&v.sess[0], v.step[0], v.out);
         }
-        return;
+    } else {
+        for (int s = blockIdx.x; s < S_cap; s += gridDim.x)
+            if (tid == 0) icp_finish(&v.sess[s], v.step[s], v.out + s);
     }
-
-    for (int s = blockIdx.x; s < S_cap; s += gridDim.x)
-        if (tid == 0) icp_finish(&v.sess[s], v.step[s], v.out + s);
 }
 
 int icp_max_grid(int num_sms) { return num_sms; }
