@@ -563,6 +563,13 @@ def run_served(kf, torch, seconds, seed=11):
     stats = srv.stats()
     srv.close()
     wall = (kf.Server.now_ms() - t0) / 1000.0
+    # four of the schedule's sessions (both resolutions, different volumes) served together
+    # with frames arriving unevenly, against each run alone through a plain session
+    pick = []
+    for sz in (0, 1):
+        pick += [i for i in range(nsess) if int(sizes[i]) == sz][:2]
+    check = served_vs_alone(kf, [cfg_of(i) for i in pick], [seqs[(int(sizes[i]), i % 4)][:8] for i in pick])
+    progress("served: check against sessions alone done")
     return {"workload": "64 sessions over %.0f s (C5 scaled by %.2f): lifetimes U(5,30) s x %.2f, 30 fps Poisson "
                         "arrivals, 50/50 320x240 / 640x480, volumes {128,256,384,512}^3 f16+u16, 150 GB budget"
                         % (seconds, scale, scale),
@@ -572,7 +579,42 @@ def run_served(kf, torch, seconds, seed=11):
             "admitted": int(stats["sessions_admitted"]), "refused_at_open": int(stats["sessions_refused"]),
             "never_admitted": int(nsess - stats["sessions_admitted"]),
             "max_active": int(stats["max_active_sessions"]),
-            "latency": "arrival of the frame (client queueing included) to result ready"}
+            "latency": "arrival of the frame (client queueing included) to result ready",
+            "vs_alone": check}
+
+
+def served_vs_alone(kf, cfgs, frames):
+    """Serve the sessions together, a different subset of them stepping each time, then run each
+    alone through a plain session: the largest pose difference per frame and whether the final
+    raycast maps are equal."""
+    srv = kf.Server(8, 150 * 10 ** 9)
+    ids = [srv.open(c) for c in cfgs]
+    n = len(cfgs)
+    nf = min(len(f) for f in frames)
+    pending, got = [0] * n, [[] for _ in range(n)]
+    k = 0
+    while min(pending) < nf:
+        batch = [j for j in range(n) if pending[j] < nf and (k + j) % 3 != 0] or \
+                [j for j in range(n) if pending[j] < nf]
+        for j in batch:
+            srv.submit(ids[j], frames[j][pending[j]])
+        srv.step()
+        for j in batch:
+            got[j].append(srv.result(ids[j])[0])
+            pending[j] += 1
+        k += 1
+    served_maps = [srv.session(ids[j]).raycast_maps(0) for j in range(n)]
+    srv.close()
+    worst, maps_equal = 0.0, True
+    for j, c in enumerate(cfgs):
+        s = kf.KinectFusion(c)
+        for f in range(nf):
+            worst = max(worst, float(np.max(np.abs(s.process_frame(frames[j][f])[1] - got[j][f]))))
+        v, nm = s.raycast_maps(0)
+        maps_equal = maps_equal and bool(np.array_equal(v, served_maps[j][0]) and np.array_equal(nm, served_maps[j][1]))
+        s.close()
+    return {"sessions": n, "frames_each": nf, "max_pose_abs_diff": worst, "raycast_maps_equal": maps_equal,
+            "method": "served together with uneven arrivals vs each session alone, same frames"}
 
 
 # ---------------------------------------------------------------------------------------------
