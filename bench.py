@@ -280,7 +280,9 @@ def stage_rooflines(cfg, ab, stage_ms, peak, icp_iters, traffic, fps):
         ms = float(ms)
         gbs = b / (ms / 1000.0) / 1e9 if ms > 0 else None
         out[k] = {"ms": round(float(ms), 5), "algorithmic_bytes": int(b), "achieved_gbs": round(gbs, 1) if gbs else None,
-                  "frac": round(gbs / peak, 4) if gbs else None, "dram_bytes_ncu": traffic.get(k), "bytes": note}
+                  "frac": round(gbs / peak, 4) if gbs else None,
+                  "frac_of_nominal_8tbs": round(gbs / 8000.0, 4) if gbs else None,
+                  "dram_bytes_ncu": traffic.get(k), "bytes": note}
     fuse_s = stage_ms[3] / 1000.0
     out["fuse"]["updated_bytes"] = int(ab["fuse_updated"])
     out["fuse"]["updated_gbs"] = round(ab["fuse_updated"] / fuse_s / 1e9, 1) if fuse_s > 0 else None
