@@ -16,7 +16,7 @@
 //     reference never returns to large steps); super-bricks let them cross free space 94 steps
 //     at a time.
 //   - Load balance: each warp pulls 8 x 4-ray tiles from an atomic counter, and a lane marches
-//     at most 32 iterations (64 in steps of many sessions); longer rays are queued with their
+//     at most 40 iterations (64 in steps of many sessions); longer rays are queued with their
 //     exact march state.
 //   - Long rays: a second kernel marches each queued ray with a whole warp, 32 consecutive
 //     samples per round, taking the first sample (in order) that changes the state.
@@ -28,7 +28,7 @@ namespace kf {
 constexpr int kMaxMarchSamples = 1 << 16;
 // loop iterations a lane marches before queueing the ray: a short budget keeps the tail of a
 // single session's frame short; steps of many sessions hand off fewer rays with a longer one
-constexpr int kSerialBudgetSingle = 32;
+constexpr int kSerialBudgetSingle = 40;
 constexpr int kSerialBudgetMany = 64;
 constexpr int kManyRayTiles = 25000;   // more ray tiles than this in a step: kSerialBudgetMany
 

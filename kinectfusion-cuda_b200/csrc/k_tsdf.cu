@@ -12,10 +12,9 @@
 //     under it, or every voxel more than mu behind the farthest valid depth under it -- then
 //     no voxel of it can update.  The surviving blocks (a few percent of a 512^3 volume) are
 //     appended to a queue with one atomic per warp.
-//   - fuse_kernel's persistent warps take queue entries a quarter block (16 rows) at a time
-//     and walk the rows four at a time with one voxel per lane along x, so every depth gather
-//     and volume access of the warp touches 32 consecutive voxels, and a lane reads and
-//     writes the volume only for voxels that update.
+//   - fuse_kernel's persistent warps take queue entries whole, or in halves or quarters when
+//     there are few, and walk the rows four at a time, each lane four consecutive voxels along
+//     x, so the warp reads and writes the volume as 16-byte vectors in 128-byte rows.
 // Each 8^3 brick keeps a lower bound of its distances (an atomic minimum of every value
 // fusion stores), and a small pass widens it to the 2 x 2 x 2 bricks a trilinear sample can
 // touch; the raycaster skips samples whose bound proves they cannot matter.
@@ -308,13 +307,23 @@ __global__ void __launch_bounds__(256) fuse_cull_kernel(EngineView v) {
 }
 
 constexpr int kFuseWarps = 8;
-constexpr int kFuseSplit = 4;    // queue entries are taken a quarter block (16 rows) at a time
+
+// Queue entries are taken whole (64 rows) when there are at least eight per warp of the grid
+// (a batch), in halves from four per warp, and in quarters below that (a single session's
+// frame), so every warp has work and few entries pay the per-entry set-up.  Which warp fuses
+// which rows changes no voxel's arithmetic.
+__device__ __forceinline__ int fuse_split(unsigned int blocks) {
+    const unsigned int warps = gridDim.x * kFuseWarps;
+    return blocks >= 8u * warps ? 1 : blocks >= 4u * warps ? 2 : 4;
+}
 
 __global__ void __launch_bounds__(256, 4) fuse_kernel(EngineView v) {
     __shared__ FuseCtx ctx[kFuseWarps];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int S_cap = v.tb->S;
-    const unsigned int items = min(__ldcg(&v.counters[4]), unsigned(v.fuseq_cap)) * kFuseSplit;
+    const unsigned int blocks = min(__ldcg(&v.counters[4]), unsigned(v.fuseq_cap));
+    const int split = fuse_split(blocks), rows = 64 / split;
+    const unsigned int items = blocks * unsigned(split);
     FuseCtx& c = ctx[warp];
     int cur_s = -1;
     while (true) {
@@ -322,8 +331,8 @@ __global__ void __launch_bounds__(256, 4) fuse_kernel(EngineView v) {
         if (lane == 0) i = atomicAdd(&v.counters[5], 1u);
         i = __shfl_sync(0xffffffffu, i, 0);
         if (i >= items) break;
-        const long long g = __ldcg(v.fuseq + i / kFuseSplit);
-        const int part = int(i % kFuseSplit);
+        const long long g = __ldcg(v.fuseq + i / unsigned(split));
+        const int part = int(i % unsigned(split));
         const int s = unit_session(v, g, S_cap);
         if (s != cur_s) {
             cur_s = s;
@@ -333,7 +342,7 @@ __global__ void __launch_bounds__(256, 4) fuse_kernel(EngineView v) {
         }
         int x0, j0, k0;
         unit_origin(c.n, int(g - __ldg(v.fuse_prefix + s)), x0, j0, k0);
-        fuse_rows(c, x0, j0, k0, part * (64 / kFuseSplit), (part + 1) * (64 / kFuseSplit), lane);
+        fuse_rows(c, x0, j0, k0, part * rows, (part + 1) * rows, lane);
     }
 }
 

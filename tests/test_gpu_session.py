@@ -110,7 +110,7 @@ def test_raycast_maps(kf, run_small):
 
 
 def test_pipeline_raycast_equals_serial_stage(kf, cuda):
-    """The pipeline's march (cell skipping, 32-iteration lane budget, long rays marched by a
+    """The pipeline's march (cell skipping, 40-iteration lane budget, long rays marched by a
     whole warp) takes the same samples as a plain serial march: compare with the stage
     raycast (no skipping, no hand-off) on the same volume and pose."""
     from kfb200 import synth
