@@ -269,3 +269,39 @@ def test_pipeline_frame0_fuses_only(orc, kf):
     assert P.last_fused() > 0
     st, _ = P.process_frame(frames[1])
     assert st == 0 and sum(P.iters()) > 0
+
+
+# ---- the fixture against the reference's test sources it was transcribed from ----
+
+REFERENCE_ROOT = os.environ.get("KF_REFERENCE_ROOT", "/root/reference")
+
+
+def _transcription():
+    import importlib.util
+    spec = importlib.util.spec_from_file_location(
+        "check_transcription", os.path.join(ROOT, "tests", "golden", "check_transcription.py"))
+    mod = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mod)
+    return mod
+
+
+def test_golden_transcription_matches_reference_sources():
+    """Every number of every fixture entry appears among the numeric literals of the test lines
+    it cites (runs where a reference checkout is present; KF_REFERENCE_ROOT points at one)."""
+    import pytest
+    if not os.path.isdir(os.path.join(REFERENCE_ROOT, "test")):
+        pytest.skip("no reference checkout on this machine")
+    assert _transcription().check(REFERENCE_ROOT) == []
+
+
+def test_golden_transcription_check_catches_a_changed_value():
+    """A planted transcription mistake (b of TestComputeAndFillB changed from -7 to -7.5) is
+    reported for that entry alone."""
+    import copy
+    import pytest
+    if not os.path.isdir(os.path.join(REFERENCE_ROOT, "test")):
+        pytest.skip("no reference checkout on this machine")
+    fx = copy.deepcopy(GOLDEN)
+    fx["fill_a_b"]["b"] = -7.5
+    bad = _transcription().check(REFERENCE_ROOT, fx)
+    assert [(k, m) for k, _, m in bad] == [("fill_a_b", [-7.5])]
