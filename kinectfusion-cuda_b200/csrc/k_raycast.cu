@@ -19,7 +19,8 @@
 //     at most 40 iterations (64 in steps of many sessions); longer rays are queued with their
 //     exact march state.
 //   - Long rays: a second kernel marches each queued ray with a whole warp, 32 consecutive
-//     samples per round, taking the first sample (in order) that changes the state.
+//     samples per round (64 after a round in which nothing changed), taking the first sample
+//     (in order) that changes the state.
 #include "kf_host.h"
 #include "kf_march.h"
 
@@ -230,48 +231,75 @@ __device__ int march_serial(const SessionDev* S, const RayGeo& g, const TF* f, R
 // The same loop for one ray, carried by all 32 lanes of a warp (every lane holds the same
 // g and st): each round lane k evaluates the sample k steps ahead (its t formed by k
 // sequential float additions, exactly the reference's positions), and the first sample that
-// changes the state -- a negative value, or below 0.99 during large steps -- is applied.
+// changes the state -- a negative value, or below 0.99 during large steps -- is applied.  A
+// round that follows a round without any such sample takes two sets, samples k and 32 + k
+// (such rays are in a long run of samples that change nothing, a grazing ray in small steps
+// for instance); the first event in sample order is applied all the same.
 template <class TF>
 __device__ void march_coop(const SessionDev* S, const RayGeo& g, const TF* f, RayState& st, int lane,
                            float& precise) {
     const float mu = S->mu, large = mu * S->step_l, small = mu * S->step_s;
     const unsigned int full = 0xffffffffu;
+    bool wide = false;   // the last round changed nothing
     while (st.t < st.far_d && st.guard < kMaxMarchSamples) {
         const float inc = st.small ? small : large;
         if (S->bdil) {
             float x, y, z;
             texel(g, st.t, x, y, z);
-            if (skip_cell(S, g, st, x, y, z, inc)) continue;   // every lane takes the same steps
+            if (skip_cell(S, g, st, x, y, z, inc)) {   // every lane takes the same steps
+                wide = false;
+                continue;
+            }
         }
-        float tk;
-        if (!add_k_times(st.t, inc, lane, tk)) {   // the same float as lane sequential additions
-            tk = st.t;
-            for (int q = 0; q < lane; ++q) tk += inc;
+        float tk[2], fk[2];
+        bool valid[2];
+#pragma unroll
+        for (int j = 0; j < 2; ++j) {
+            const int n = 32 * j + lane;   // sample n of the round, n sequential additions ahead
+            tk[j] = st.t;
+            valid[j] = false;
+            if (j == 0 || wide) {
+                if (!add_k_times(st.t, inc, n, tk[j]))   // the same float as n sequential additions
+                    for (int q = 0; q < n; ++q) tk[j] += inc;
+                valid[j] = tk[j] < st.far_d && st.guard + n < kMaxMarchSamples;
+            }
         }
-        const bool valid = tk < st.far_d && st.guard + lane < kMaxMarchSamples;
-        const float fk = valid ? sample_at(S, g, f, tk) : 0.0f;
-        const bool event = valid && (fk < 0.0f || (!st.small && fk < 0.99f));
-        const unsigned int evm = __ballot_sync(full, event);
-        const unsigned int valm = __ballot_sync(full, valid);
-        if (!evm) {
-            if (!valm) break;
-            const int last = 31 - __clz(valm);   // valid lanes form a prefix
-            const float tl = __shfl_sync(full, tk, last);
-            st.prev = __shfl_sync(full, fk, last);
+#pragma unroll
+        for (int j = 0; j < 2; ++j) fk[j] = valid[j] ? sample_at(S, g, f, tk[j]) : 0.0f;
+        unsigned int evm[2], valm[2];
+#pragma unroll
+        for (int j = 0; j < 2; ++j) {
+            evm[j] = __ballot_sync(full, valid[j] && (fk[j] < 0.0f || (!st.small && fk[j] < 0.99f)));
+            valm[j] = __ballot_sync(full, valid[j]);   // valid samples form a prefix in n
+        }
+        if (!evm[0] && !evm[1]) {
+            if (!valm[0]) break;
+            const int js = valm[1] ? 1 : 0;
+            const int last = 31 - __clz(js ? valm[1] : valm[0]);
+            const float tl = __shfl_sync(full, js ? tk[1] : tk[0], last);
+            st.prev = __shfl_sync(full, js ? fk[1] : fk[0], last);
             st.prev_t = tl;
             st.prev_known = 1;
-            st.guard += last + 1;
+            st.guard += 32 * js + last + 1;
             st.t = tl + inc;
+            wide = true;
             continue;
         }
-        const int e = __ffs(evm) - 1;
-        const float te = __shfl_sync(full, tk, e), fe = __shfl_sync(full, fk, e);
-        if (e > 0) {
-            st.prev = __shfl_sync(full, fk, e - 1);
-            st.prev_t = __shfl_sync(full, tk, e - 1);
+        wide = false;
+        const int js = evm[0] ? 0 : 1;
+        const float tj = js ? tk[1] : tk[0], fj = js ? fk[1] : fk[0];
+        const int e = __ffs(js ? evm[1] : evm[0]) - 1;
+        const float te = __shfl_sync(full, tj, e), fe = __shfl_sync(full, fj, e);
+        // the sample before the event: lane e - 1 of the same set, or the first set's last lane
+        const float tb = __shfl_sync(full, tj, max(e - 1, 0)), fb = __shfl_sync(full, fj, max(e - 1, 0));
+        const float tb0 = __shfl_sync(full, tk[0], 31), fb0 = __shfl_sync(full, fk[0], 31);
+        const int ne = 32 * js + e;
+        if (ne > 0) {
+            st.prev = e > 0 ? fb : fb0;
+            st.prev_t = e > 0 ? tb : tb0;
             st.prev_known = 1;
         }
-        st.guard += e + 1;
+        st.guard += ne + 1;
         if (fe < 0.0f) {
             if (te != st.near_d) {
                 if (!st.small) {
