@@ -367,6 +367,7 @@ kf_status grow(T*& ptr, int& cap, int need) {
     int nc = std::max(need, std::max(16, cap * 2));
     if (ptr) cudaFree(ptr);
     ptr = nullptr;
+    cap = 0;   // a failed allocation leaves an empty buffer, never a stale capacity
     KF_CK(cudaMalloc(&ptr, sizeof(T) * size_t(nc)));
     KF_CK(cudaMemset(ptr, 0, sizeof(T) * size_t(nc)));
     cap = nc;
