@@ -291,6 +291,21 @@ def test_compute_pose_vs_oracle(kf, orc, cuda, frames_small):
     assert a <= 1e-4 and d <= 1e-4
 
 
+def test_compute_pose_two_synthetic_frames_device(kf, orc, cuda):
+    """TestComputePose (test/icp_tests.cpp:233-326) through the C ABI, on two synthetic frames
+    in place of TUM fr1/xyz: a 0.15 rad / 0.32 m step of the loop trajectory, recovered within
+    the reference's bounds (angle of R (1,1,1)/sqrt(3) <= pi / 90, translation within 0.01 m
+    per axis).  The maps are the oracle's (test_oracle_golden.two_frame_case)."""
+    from kfb200 import synth
+    from test_oracle_golden import rotated_diagonal_angle, two_frame_case
+    cfg, true, vb, va, na = two_frame_case(kf, orc, synth.LOOP, 3, 10, 11)
+    st, est, _ = kf.ICP(cfg).computePose([dev(cuda, v) for v in vb], [dev(cuda, v) for v in va],
+                                         [dev(cuda, v) for v in na], np.eye(4, dtype=np.float32))
+    assert st == 0
+    assert rotated_diagonal_angle(true[:3, :3], est[:3, :3]) <= PI / 90.0
+    assert np.max(np.abs(true[:3, 3] - est[:3, 3])) <= 0.01
+
+
 def test_bounded_wait_times_out_and_context_survives(kf, cuda):
     st, waited = kf.selftest_bounded_wait(50)
     assert st == kf.KF_ERR_TIMEOUT
