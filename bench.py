@@ -197,7 +197,8 @@ def plain_config(world):
     """config of the plain full-size line (both arms print the same)."""
     return {"workload": "plain full size: 640x480, 512^3 f32+f32 TSDF over 3 m, mu 0.02 m, "
                         "ICP 4/5/10 coarse to fine, bilateral 4.5 px / 30 mm / 5x5",
-            "frames": "seeded synthetic loop (plane, 0.4 m sphere, 0.5 m box), one session per GPU",
+            "frames": "seeded synthetic 300-frame loop (plane, 0.4 m sphere, 0.5 m box; about 1.6 cm and "
+                      "0.4 degrees per frame), one session per GPU",
             "l2": "inputs larger than L2 (the 1 GiB volume is streamed every frame)",
             "parallelism": "replicas" if world > 1 else "single"}
 
@@ -317,8 +318,8 @@ def c4_configs(kf, seed=7):
 
 
 def session_frames(kf, cfgs, count, seed0, torch):
-    """Per-session seeded loop sequences (period `count`, so cyclic reuse is smooth), stacked
-    on the device."""
+    """Per-session seeded loop sequences (the first `count` frames of each session's 300-frame
+    loop; a whole loop closes, so cyclic reuse of 300 frames is smooth), stacked on the device."""
     from kfb200 import synth
     out = []
     for i, c in enumerate(cfgs):
@@ -409,7 +410,7 @@ def run_batched(kf, torch, steps, plain_fps):
     # out every step (closed loop: each frame's latency is its step's), against the plain
     # single-stream f32 pipeline
     sweep = []
-    nfr = 60
+    nfr = 300   # a whole loop: frames are reused cyclically
     base = kf.config_full(tsdf_format=kf.KF_TSDF_F16U16)
     seqs = session_frames(kf, [base] * 8, nfr, 200, torch)
     pins = []
@@ -454,6 +455,7 @@ def run_served(kf, torch, seconds, seed=11):
     rng = np.random.default_rng(seed)
     scale = seconds / 60.0
     nsess = 64
+    LOOP = synth.LOOP_FRAMES   # each session cycles through a whole (closed) loop
     sizes = rng.integers(0, 2, nsess)
     vols = rng.choice([128, 256, 384, 512], nsess)
     life = rng.uniform(5.0, 30.0, nsess) * scale
@@ -462,7 +464,7 @@ def run_served(kf, torch, seconds, seed=11):
     for sz in (0, 1):
         c = kf.config_small() if sz == 0 else kf.config_full()
         for q in range(4):
-            seqs[(sz, q)] = synth.sequence(c, 60, seed=300 + 10 * sz + q, kind=synth.LOOP)[0]
+            seqs[(sz, q)] = synth.sequence(c, LOOP, seed=300 + 10 * sz + q, kind=synth.LOOP)[0]
 
     def cfg_of(i):
         n = int(vols[i])
@@ -538,7 +540,7 @@ def run_served(kf, torch, seconds, seed=11):
                     if sid is None:
                         retry_at[i] = now + 50.0
                         continue
-                    state[i] = [sid, now, int(rng.integers(0, 60)), []]
+                    state[i] = [sid, now, int(rng.integers(0, LOOP)), []]
                 elif now >= start[i] * 1000.0 and now >= retry_at.get(i, 0.0):
                     opening[i] = admin.submit(srv.try_open, cfg_of(i))
                 continue
@@ -552,7 +554,7 @@ def run_served(kf, torch, seconds, seed=11):
                 st[3].append(st[1])
                 st[1] += float(rng.exponential(1000.0 / 30.0))
             if st[3]:
-                img = seqs[(int(sizes[i]), i % 4)][st[2] % 60]
+                img = seqs[(int(sizes[i]), i % 4)][st[2] % LOOP]
                 if srv.submit(st[0], img, t0 + st[3][0]) == kf.KF_OK:
                     st[3].pop(0)
                     st[2] += 1
@@ -573,7 +575,9 @@ def run_served(kf, torch, seconds, seed=11):
     check = served_vs_alone(kf, [cfg_of(i) for i in pick], [seqs[(int(sizes[i]), i % 4)][:8] for i in pick])
     progress("served: check against sessions alone done")
     return {"workload": "64 sessions over %.0f s (C5 scaled by %.2f): lifetimes U(5,30) s x %.2f, 30 fps Poisson "
-                        "arrivals, 50/50 320x240 / 640x480, volumes {128,256,384,512}^3 f16+u16, 150 GB budget"
+                        "arrivals, 50/50 320x240 / 640x480, volumes {128,256,384,512}^3 f16+u16, 150 GB budget; "
+                        "truncation mu = max(0.03 m at 320x240 / 0.02 m at 640x480, 2.5 voxels), since a band "
+                        "thinner than a voxel loses the surface in 128^3 over 3 m"
                         % (seconds, scale, scale),
             "value": round(stats["frames_done"] / wall, 2), "unit": "frames/s",
             "p50_ms": round(stats["p50_ms"], 3), "p99_ms": round(stats["p99_ms"], 3), "max_ms": round(stats["max_ms"], 3),
@@ -624,77 +628,116 @@ def served_vs_alone(kf, cfgs, frames):
 # ---------------------------------------------------------------------------------------------
 def synced_errors(kf, orc, cfg, imgs):
     """Per frame, the oracle (FP64) starts from the device's TSDF and pose, then both process
-    the frame.  Returns max pose error, TSDF RMS (truncation units, voxels both observed),
-    raycast depth error (mm, pixels where both hit) and ICP-mask agreement."""
+    the frame.  Returns the max pose error; the raycast depth error (mm, where both hit) as a
+    maximum over rays whose march took the same decisions (equal decision traces) and over all,
+    with the rays whose decisions flipped counted; each frame's fusion against the oracle fusing
+    it at the device's pose (max over touched voxels but boundary flips, oracle/parity.py); and
+    the TSDF RMS over voxels both observed."""
+    import parity
+    xs, zs = orc.voxel_axes(cfg.volume_n, cfg.volume_width)
     s = kf.KinectFusion(kf.KfConfig.from_buffer_copy(cfg))
+    s.set_debug(kf.KF_DEBUG_RAY_TRACE)
     P = orc.Pipeline(cfg, prec=1)
     worst_a = worst_d = same_a = same_d = 0.0
-    rms, ray_mm, ray_hit = [], [], []
+    rms = []
     flips = 0
+    ray = {"rays": 0, "trace_flips": 0, "both_hit_same_trace": 0, "over_1mm_flipped": 0}
+    ray_max_same = ray_max_all = 0.0
+    hit_agree = 1.0
+    fus = {"touched": 0, "boundary_flips": 0}
+    fus_max = fus_max_all = 0.0
     for k, img in enumerate(imgs):
-        f, w = s.tsdf()
-        P.set_tsdf(f, w)
+        f0, w0 = s.tsdf()
+        P.set_tsdf(f0, w0)
         P.set_pose(s.pose())
         cam = s.pose()[:3, 3].astype(np.float64)
         P.process_frame(img)
         s.process_frame(img)
-        a, d = kf.poseError(P.pose(), s.pose())
+        pose_g = s.pose()
+        a, d = kf.poseError(P.pose(), pose_g)
         worst_a, worst_d = max(worst_a, a), max(worst_d, d)
         if list(P.iters()) == list(s.frame_stats()["icp_iters"]):
             same_a, same_d = max(same_a, a), max(same_d, d)
         else:
             flips += 1   # the 0.1 deg / 1 cm early stop decided differently: one more or fewer pass
+        gf, gw = s.tsdf()
+        fo, wo = f0.copy(), w0.copy()
+        depth_m = orc.convert(img, cfg.depth_scale)
+        orc.fuse(depth_m, kf.level_intrinsics(cfg, 0), fo, wo, cfg.volume_width, cfg.mu, pose_g, prec=1)
+        t = parity.tsdf_frame_parity(cfg, f0, w0, gf, gw, fo, wo, pose_g, depth_m, xs, zs)
+        fus["touched"] += t["touched"]
+        fus["boundary_flips"] += t["boundary_flips"]
+        fus_max, fus_max_all = max(fus_max, t["max_nonflip"]), max(fus_max_all, t["max_all"])
+        del f0, w0, fo, wo
         if k == 0:
             continue
-        gf, gw = s.tsdf()
         of, ow = P.tsdf()
         both = (gw > 0) & (ow > 0)
         rms.append(float(np.sqrt(np.mean((gf[both].astype(np.float64) - of[both]) ** 2))))
-        gv, _ = s.raycast_maps(0)
-        ov, _ = P.raycast_maps(0)
-        gh, oh = gv[..., 3] == -1, ov[..., 3] == -1
-        ray_hit.append(float(np.mean(gh == oh)))
-        m = gh & oh
-        if m.any():
-            dz = np.abs(np.linalg.norm(gv[m][:, :3] - cam, axis=1) - np.linalg.norm(ov[m][:, :3] - cam, axis=1))
-            ray_mm.append(dz * 1000.0)
+        del gf, gw, of, ow, both
+        for level in range(cfg.levels):
+            r = parity.raycast_parity(s.raycast_maps(level)[0], P.raycast_maps(level)[0], s.ray_trace(level),
+                                      P.ray_trace(level), cam)
+            for key in ray:
+                ray[key] += r[key]
+            ray_max_same = max(ray_max_same, r["max_mm_same_trace"])
+            ray_max_all = max(ray_max_all, r["max_mm_all"])
+            hit_agree = min(hit_agree, r["hit_agreement"])
     s.close()
     P.close()
-    mm = np.concatenate(ray_mm) if ray_mm else np.zeros(1)
     return {"frames": len(imgs), "pose_rad_max": float(worst_a), "pose_m_max": float(worst_d),
             "frames_icp_iterations_differ": flips,
             "pose_rad_max_same_iterations": float(same_a), "pose_m_max_same_iterations": float(same_d),
-            "tsdf_rms_trunc_max": float(max(rms)) if rms else None,
-            "raycast_mm_max": round(float(mm.max()), 4), "raycast_mm_p999": round(float(np.quantile(mm, 0.999)), 4),
-            "raycast_hit_agreement_min": round(float(min(ray_hit)), 5) if ray_hit else None}
+            "raycast_mm_max_same_decisions": round(ray_max_same, 5), "raycast_mm_max_all": round(ray_max_all, 4),
+            "raycast_rays": ray["rays"], "raycast_decision_flips": ray["trace_flips"],
+            "raycast_over_1mm_all_flipped": ray["over_1mm_flipped"],
+            "raycast_hit_agreement_min": round(hit_agree, 6),
+            "fusion_trunc_max_nonflip": fus_max, "fusion_trunc_max_all": fus_max_all,
+            "fusion_voxels_touched": fus["touched"], "fusion_boundary_flips": fus["boundary_flips"],
+            "tsdf_rms_trunc_max": float(max(rms)) if rms else None}
 
 
-def drift(kf, orc, cfg, imgs):
-    """Free-running: device and FP64 oracle each track the whole sequence; final pose error."""
+def drift(kf, orc, cfg, imgs, gt):
+    """Free-running: device and FP64 oracle each track the whole sequence.  Final pose error
+    between them, and each one's error against the synthetic ground truth (relative to the
+    first frame, whose pose both take as given)."""
     s = kf.KinectFusion(kf.KfConfig.from_buffer_copy(cfg))
     P = orc.Pipeline(cfg, prec=1)
     for img in imgs:
         s.process_frame(img)
         P.process_frame(img)
     a, d = kf.poseError(P.pose(), s.pose())
+    # ground truth in the tracker's world frame: the start pose composed with the motion since frame 0
+    start = kf.start_pose(cfg.volume_width).astype(np.float64)
+    g0 = np.asarray(gt[0], np.float64)
+    truth = (start @ np.linalg.inv(g0) @ np.asarray(gt[len(imgs) - 1], np.float64)).astype(np.float32)
+    ag, dg = kf.poseError(truth, s.pose())
+    ao, do = kf.poseError(truth, P.pose())
     s.close()
     P.close()
-    return {"frames": len(imgs), "pose_rad": float(a), "pose_m": float(d)}
+    return {"frames": len(imgs), "pose_rad": float(a), "pose_m": float(d),
+            "device_vs_truth_rad": float(ag), "device_vs_truth_m": float(dg),
+            "oracle_vs_truth_rad": float(ao), "oracle_vs_truth_m": float(do)}
 
 
-def run_accuracy(kf, full_frames=6, small_frames=30, drift_frames=150):
+def run_accuracy(kf, full_frames=6, small_frames=30, drift_frames=150, full_drift_frames=30):
     import oracle as orc
     from kfb200 import synth
-    out = {"reference": "FP64 CPU restatement (oracle/kf_oracle.cpp), synced per frame from the device state"}
+    out = {"reference": "FP64 CPU restatement (oracle/kf_oracle.cpp), synced per frame from the device state",
+           "frames": "small: seeded wobble; full: the start of the 300-frame seeded loop (about 1.6 cm per frame)"}
     small = kf.config_small()
-    imgs, _ = synth.sequence(small, max(small_frames, drift_frames), seed=61)
+    imgs, gts = synth.sequence(small, max(small_frames, drift_frames), seed=61)
     out["small_f32"] = synced_errors(kf, orc, small, imgs[:small_frames])
     s16 = kf.config_small(tsdf_format=kf.KF_TSDF_F16U16)
     out["small_f16u16"] = synced_errors(kf, orc, s16, imgs[:small_frames])
-    out["small_f16u16_drift"] = drift(kf, orc, s16, imgs[:drift_frames])
-    full = kf.config_full(tsdf_format=kf.KF_TSDF_F16U16)
-    fimgs, _ = synth.sequence(full, full_frames, seed=63, kind=synth.LOOP)
-    out["full_f16u16"] = synced_errors(kf, orc, full, fimgs)
+    out["small_f16u16_drift"] = drift(kf, orc, s16, imgs[:drift_frames], gts)
+    full = kf.config_full()
+    fimgs, fgts = synth.sequence(full, max(full_frames, full_drift_frames), seed=63, kind=synth.LOOP)
+    out["full_f32"] = synced_errors(kf, orc, full, fimgs[:full_frames])
+    f16 = kf.config_full(tsdf_format=kf.KF_TSDF_F16U16)
+    out["full_f16u16"] = synced_errors(kf, orc, f16, fimgs[:full_frames])
+    if full_drift_frames > 0:
+        out["full_f16u16_drift"] = drift(kf, orc, f16, fimgs[:full_drift_frames], fgts)
     return out
 
 
@@ -763,22 +806,23 @@ def run_ours(args, world, rank, local):
     stage_ms = acc / nprof
     s.set_profiling(False)
 
-    # e2e through the public API: pinned host frames in, pose + statistics out, every step
-    npin = min(steps, 64)   # pinned frames reused cyclically along the loop
-    pinned = torch.empty((npin,) + imgs[0].shape, dtype=torch.int16, pin_memory=True)
-    for i in range(npin):
-        pinned[i].copy_(torch.from_numpy(imgs[i % nimg].view(np.int16)))
+    # e2e through the public API: pinned host frames in, pose + statistics out, every step; a
+    # fresh session takes the same frames in the same order as the device-resident loop above
+    pinned = torch.empty((nimg,) + imgs[0].shape, dtype=torch.int16, pin_memory=True)
+    for i in range(nimg):
+        pinned[i].copy_(torch.from_numpy(imgs[i].view(np.int16)))
     host_frames = pinned.numpy().view(np.uint16)
     s2 = kf.KinectFusion(cfg)
+    s2.process_frame(host_frames[0])
     for i in range(warmup):
-        s2.process_frame(host_frames[i % npin])
+        s2.process_frame(host_frames[(1 + i) % nimg])
     barrier()
     torch.cuda.synchronize()
     lat = np.zeros(steps)
     t0 = time.perf_counter()
     for i in range(steps):
         t1 = time.perf_counter()
-        s2.process_frame(host_frames[(warmup + i) % npin])
+        s2.process_frame(host_frames[(1 + warmup + i) % nimg])
         lat[i] = time.perf_counter() - t1
     torch.cuda.synchronize()
     e2e_s = max_over_ranks(time.perf_counter() - t0)

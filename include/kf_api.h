@@ -384,6 +384,19 @@ kf_status kf_session_set_profiling(kf_session* s, int on);
 /* Device durations (ms) of the last completed step: preprocess, raycast, ICP, fusion.  The
  * preprocess runs on a graph branch beside the raycast, so the raycast figure spans both. */
 kf_status kf_session_stage_times(kf_session* s, float ms[4]);
+/* Debug modes of a session (flags, 0 = off).  KF_DEBUG_RAY_TRACE makes every raycast record,
+ * per pixel, the decisions its march took: how many samples it took before leaving large steps
+ * and how (a sample below 0.99, or a negative one that backs off by mu), how many it took in
+ * all and how it ended (bits 40.., 8..39, 4..5 and 0..1 of a uint64; 0 for a ray that never
+ * marched).  Two implementations of the reference's march (project/src/raycast.cu:75-117) that
+ * give a pixel the same trace took the same samples in the same order, so their hits can only
+ * differ by arithmetic rounding; a different trace means a sample near 0.99 or 0 decided
+ * otherwise.  No counterpart in the reference (a parity aid). */
+#define KF_DEBUG_RAY_TRACE 1
+kf_status kf_session_set_debug(kf_session* s, int flags);
+/* The traces of the last raycast at `level` (w * h uint64; host memory when to_host = 1).
+ * KF_ERR_STATE unless KF_DEBUG_RAY_TRACE is on. */
+kf_status kf_get_ray_trace(kf_session* s, int level, uint64_t* dst, int to_host);
 kf_status kf_batch_set_profiling(kf_batch* b, int on);
 kf_status kf_batch_stage_times(kf_batch* b, float ms[4]);
 /* Self-test of the bounded device-side waits: a cooperative launch whose barrier is never

@@ -58,7 +58,7 @@ def build(verbose=False, ptxas_info=False):
     os.makedirs(LIB, exist_ok=True)
     os.makedirs(OBJ, exist_ok=True)
     nvcc = _nvcc()
-    headers = [os.path.join(CSRC, h) for h in ("kf_device.cuh", "kf_host.h", "kf_march.h")] + \
+    headers = [os.path.join(CSRC, h) for h in ("kf_device.cuh", "kf_host.h")] + \
         [os.path.join(REPO, "include", "kf_api.h")]
     extra = ["-Xptxas", "-v"] if ptxas_info else []
     objs = []

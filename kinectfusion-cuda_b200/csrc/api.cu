@@ -1425,27 +1425,39 @@ kf_status kf_construct_icp_residuals(const float* vertex, const float* target_ve
 }
 
 // scratch of kf_solve_linear_least_squares: block partials + the FP64 solution, kept per
-// process and grown on demand
-static std::mutex g_lls_mu;
-static float* g_lls_partials = nullptr;
-static int g_lls_cap = 0;
-static double* g_lls_x = nullptr;
+// process and per device ordinal (a call finds the scratch of the device current at the
+// call), grown on demand
+namespace {
+constexpr int kLlsMaxDevices = 64;
+struct LlsScratch {
+    float* partials = nullptr;
+    int cap = 0;
+    double* x = nullptr;
+};
+std::mutex g_lls_mu;
+LlsScratch g_lls[kLlsMaxDevices];
+}  // namespace
 
 kf_status kf_solve_linear_least_squares(const float* mat_a, const float* vec_b, int n, float x_out[6], void* stream) {
     if (!mat_a || !vec_b || !x_out || n <= 0) return KF_ERR_ARG;
+    int dev = -1;
+    KF_CK(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= kLlsMaxDevices) return KF_ERR_ARG;
     std::lock_guard<std::mutex> lk(g_lls_mu);
+    LlsScratch& sc = g_lls[dev];
     const int nb = lls_num_blocks(n);
-    if (nb > g_lls_cap || !g_lls_partials) {
-        if (g_lls_partials) cudaFree(g_lls_partials);
-        g_lls_partials = nullptr;
-        KF_CK(cudaMalloc(&g_lls_partials, sizeof(float) * 54 * size_t(nb)));
-        g_lls_cap = nb;
+    if (nb > sc.cap || !sc.partials) {
+        if (sc.partials) cudaFree(sc.partials);
+        sc.partials = nullptr;
+        sc.cap = 0;
+        KF_CK(cudaMalloc(&sc.partials, sizeof(float) * 54 * size_t(nb)));
+        sc.cap = nb;
     }
-    if (!g_lls_x) KF_CK(cudaMalloc(&g_lls_x, sizeof(double) * 6));
+    if (!sc.x) KF_CK(cudaMalloc(&sc.x, sizeof(double) * 6));
     cudaStream_t st = as_stream(stream);
-    KF_CK(stage_lls(mat_a, vec_b, n, g_lls_partials, g_lls_x, nb, st));
+    KF_CK(stage_lls(mat_a, vec_b, n, sc.partials, sc.x, nb, st));
     double x[6];
-    KF_CK(cudaMemcpyAsync(x, g_lls_x, sizeof(x), cudaMemcpyDeviceToHost, st));
+    KF_CK(cudaMemcpyAsync(x, sc.x, sizeof(x), cudaMemcpyDeviceToHost, st));
     KF_CK(cudaStreamSynchronize(st));
     for (int q = 0; q < 6; ++q) x_out[q] = float(x[q]);
     for (int q = 0; q < 6; ++q)
@@ -2113,6 +2125,37 @@ kf_status kf_session_set_profiling(kf_session* s, int on) {
 kf_status kf_session_stage_times(kf_session* s, float ms[4]) {
     if (!s || !ms) return KF_ERR_ARG;
     return s->eng->stage_times(ms);
+}
+
+kf_status kf_session_set_debug(kf_session* s, int flags) {
+    if (!s || (flags & ~KF_DEBUG_RAY_TRACE)) return KF_ERR_ARG;
+    Slot& sl = s->sl();
+    if (sl.external) return KF_ERR_STATE;
+    KF_CK(cudaDeviceSynchronize());
+    const bool want = (flags & KF_DEBUG_RAY_TRACE) != 0;
+    for (int l = 0; l < sl.cfg.levels; ++l) {
+        if (want && !sl.d.trace[l]) {
+            void* p = nullptr;
+            const size_t bytes = level_px(sl.cfg, l) * sizeof(unsigned long long);
+            KF_CK(cudaMalloc(&p, bytes));
+            sl.allocs.push_back(p);
+            KF_CK(cudaMemset(p, 0, bytes));
+            sl.d.trace[l] = static_cast<unsigned long long*>(p);
+        } else if (!want && sl.d.trace[l]) {
+            // the buffer stays with the slot (freed with it); the kernels stop writing it
+            sl.d.trace[l] = nullptr;
+        }
+    }
+    s->eng->tables_dirty = true;   // the session record on the device carries the pointers
+    return KF_OK;
+}
+
+kf_status kf_get_ray_trace(kf_session* s, int level, uint64_t* dst, int to_host) {
+    if (!s || !dst) return KF_ERR_ARG;
+    const Slot& sl = s->sl();
+    if (level < 0 || level >= sl.cfg.levels) return KF_ERR_ARG;
+    if (!sl.d.trace[level]) return KF_ERR_STATE;
+    return copy_out(dst, sl.d.trace[level], level_px(sl.cfg, level) * sizeof(uint64_t), to_host);
 }
 
 kf_status kf_batch_set_profiling(kf_batch* b, int on) {

@@ -5,13 +5,18 @@
 // (project/src/kinect_fusion.cpp:137-144).  The reference samples a cudaArray through the
 // texture unit; here the distance array stays in linear HBM (x fastest), so fusion can stream
 // it, and the march does its own trilinear interpolation with the reference's texel mapping
-// (uvw * n - 0.5, clamp).  Every sample the reference takes is taken at the same float
-// position, in the same order; three things make that fast:
+// (uvw * n - 0.5, clamp).  The march takes the reference's samples in the reference's order,
+// with one difference in arithmetic: the reference forms each position by adding the step to
+// the last one (t <- t + inc, project/src/raycast.cu:78), so float rounding drifts along a ray
+// (up to ~1e-4 m over a grazing ray of a thousand small steps, which moves its hit by up to a
+// millimetre); here sample k of a phase is at base + k * inc with a single rounding, where base
+// is the near distance, the sample that left large steps, or t - mu after a back-off.  That is
+// the FP64 march's position to within a rounding, and any sample's position is known without
+// the ones before it.  Three things make the march fast:
 //   - Skipping: a sample whose eight taps lie in cells (32^3 super-bricks, then 8^3 bricks)
 //     whose distance lower bound proves it cannot change the march (>= 0.991 during large
 //     steps, >= 0.001 during small steps) is not evaluated, nor is any later sample in the
-//     same cell; t still lands on the reference's repeated float additions (the first eight
-//     one by one, longer runs in closed form within each binade, kf_march.h).  Rays that pass
+//     same cell; the march jumps to the first sample index past the cell.  Rays that pass
 //     within mu of a surface without crossing it keep 0.1 mu steps to the far plane (the
 //     reference never returns to large steps); super-bricks let them cross free space 94 steps
 //     at a time.
@@ -22,7 +27,6 @@
 //     samples per round (64 after a round in which nothing changed), taking the first sample
 //     (in order) that changes the state.
 #include "kf_host.h"
-#include "kf_march.h"
 
 namespace kf {
 
@@ -45,11 +49,42 @@ struct RayGeo {
 
 // march state: everything the reference's loop carries from one sample to the next
 struct RayState {
-    float t, prev, prev_t, near_d, far_d;
+    float t;          // position of the next sample: base + idx * inc, one rounding
+    float base;       // start of the current phase of the march
+    float prev, prev_t, near_d, far_d;
+    int idx;          // index of the next sample within the phase
     int small;        // 0 while stepping by 1.99 mu, 1 once stepping by 0.1 mu
     int prev_known;   // 0 when the last non-negative sample was skipped (value not computed)
     int guard;        // samples taken (hard bound)
+    int sw;           // (samples taken when large steps ended) << 2 | how: 1 below 0.99, 2 negative
 };
+
+// position of sample k of the phase that starts at base
+__device__ __forceinline__ float march_pos(float base, int k, float inc) { return __fmaf_rn(float(k), inc, base); }
+
+// enter small steps: the next sample is base + inc (the sample that left large steps, or
+// t - mu after a back-off, is the new base)
+__device__ __forceinline__ void begin_small(RayState& st, float base, float small) {
+    st.small = 1;
+    st.base = base;
+    st.idx = 1;
+    st.t = march_pos(base, 1, small);
+}
+
+// The march's decision trace of one ray (written only in debug mode), so that a test can tell
+// rays whose march took the same decisions as another implementation's from rays where a sample
+// near 0.99 or 0 decided differently:
+//   bits 40..  samples taken when the march left large steps (0: it never did)
+//   bits  8..39 samples taken when the march ended (skipped samples count as taken)
+//   bits  4..5  how it left large steps: 1 a sample in [0, 0.99), 2 a negative one (back-off)
+//   bits  0..1  how it ended: 0 past the far plane or the sample bound, 1 negative first
+//               sample, 2 refined hit
+// A ray that returns before marching has trace 0.
+__device__ __forceinline__ unsigned long long ray_trace_code(const RayState& st, float precise) {
+    const int end = precise != 0.0f ? 2 : (st.t < st.far_d && st.guard < kMaxMarchSamples ? 1 : 0);
+    return (static_cast<unsigned long long>(st.sw >> 2) << 40) | (static_cast<unsigned long long>(st.guard) << 8) |
+           static_cast<unsigned long long>((st.sw & 3) << 4) | static_cast<unsigned long long>(end);
+}
 
 // a ray handed from a lane to a warp: where it is, its exact march state and its geometry (so
 // the warp neither reloads the pose nor divides again)
@@ -117,6 +152,8 @@ __device__ __forceinline__ bool ray_start(const SessionDev* S, const RayGeo& g, 
     const float near_d = fmaxf(S->min_d, tmin), far_d = fminf(S->max_d, tmax);
     if (near_d >= far_d) return false;
     st.t = near_d;
+    st.base = near_d;
+    st.idx = 0;
     st.near_d = near_d;
     st.far_d = far_d;
     st.prev = 0.f;
@@ -124,6 +161,7 @@ __device__ __forceinline__ bool ray_start(const SessionDev* S, const RayGeo& g, 
     st.small = 0;
     st.prev_known = 1;
     st.guard = 0;
+    st.sw = 0;
     return true;
 }
 
@@ -141,14 +179,11 @@ __device__ __forceinline__ float box_exit(const RayGeo& g, int n, int lox, int h
     return t;
 }
 
-// The reference's march loop for one lane (project/src/raycast.cu:75-117).  Returns 1 when
-// the ray is finished (precise = refined hit distance, 0 for none) and 0 when `budget`
-// iterations ran out with the ray still marching (state kept in st).
 // Samples whose base voxel lies in a cell whose distance lower bound is at or above the
 // current threshold (0.991 during large steps, 0.001 during small steps) cannot change the
 // march.  If the sample at st.t is such a sample, advance st past every following sample in the
-// same cell -- its 32^3 super-brick when that one qualifies, else its 8^3 brick -- by the
-// reference's own float additions, and return true.
+// same cell -- its 32^3 super-brick when that one qualifies, else its 8^3 brick -- to the first
+// sample index whose position is at or past the cell's exit, and return true.
 __device__ __forceinline__ bool skip_cell(const SessionDev* S, const RayGeo& g, RayState& st, float x, float y, float z,
                                           float inc) {
     const int n = S->n;
@@ -169,23 +204,27 @@ __device__ __forceinline__ bool skip_cell(const SessionDev* S, const RayGeo& g, 
         lo[0] = bx * 8; lo[1] = by * 8; lo[2] = bz * 8;
         hi[0] = lo[0] + 8; hi[1] = lo[1] + 8; hi[2] = lo[2] + 8;
     }
-    // skip this sample and every later one whose base voxel stays in the box
-    const float t_safe = box_exit(g, n, lo[0], hi[0], lo[1], hi[1], lo[2], hi[2], st.far_d);
-    // first steps one by one (most skips are short), the rest in closed form
-    const float lim = fminf(t_safe, st.far_d);
-    int k = 0;
-    do {
-        st.prev_t = st.t;
-        st.t += inc;
-        ++st.guard;
-        ++k;
-    } while (st.t < lim && st.guard < kMaxMarchSamples && k < 8);
-    if (st.t < lim && st.guard < kMaxMarchSamples)
-        st.guard += advance_steps(st.t, st.prev_t, inc, lim, kMaxMarchSamples - st.guard);
+    // skip this sample and every later one whose base voxel stays in the box: the next sample
+    // is the first index k > idx with base + k inc >= lim (positions increase with k), or the
+    // last index the sample bound allows
+    const float lim = fminf(box_exit(g, n, lo[0], hi[0], lo[1], hi[1], lo[2], hi[2], st.far_d), st.far_d);
+    const int k_lo = st.idx + 1, k_hi = st.idx + (kMaxMarchSamples - st.guard);
+    int k = k_lo;
+    const float est = __fdividef(lim - st.base, inc);   // within an index or two of the answer
+    if (est > float(k_lo)) k = int(fminf(est, float(k_hi)));
+    while (k > k_lo && !(march_pos(st.base, k - 1, inc) < lim)) --k;
+    while (k < k_hi && march_pos(st.base, k, inc) < lim) ++k;
+    st.guard += k - st.idx;
+    st.idx = k;
+    st.prev_t = march_pos(st.base, k - 1, inc);
+    st.t = march_pos(st.base, k, inc);
     st.prev_known = 0;
     return true;
 }
 
+// The reference's march loop for one lane (project/src/raycast.cu:75-117).  Returns 1 when
+// the ray is finished (precise = refined hit distance, 0 for none) and 0 when `budget`
+// iterations ran out with the ray still marching (state kept in st).
 template <class TF>
 __device__ int march_serial(const SessionDev* S, const RayGeo& g, const TF* f, RayState& st, int budget,
                             float& precise) {
@@ -203,10 +242,9 @@ __device__ int march_serial(const SessionDev* S, const RayGeo& g, const TF* f, R
         ++st.guard;
         if (tsdf < 0.0f) {
             if (st.t != st.near_d) {
-                if (!st.small) {   // went through the surface with a large step: back off
-                    st.t -= mu;
-                    st.small = 1;
-                    st.t += small;
+                if (!st.small) {   // went through the surface with a large step: back off by mu
+                    st.sw = (st.guard << 2) | 2;
+                    begin_small(st, __fsub_rn(st.t, mu), small);
                     continue;
                 }
                 if (!st.prev_known) {
@@ -217,22 +255,25 @@ __device__ int march_serial(const SessionDev* S, const RayGeo& g, const TF* f, R
                 precise = st.t - small * st.prev / (tsdf - st.prev);   // the reference's formula
             }
             return 1;
-        } else if (tsdf < 0.99f) {
-            st.small = 1;
         }
         st.prev = tsdf;
         st.prev_known = 1;
         st.prev_t = st.t;
-        st.t += st.small ? small : large;
+        if (!st.small && tsdf < 0.99f) {   // the region of uncertainty: small steps from here
+            st.sw = (st.guard << 2) | 1;
+            begin_small(st, st.t, small);
+        } else {
+            ++st.idx;
+            st.t = march_pos(st.base, st.idx, inc);
+        }
     }
     return 1;
 }
 
 // The same loop for one ray, carried by all 32 lanes of a warp (every lane holds the same
-// g and st): each round lane k evaluates the sample k steps ahead (its t formed by k
-// sequential float additions, exactly the reference's positions), and the first sample that
-// changes the state -- a negative value, or below 0.99 during large steps -- is applied.  A
-// round that follows a round without any such sample takes two sets, samples k and 32 + k
+// g and st): each round lane k evaluates the sample k indices ahead, and the first sample
+// that changes the state -- a negative value, or below 0.99 during large steps -- is applied.
+// A round that follows a round without any such sample takes two sets, samples k and 32 + k
 // (such rays are in a long run of samples that change nothing, a grazing ray in small steps
 // for instance); the first event in sample order is applied all the same.
 template <class TF>
@@ -255,14 +296,9 @@ __device__ void march_coop(const SessionDev* S, const RayGeo& g, const TF* f, Ra
         bool valid[2];
 #pragma unroll
         for (int j = 0; j < 2; ++j) {
-            const int n = 32 * j + lane;   // sample n of the round, n sequential additions ahead
-            tk[j] = st.t;
-            valid[j] = false;
-            if (j == 0 || wide) {
-                if (!add_k_times(st.t, inc, n, tk[j]))   // the same float as n sequential additions
-                    for (int q = 0; q < n; ++q) tk[j] += inc;
-                valid[j] = tk[j] < st.far_d && st.guard + n < kMaxMarchSamples;
-            }
+            const int n = 32 * j + lane;   // sample n of the round
+            tk[j] = march_pos(st.base, st.idx + n, inc);
+            valid[j] = (j == 0 || wide) && tk[j] < st.far_d && st.guard + n < kMaxMarchSamples;
         }
 #pragma unroll
         for (int j = 0; j < 2; ++j) fk[j] = valid[j] ? sample_at(S, g, f, tk[j]) : 0.0f;
@@ -276,12 +312,12 @@ __device__ void march_coop(const SessionDev* S, const RayGeo& g, const TF* f, Ra
             if (!valm[0]) break;
             const int js = valm[1] ? 1 : 0;
             const int last = 31 - __clz(js ? valm[1] : valm[0]);
-            const float tl = __shfl_sync(full, js ? tk[1] : tk[0], last);
             st.prev = __shfl_sync(full, js ? fk[1] : fk[0], last);
-            st.prev_t = tl;
+            st.prev_t = __shfl_sync(full, js ? tk[1] : tk[0], last);
             st.prev_known = 1;
             st.guard += 32 * js + last + 1;
-            st.t = tl + inc;
+            st.idx += 32 * js + last + 1;
+            st.t = march_pos(st.base, st.idx, inc);
             wide = true;
             continue;
         }
@@ -303,9 +339,8 @@ __device__ void march_coop(const SessionDev* S, const RayGeo& g, const TF* f, Ra
         if (fe < 0.0f) {
             if (te != st.near_d) {
                 if (!st.small) {
-                    st.t = te - mu;
-                    st.small = 1;
-                    st.t += small;
+                    st.sw = (st.guard << 2) | 2;
+                    begin_small(st, __fsub_rn(te, mu), small);
                     continue;
                 }
                 if (!st.prev_known) st.prev = sample_at(S, g, f, st.prev_t);
@@ -313,11 +348,11 @@ __device__ void march_coop(const SessionDev* S, const RayGeo& g, const TF* f, Ra
             }
             return;
         }
-        st.small = 1;   // 0 <= fe < 0.99 during large steps
+        st.sw = (st.guard << 2) | 1;   // 0 <= fe < 0.99 during large steps (only they are events)
         st.prev = fe;
         st.prev_t = te;
         st.prev_known = 1;
-        st.t = te + small;
+        begin_small(st, te, small);
     }
 }
 
@@ -369,8 +404,15 @@ __device__ __forceinline__ void write_hit(const SessionDev* S, int level, int i,
     *on = make_float4(0.f, 0.f, 0.f, kInvalid);
 }
 
+__device__ __forceinline__ void write_trace(const SessionDev* S, int level, int i, int j, unsigned long long code) {
+    unsigned long long* tr = S->trace[level];
+    if (tr) tr[size_t(j) * S->lv[level].w + i] = code;
+}
+
 template <class TF>
-__device__ void finish_ray(const SessionDev* S, const RayGeo& g, const TF* f, int level, int i, int j, float precise) {
+__device__ void finish_ray(const SessionDev* S, const RayGeo& g, const TF* f, int level, int i, int j, float precise,
+                           const RayState& st) {
+    write_trace(S, level, i, j, ray_trace_code(st, precise));
     const HitGeo h = hit_geo(S, g, precise);
     float v[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
     if (precise != 0.0f) {
@@ -384,7 +426,8 @@ __device__ void finish_ray(const SessionDev* S, const RayGeo& g, const TF* f, in
 // writes
 template <class TF>
 __device__ void finish_ray_warp(const SessionDev* S, const RayGeo& g, const TF* f, int level, int i, int j,
-                                float precise, int lane) {
+                                float precise, int lane, const RayState& st) {
+    if (lane == 0) write_trace(S, level, i, j, ray_trace_code(st, precise));
     const HitGeo h = hit_geo(S, g, precise);
     float mine = 0.f;
     if (precise != 0.0f && lane < 6) mine = grad_sample(f, S->n, h, lane);
@@ -395,6 +438,7 @@ __device__ void finish_ray_warp(const SessionDev* S, const RayGeo& g, const TF* 
 }
 
 __device__ __forceinline__ void write_miss(const SessionDev* S, int level, int i, int j) {
+    write_trace(S, level, i, j, 0ull);
     if (S->keep_on_miss) return;
     const int w = S->lv[level].w;
     S->pv[level][size_t(j) * w + i] = make_float4(0.f, 0.f, 0.f, kInvalid);
@@ -421,7 +465,7 @@ __device__ void serial_ray(const EngineView& v, const SessionDev* S, int s, cons
         }
         march_serial(S, g, f, st, 0x7fffffff, precise);   // queue full: finish here
     }
-    finish_ray(S, g, f, level, i, j, precise);
+    finish_ray(S, g, f, level, i, j, precise, st);
 }
 
 // Each warp pulls 8 x 4-ray tiles on its own (no block-wide barrier).  Steps of many ray tiles
@@ -462,7 +506,7 @@ __device__ void coop_ray(const SessionDev* S, const LongRay& L, int lane) {
     RayState st = L.st;
     float precise = 0.0f;
     march_coop(S, g, f, st, lane, precise);
-    finish_ray_warp(S, g, f, L.level, L.i, L.j, precise, lane);
+    finish_ray_warp(S, g, f, L.level, L.i, L.j, precise, lane, st);
 }
 
 // the queued long rays, one warp each
@@ -517,7 +561,7 @@ __global__ void raycast_stage_kernel(SessionDev S, RayStage rs, int w, int h) {
     }
     float precise = 0.0f;
     march_serial(&S, g, f, st, 0x7fffffff, precise);
-    finish_ray(&S, g, f, 0, i, j, precise);
+    finish_ray(&S, g, f, 0, i, j, precise, st);
 }
 
 cudaError_t stage_raycast(const kf_volume* vol, const float* pose, const float* ik, float4* vtx, float4* nrm, int w,

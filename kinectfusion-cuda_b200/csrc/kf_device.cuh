@@ -60,6 +60,9 @@ struct SessionDev {
     float4* pv[kMaxLevels];   // predicted (raycast) vertices, world frame
     float4* pn[kMaxLevels];   // predicted normals, world frame
     uint8_t* mask[kMaxLevels];// ICP correspondence masks (null unless exported)
+    // debug mode only (null otherwise): per-pixel march decision traces of the last raycast,
+    // see ray_trace_code in k_raycast.cu
+    unsigned long long* trace[kMaxLevels];
     // volume
     int n, fmt;
     float vol_w, res, mu, max_w;

@@ -19,7 +19,7 @@ import os
 import numpy as np
 
 from . import _lib
-from ._lib import (KF_ERR_ARG, KF_ERR_CAPACITY, KF_ERR_CUDA, KF_ERR_NONFINITE, KF_ERR_OOM_BUDGET, KF_ERR_SHAPE,
+from ._lib import (KF_DEBUG_RAY_TRACE, KF_ERR_ARG, KF_ERR_CAPACITY, KF_ERR_CUDA, KF_ERR_NONFINITE, KF_ERR_OOM_BUDGET, KF_ERR_SHAPE,
                    KF_ERR_STATE, KF_ERR_TIMEOUT, KF_MAX_LEVELS, KF_OK, KF_RENDER_NORMALS, KF_RENDER_SHADING,
                    KF_TSDF_F16U16, KF_TSDF_F32F32, KF_WEIGHT_SCALE, KfConfig, KfError, KfFrameStats, KfServerStats,
                    KfVolume, check, lib)
@@ -315,6 +315,17 @@ class KinectFusion:
         ms = (ctypes.c_float * 4)()
         check(lib.kf_session_stage_times(self._s, ms))
         return list(ms)
+
+    def set_debug(self, flags):
+        """Debug modes (KF_DEBUG_RAY_TRACE: record march decision traces)."""
+        check(lib.kf_session_set_debug(self._s, int(flags)), "kf_session_set_debug")
+
+    def ray_trace(self, level=0):
+        """(h, w) int64 march decision traces of the last raycast at `level` (debug mode)."""
+        w, h = self._lw(level)
+        t = np.empty((h, w), np.int64)
+        check(lib.kf_get_ray_trace(self._s, level, _np_ptr(t), 1), "kf_get_ray_trace")
+        return t
 
 
 # ------------------------------------------------------------------------------------------

@@ -26,6 +26,7 @@ KF_ERR_TOO_LARGE = 9
 KF_LLS_NOALLOC_MAX_ROWS = 1048576   # row limit of kf_solve_linear_least_squares_noalloc
 KF_RENDER_NORMALS = 0
 KF_RENDER_SHADING = 1
+KF_DEBUG_RAY_TRACE = 1
 
 KF_TSDF_F32F32 = 0
 KF_TSDF_F16U16 = 1
@@ -153,6 +154,8 @@ SIGNATURES = {
     "kf_now_ms": (ctypes.c_double, []),
     "kf_session_set_profiling": (_I, [_P, _I]),
     "kf_session_stage_times": (_I, [_P, _FP]),
+    "kf_session_set_debug": (_I, [_P, _I]),
+    "kf_get_ray_trace": (_I, [_P, _I, _P, _I]),
     "kf_batch_set_profiling": (_I, [_P, _I]),
     "kf_batch_stage_times": (_I, [_P, _FP]),
     "kf_selftest_bounded_wait": (_I, [_I, _IP]),

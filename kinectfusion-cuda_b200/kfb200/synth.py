@@ -33,6 +33,10 @@ _lib.kfs_render.restype = ctypes.c_int
 
 WOBBLE = 0   # smooth wobble around the start pose (<= 2 cm, <= 1 degree per frame)
 LOOP = 1     # closed loop around the objects
+# frames of one closed loop: the full-size sequence (about 1.6 cm and 0.4 degrees per frame).
+# A shorter LOOP request is the start of this loop, not a faster loop: a loop squeezed into a
+# few frames moves the camera up to 0.8 m per frame, which no tracker follows.
+LOOP_FRAMES = 300
 
 
 def scene(cube_width):
@@ -43,11 +47,13 @@ def scene(cube_width):
 
 
 def trajectory(kind, frames, seed, cube_width):
-    """Camera->world poses, (frames, 4, 4) float32, indexed [row, col]."""
-    buf = np.zeros((frames, 16), np.float32)
-    if _lib.kfs_trajectory(int(kind), int(frames), int(seed), float(cube_width), buf.ctypes.data) != 0:
+    """Camera->world poses, (frames, 4, 4) float32, indexed [row, col].  A LOOP of fewer
+    than LOOP_FRAMES frames is the start of the LOOP_FRAMES-frame loop."""
+    total = max(int(frames), LOOP_FRAMES) if kind == LOOP else int(frames)
+    buf = np.zeros((total, 16), np.float32)
+    if _lib.kfs_trajectory(int(kind), total, int(seed), float(cube_width), buf.ctypes.data) != 0:
         raise ValueError("bad trajectory request")
-    return buf.reshape(frames, 4, 4).transpose(0, 2, 1).copy()
+    return buf.reshape(total, 4, 4).transpose(0, 2, 1)[: int(frames)].copy()
 
 
 def render(sc, pose, width, height, fx, fy, cx, cy, seed, frame, noise=True, true_depth=False):

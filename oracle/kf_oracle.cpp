@@ -352,13 +352,33 @@ template <class T> inline V3<T> gradient(V3<T> p, const T* f, int n, T width, T 
 struct RaycastParams {
     float min_d, max_d, step_l, step_s;
     int keep_on_miss, tex9bit;
+    // 0: sample positions by the reference's repeated additions t <- t + inc
+    //    (project/src/raycast.cu:78), whose float rounding drifts along a ray;
+    // 1: the CUDA library's positions, t_k = base + k * inc with one rounding (base: the near
+    //    distance, the sample that left large steps, or t - mu after a back-off), which follow
+    //    the FP64 march to within a rounding.  In FP64 both agree to ~1e-16.
+    int exact_positions = 0;
 };
 
 // raycastKernel, project/src/raycast.cu:44-145.  Returns the number of TSDF samples taken
 // (march samples plus six per gradient), the unit of the raycast's algorithmic traffic.
+// The march's decision trace of one ray, in the encoding the CUDA library's debug mode writes
+// (so a test can tell pixels whose march took the same decisions from pixels where a sample
+// near 0.99 or 0 decided differently):
+//   bits 40..  samples taken when the march left large steps (0: it never did)
+//   bits  8..39 samples taken when the march ended
+//   bits  4..5  how it left large steps: 1 a sample in [0, 0.99), 2 a negative one (back-off)
+//   bits  0..1  how it ended: 0 past the far plane or the sample bound, 1 negative first
+//               sample, 2 refined hit
+// A ray that returns before marching (no volume in range) has trace 0.
+inline int64_t march_trace(int taken_sw, int mode, int taken_end, int end) {
+    return (int64_t(taken_sw) << 40) | (int64_t(taken_end) << 8) | (int64_t(mode) << 4) | int64_t(end);
+}
+
 template <class T>
 long long raycast(const T* f, int n, float width_f, float mu_f, const Pose<T>& pose, const M3<T>& inv_k,
-                  V4<T>* vmap, V4<T>* nmap, int w, int cw, int ch, const RaycastParams& rp) {
+                  V4<T>* vmap, V4<T>* nmap, int w, int cw, int ch, const RaycastParams& rp,
+                  int64_t* trace = nullptr) {
     const T width = T(width_f), mu = T(mu_f);
     const M3<T> ray_m = mul(pose.R, inv_k);
     const V3<T> o = pose.t;
@@ -388,30 +408,57 @@ long long raycast(const T* f, int n, float width_f, float mu_f, const Pose<T>& p
                     ov = {T(0), T(0), T(0), T(kInvalid)};
                     on = {T(0), T(0), T(0), T(kInvalid)};
                 }
+                if (trace) trace[size_t(j) * w + i] = 0;
                 continue;
             }
             T inc = large, prev = 0, precise = 0;
             int guard = 0;   // the CUDA library's bound on samples per ray
-            for (T t = near_d; t < far_d && guard < (1 << 16); t += inc, ++guard) {
+            int taken = 0, taken_sw = 0, mode = 0, end = 0;
+            T base = near_d;   // exact_positions: t = base + idx * inc
+            int idx = 0;
+            // the reference's for loop: t = near; while t < far; t += inc (or the exact position)
+            T t = near_d;
+            while (t < far_d && guard < (1 << 16)) {
                 const V3<T> p = add(o, scale(dir, t));
                 const V3<T> u = to_uvw(p, width);
                 const T tsdf = sample(f, n, u.x, u.y, u.z, rp.tex9bit);
                 ++samples;
+                ++taken;
                 if (tsdf < T(0)) {
                     if (t != near_d) {
                         if (inc == large) {
                             t -= mu;
                             inc = small;
+                            taken_sw = taken;
+                            mode = 2;
+                            base = t;
+                            idx = 0;
+                            t = rp.exact_positions ? T(std::fma(T(idx + 1), inc, base)) : T(t + inc);
+                            ++idx;
+                            ++guard;
                             continue;
                         }
                         precise = t - inc * prev / (tsdf - prev);
+                        end = 2;
+                    } else {
+                        end = 1;
                     }
                     break;
                 } else if (tsdf < T(0.99f)) {
+                    if (inc == large) {
+                        taken_sw = taken;
+                        mode = 1;
+                        base = t;
+                        idx = 0;
+                    }
                     inc = small;
                 }
                 prev = tsdf;
+                ++guard;
+                ++idx;
+                t = rp.exact_positions ? T(std::fma(T(idx), inc, base)) : T(t + inc);
             }
+            if (trace) trace[size_t(j) * w + i] = march_trace(taken_sw, mode, taken, end);
             if (precise != T(0)) {
                 const V3<T> vtx = add(o, scale(dir, precise));
                 V3<T> g = gradient(vtx, f, n, width, mu, rp.tex9bit);
@@ -649,6 +696,7 @@ template <class T> struct Pipeline {
     int frame = 0, status = 0;
     int iters_done[KF_MAX_LEVELS]{};
     long long last_samples[KF_MAX_LEVELS]{};
+    std::vector<int64_t> trace[KF_MAX_LEVELS];   // march decision traces of the last raycast
     long long last_fused = 0;
     int tex9bit = 0;
 
@@ -668,6 +716,7 @@ template <class T> struct Pipeline {
             pv[l].assign(size_t(w[l]) * h[l], V4<T>{0, 0, 0, 0});
             pn[l].assign(size_t(w[l]) * h[l], V4<T>{0, 0, 0, 0});
             mask[l].assign(size_t(w[l]) * h[l], 0);
+            trace[l].assign(size_t(w[l]) * h[l], 0);
         }
         depth_m.assign(size_t(c.width) * c.height, T(0));
         n = c.volume_n;
@@ -709,7 +758,7 @@ template <class T> struct Pipeline {
         RaycastParams rp{cfg.min_depth, cfg.max_depth, cfg.step_large, cfg.step_small, cfg.keep_on_miss, tex9bit};
         for (int l = 0; l < L; ++l)
             last_samples[l] = raycast(F.data(), n, cfg.volume_width, cfg.mu, pose, iK[l], pv[l].data(),
-                                      pn[l].data(), w[l], cw[l], ch[l], rp);
+                                      pn[l].data(), w[l], cw[l], ch[l], rp, trace[l].data());
         // computePose (:146-161) -> ICP::computePose (project/src/icp.cpp:25-58)
         Pose<T> est = pose;
         const bool ok = compute_pose(est);
@@ -848,23 +897,25 @@ int kfo_compute_normal(const float* vmap, int w, int h, int i, int j, float out[
     return 0;
 }
 
+// trace (may be NULL): w * h march decision traces (march_trace)
 long long kfo_raycast(const float* tsdf_f, int n, float width, float mu, const float pose[16],
                       const float inv_k[9], float* vmap, float* nmap, int w, int h, float min_d, float max_d,
-                      float step_l, float step_s, int keep_on_miss, int tex9bit, int trunc8, int prec) {
+                      float step_l, float step_s, int keep_on_miss, int tex9bit, int trunc8, int prec,
+                      int64_t* trace, int exact_positions) {
     const size_t np = size_t(w) * h;
-    RaycastParams rp{min_d, max_d, step_l, step_s, keep_on_miss, tex9bit};
+    RaycastParams rp{min_d, max_d, step_l, step_s, keep_on_miss, tex9bit, exact_positions};
     long long samples;
     if (prec) {
         std::vector<double> f = from_float<double>(tsdf_f, size_t(n) * n * n);
         std::vector<V4<double>> v = from_float4<double>(vmap, np), nn = from_float4<double>(nmap, np);
         samples = raycast<double>(f.data(), n, width, mu, pose_from16<double>(pose), from_flat9<double>(inv_k),
-                                  v.data(), nn.data(), w, cover8(w, trunc8), cover8(h, trunc8), rp);
+                                  v.data(), nn.data(), w, cover8(w, trunc8), cover8(h, trunc8), rp, trace);
         to_float4(v, vmap);
         to_float4(nn, nmap);
     } else {
         std::vector<V4<float>> v = from_float4<float>(vmap, np), nn = from_float4<float>(nmap, np);
         samples = raycast<float>(tsdf_f, n, width, mu, pose_from16<float>(pose), from_flat9<float>(inv_k),
-                                 v.data(), nn.data(), w, cover8(w, trunc8), cover8(h, trunc8), rp);
+                                 v.data(), nn.data(), w, cover8(w, trunc8), cover8(h, trunc8), rp, trace);
         to_float4(v, vmap);
         to_float4(nn, nmap);
     }
@@ -1104,6 +1155,12 @@ int kfo_pipeline_get_vertex(void* h, int level, float* dst) {
 
 int kfo_pipeline_get_raycast(void* h, int level, float* vtx, float* nrm) {
     KFO_DISPATCH(h, { to_float4(P->pv[level], vtx); to_float4(P->pn[level], nrm); });
+    return 0;
+}
+
+// march decision traces of the last frame's raycast at `level` (march_trace encoding)
+int kfo_pipeline_get_trace(void* h, int level, int64_t* dst) {
+    KFO_DISPATCH(h, std::memcpy(dst, P->trace[level].data(), P->trace[level].size() * sizeof(int64_t)));
     return 0;
 }
 

@@ -35,7 +35,7 @@ _SIG = {
     "kfo_vertex_map": (_I, [_P, _P, _I, _I, _P, _I, _I]),
     "kfo_normal_map": (_I, [_P, _P, _I, _I, _I, _I]),
     "kfo_compute_normal": (_I, [_P, _I, _I, _I, _I, _P]),
-    "kfo_raycast": (_LL, [_P, _I, _F, _F, _P, _P, _P, _P, _I, _I, _F, _F, _F, _F, _I, _I, _I, _I]),
+    "kfo_raycast": (_LL, [_P, _I, _F, _F, _P, _P, _P, _P, _I, _I, _F, _F, _F, _F, _I, _I, _I, _I, _P, _I]),
     "kfo_fuse": (_LL, [_P, _I, _I, _P, _P, _P, _I, _F, _F, _F, _P, _F, _F, _I, _I]),
     "kfo_voxel_axes": (_I, [_I, _F, _P, _P]),
     "kfo_icp_residuals": (_I, [_P, _P, _P, _I, _I, _P, _P, _P, _P, _P, _F, _F, _P, _P, _P, _I]),
@@ -58,6 +58,7 @@ _SIG = {
     "kfo_pipeline_get_vertex": (_I, [_P, _I, _P]),
     "kfo_pipeline_get_raycast": (_I, [_P, _I, _P, _P]),
     "kfo_pipeline_get_mask": (_I, [_P, _I, _P]),
+    "kfo_pipeline_get_trace": (_I, [_P, _I, _P]),
     "kfo_pipeline_get_tsdf": (_I, [_P, _P, _P]),
     "kfo_pipeline_set_tsdf": (_I, [_P, _P, _P]),
     "kfo_pipeline_last_samples": (_LL, [_P, _I]),
@@ -138,15 +139,21 @@ def compute_normal(vmap, i, j):
 
 
 def raycast(tsdf_f, width, mu, pose, inv_k, w, h, min_d=0.4, max_d=6.0, step_l=1.99, step_s=0.1,
-            keep_on_miss=True, tex9bit=False, prec=0, vmap=None, nmap=None, trunc8=False):
-    """Returns (vertex (h,w,4), normal (h,w,4), samples)."""
+            keep_on_miss=True, tex9bit=False, prec=0, vmap=None, nmap=None, trunc8=False, trace=False,
+            exact_positions=False):
+    """Returns (vertex (h,w,4), normal (h,w,4), samples), plus the (h, w) int64 march decision
+    traces (see march_trace in kf_oracle.cpp) when trace is true.  exact_positions: sample
+    positions base + k * inc with one rounding (the CUDA library's) instead of the reference's
+    repeated additions."""
     n = tsdf_f.shape[0]
     f = np.ascontiguousarray(tsdf_f, np.float32)
     v = np.zeros((h, w, 4), np.float32) if vmap is None else np.ascontiguousarray(vmap, np.float32).copy()
     nn = np.zeros((h, w, 4), np.float32) if nmap is None else np.ascontiguousarray(nmap, np.float32).copy()
+    tr = np.zeros((h, w), np.int64) if trace else None
     s = _lib.kfo_raycast(_p(f), n, width, mu, _p(_cm(pose)), _p(_cm(inv_k)), _p(v), _p(nn), w, h, min_d, max_d,
-                         step_l, step_s, int(keep_on_miss), int(tex9bit), int(trunc8), prec)
-    return v, nn, s
+                         step_l, step_s, int(keep_on_miss), int(tex9bit), int(trunc8), prec,
+                         _p(tr) if trace else None, int(exact_positions))
+    return (v, nn, s, tr) if trace else (v, nn, s)
 
 
 def fuse(depth_m, cam_k, tsdf_f, tsdf_w, width, mu, pose, max_w=0.0, min_d=0.4, max_d=6.0, prec=0, trunc8=False):
@@ -301,6 +308,13 @@ class Pipeline:
         n = np.zeros((h, w, 4), np.float32)
         _lib.kfo_pipeline_get_raycast(self._h, level, _p(v), _p(n))
         return v, n
+
+    def ray_trace(self, level=0):
+        """(h, w) int64 march decision traces of the last frame's raycast at `level`."""
+        w, h = self._wh(level)
+        t = np.zeros((h, w), np.int64)
+        _lib.kfo_pipeline_get_trace(self._h, level, _p(t))
+        return t
 
     def icp_mask(self, level=0):
         w, h = self._wh(level)

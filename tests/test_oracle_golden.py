@@ -273,7 +273,9 @@ def test_pipeline_frame0_fuses_only(orc, kf):
 
 # ---- the fixture against the reference's test sources it was transcribed from ----
 
-REFERENCE_ROOT = os.environ.get("KF_REFERENCE_ROOT", "/root/reference")
+# a checkout of the reference project, given by the environment; without one the two checks
+# below are skipped
+REFERENCE_ROOT = os.environ.get("KF_REFERENCE_ROOT", "")
 
 
 def _transcription():
@@ -287,9 +289,9 @@ def _transcription():
 
 def test_golden_transcription_matches_reference_sources():
     """Every number of every fixture entry appears among the numeric literals of the test lines
-    it cites (runs where a reference checkout is present; KF_REFERENCE_ROOT points at one)."""
+    it cites (runs where KF_REFERENCE_ROOT names a reference checkout)."""
     import pytest
-    if not os.path.isdir(os.path.join(REFERENCE_ROOT, "test")):
+    if not REFERENCE_ROOT or not os.path.isdir(os.path.join(REFERENCE_ROOT, "test")):
         pytest.skip("no reference checkout on this machine")
     assert _transcription().check(REFERENCE_ROOT) == []
 
@@ -299,7 +301,7 @@ def test_golden_transcription_check_catches_a_changed_value():
     reported for that entry alone."""
     import copy
     import pytest
-    if not os.path.isdir(os.path.join(REFERENCE_ROOT, "test")):
+    if not REFERENCE_ROOT or not os.path.isdir(os.path.join(REFERENCE_ROOT, "test")):
         pytest.skip("no reference checkout on this machine")
     fx = copy.deepcopy(GOLDEN)
     fx["fill_a_b"]["b"] = -7.5

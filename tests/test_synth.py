@@ -61,3 +61,16 @@ def test_trajectory_motion_bounds(synth, kind, frames):
     # the loop closes
     if kind == 1:
         np.testing.assert_allclose(poses[0], poses[-1], atol=0.03)
+
+
+def test_short_loop_is_the_start_of_the_full_loop(synth):
+    """A LOOP of a few frames follows the full-size sequence's camera (per-frame motion <= 2 cm,
+    <= 1 degree), not a loop squeezed into those frames."""
+    full = synth.trajectory(synth.LOOP, synth.LOOP_FRAMES, 63, 3.0)
+    for frames in (2, 6, 46):
+        short = synth.trajectory(synth.LOOP, frames, 63, 3.0)
+        assert short.shape == (frames, 4, 4)
+        np.testing.assert_array_equal(short, full[:frames])
+    longer = synth.trajectory(synth.LOOP, 400, 63, 3.0)
+    assert longer.shape == (400, 4, 4)
+    assert max(np.linalg.norm(b[:3, 3] - a[:3, 3]) for a, b in zip(longer[:-1], longer[1:])) <= 0.02

@@ -2,18 +2,17 @@
 kf_solve_linear_least_squares on the same device A and b.
 
 The no-allocation entry point keeps its scratch in a static device array of the library and
-runs the same kernels with the same block count, so both give the same x; the tolerance
-below allows last-bit differences only.  Calls come in a row, a large system then a smaller
-one, so the second call runs on a scratch the first one left filled.  This file is named to
-be collected last: it must pass alone and after every other test."""
+runs the same kernels with the same block count and reduction order, so both give the same x
+bit for bit; the comparison with the allocating entry point is exact, and only the check
+against an FP64 solve of the normal equations has a tolerance.  Calls come in a row, a large
+system then a smaller one, so the second call runs on a scratch the first one left filled.
+This file is named to be collected last: it must pass alone and after every other test."""
 import ctypes
 
 import numpy as np
 import pytest
 
 pytestmark = pytest.mark.gpu
-
-RTOL, ATOL = 1e-6, 1e-7
 
 
 def system(cuda, n, seed):
@@ -38,7 +37,7 @@ def test_two_calls_in_a_row_match_the_allocating_entry(kf, cuda):
         st_ref, x_ref = solve(kf, lib.kf_solve_linear_least_squares, Ad, bd, n, stream)
         st_na, x_na = solve(kf, lib.kf_solve_linear_least_squares_noalloc, Ad, bd, n, stream)
         assert st_ref == st_na == kf.KF_OK, (st_ref, st_na)
-        np.testing.assert_allclose(x_na, x_ref, rtol=RTOL, atol=ATOL)
+        np.testing.assert_array_equal(x_na, x_ref)
         # and both solve the FP64 normal equations
         A64 = A.astype(np.float64)
         x64 = np.linalg.solve(A64.T @ A64, A64.T @ b.astype(np.float64))
@@ -53,7 +52,7 @@ def test_largest_system_and_default_stream(kf, cuda):
     st_ref, x_ref = solve(kf, lib.kf_solve_linear_least_squares, Ad, bd, n)
     st_na, x_na = solve(kf, lib.kf_solve_linear_least_squares_noalloc, Ad, bd, n)
     assert st_ref == st_na == kf.KF_OK
-    np.testing.assert_allclose(x_na, x_ref, rtol=RTOL, atol=ATOL)
+    np.testing.assert_array_equal(x_na, x_ref)
 
 
 def test_rejects_rows_beyond_the_scratch(kf, cuda):
