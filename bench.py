@@ -919,11 +919,32 @@ def run_profile_frames(args, local):
     cfg = full_config(kf, tsdf_format=args.tsdf_format)
     imgs, _ = render_frames(kf, cfg, args.profile_frames, seed=1)
     s = kf.KinectFusion(cfg)
+    if args.no_graph:
+        s.set_debug(kf.KF_DEBUG_NO_GRAPH)
     for img in imgs:
         st, _ = s.process_frame(img)
     torch.cuda.synchronize()
     print("profile frames done:", args.profile_frames, "status", st, s.frame_stats(), flush=True)
     s.close()
+
+
+def run_profile_batch(args, local):
+    """`--profile-frames` steps of a batch of `--profile-batch` full-size f16+u16 sessions through
+    kf_batch_step (device frames), then exit: the command under the batched ncu captures."""
+    import torch
+    import kfb200 as kf
+    torch.cuda.set_device(local)
+    stream = torch.cuda.current_stream()
+    K = args.profile_batch
+    cfgs = [kf.config_full(tsdf_format=kf.KF_TSDF_F16U16) for _ in range(K)]
+    frames = session_frames(kf, cfgs[: min(K, 8)], args.profile_frames, 200, torch)
+    b = kf.Batch(cfgs)
+    if args.no_graph:
+        b.set_debug(kf.KF_DEBUG_NO_GRAPH)
+    batch_steps(kf, b, [frames[i % len(frames)] for i in range(K)], args.profile_frames, 0, stream)
+    torch.cuda.synchronize()
+    print("profile batch done: %d sessions x %d steps" % (K, args.profile_frames), flush=True)
+    b.close()
 
 
 def main():
@@ -943,10 +964,17 @@ def main():
                     help="run this many frames of the workload through kf_process_frame and exit, "
                          "printing no measurement (a short command for ncu captures of one kernel)")
     ap.add_argument("--tsdf-format", type=int, default=0, help="0: f32+f32 volume, 1: fp16+u16 (with --profile-frames)")
+    ap.add_argument("--profile-batch", type=int, default=0,
+                    help="with --profile-frames: that many steps of a batch of this many full-size f16+u16 "
+                         "sessions, then exit (a short command for ncu captures of the batched kernels)")
+    ap.add_argument("--no-graph", action="store_true",
+                    help="with --profile-*: plain launches per stage inside NVTX ranges (KF_DEBUG_NO_GRAPH)")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
     world, rank, local = dist_setup()
-    if args.profile_frames > 0:
+    if args.profile_frames > 0 and args.profile_batch > 0:
+        run_profile_batch(args, local)
+    elif args.profile_frames > 0:
         run_profile_frames(args, local)
     elif args.impl == "reference":
         run_reference(args, world, rank)

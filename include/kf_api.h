@@ -393,7 +393,13 @@ kf_status kf_session_stage_times(kf_session* s, float ms[4]);
  * differ by arithmetic rounding; a different trace means a sample near 0.99 or 0 decided
  * otherwise.  No counterpart in the reference (a parity aid). */
 #define KF_DEBUG_RAY_TRACE 1
+/* KF_DEBUG_NO_GRAPH launches every step's kernels one by one instead of replaying the captured
+ * graph, each stage inside an NVTX range (kf.preprocess, kf.raycast, kf.icp, kf.fusion), so a
+ * profiler can select a stage's launches.  Results are the same; steps are slower. */
+#define KF_DEBUG_NO_GRAPH 2
 kf_status kf_session_set_debug(kf_session* s, int flags);
+/* The same for every session of a batch (KF_DEBUG_NO_GRAPH applies to the batch's steps). */
+kf_status kf_batch_set_debug(kf_batch* b, int flags);
 /* The traces of the last raycast at `level` (w * h uint64; host memory when to_host = 1).
  * KF_ERR_STATE unless KF_DEBUG_RAY_TRACE is on. */
 kf_status kf_get_ray_trace(kf_session* s, int level, uint64_t* dst, int to_host);

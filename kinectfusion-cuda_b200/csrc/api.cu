@@ -16,11 +16,22 @@
 #include <string>
 #include <vector>
 
+#include <nvtx3/nvToolsExt.h>
+
 #include "kf_host.h"
 
 using namespace kf;
 
 namespace {
+
+// NVTX range over a host call or a stage's launches (a no-op unless a tool such as ncu
+// injects NVTX; `ncu --nvtx --nvtx-include kf.raycast/` then selects that stage's kernels)
+struct NvtxRange {
+    explicit NvtxRange(const char* name) { nvtxRangePushA(name); }
+    ~NvtxRange() { nvtxRangePop(); }
+    NvtxRange(const NvtxRange&) = delete;
+    NvtxRange& operator=(const NvtxRange&) = delete;
+};
 
 thread_local cudaError_t g_last_cuda = cudaSuccess;
 
@@ -714,21 +725,32 @@ struct Engine {
             KF_CK(cudaEventRecord(ev_fork, st));
             KF_CK(cudaStreamWaitEvent(aux_stream, ev_fork, 0));
             if (input_wait) KF_CK(cudaStreamWaitEvent(aux_stream, ev_input, capturing ? cudaEventWaitExternal : 0));
+            NvtxRange r("kf.preprocess");
             KF_CK(launch_preprocess(v, grid_pre, aux_stream));
             if (profile) KF_CK(cudaEventRecordWithFlags(ev[1], aux_stream, cudaEventRecordExternal));
             KF_CK(cudaEventRecord(ev_join, aux_stream));
         } else {
             if (stages[0] && input_wait) KF_CK(cudaStreamWaitEvent(st, ev_input, capturing ? cudaEventWaitExternal : 0));
+            NvtxRange r("kf.preprocess");
             if (stages[0]) KF_CK(launch_preprocess(v, grid_pre, st));
             if (profile) KF_CK(cudaEventRecordWithFlags(ev[1], st, cudaEventRecordExternal));
         }
-        if (stages[1]) KF_CK(launch_raycast(v, grid_ray, st, ray_many));
+        {
+            NvtxRange r("kf.raycast");
+            if (stages[1]) KF_CK(launch_raycast(v, grid_ray, st, ray_many));
+        }
         if (fork) KF_CK(cudaStreamWaitEvent(st, ev_join, 0));
         if (profile) KF_CK(cudaEventRecordWithFlags(ev[2], st, cudaEventRecordExternal));
-        if (stages[2]) KF_CK(launch_icp(v, grid_icp, st, cap == 1));
+        {
+            NvtxRange r("kf.icp");
+            if (stages[2]) KF_CK(launch_icp(v, grid_icp, st, cap == 1));
+        }
         if (profile) KF_CK(cudaEventRecordWithFlags(ev[3], st, cudaEventRecordExternal));
-        if (stages[3]) KF_CK(launch_fuse(v, grid_fuse, st));
-        if (stages[3]) KF_CK(launch_bricks(v, grid_brick, st));
+        {
+            NvtxRange r("kf.fusion");
+            if (stages[3]) KF_CK(launch_fuse(v, grid_fuse, st));
+            if (stages[3]) KF_CK(launch_bricks(v, grid_brick, st));
+        }
         if (profile) KF_CK(cudaEventRecordWithFlags(ev[4], st, cudaEventRecordExternal));
         KF_CK(cudaMemcpyAsync(h_out, d_out, sizeof(OutDev) * cap, cudaMemcpyDeviceToHost, st));
         KF_CK(cudaMemcpyAsync(h_sync, d_sync, sizeof(GridSync), cudaMemcpyDeviceToHost, st));
@@ -962,6 +984,7 @@ kf_status kf_session_footprint(const kf_config* cfg, size_t* bytes) {
 }
 
 kf_status kf_session_create(const kf_config* cfg, kf_session** out) {
+    NvtxRange nvtx_("kf_session_create");
     if (!cfg || !out) return KF_ERR_ARG;
     KF_TRY(validate(*cfg));
     kf_session* s = new (std::nothrow) kf_session;
@@ -1009,6 +1032,7 @@ static kf_status session_enqueue(kf_session* s, const uint16_t* depth, int is_de
 }
 
 kf_status kf_process_frame(kf_session* s, const uint16_t* depth, int is_device_ptr, void* stream, float pose_out[16]) {
+    NvtxRange nvtx_("kf_process_frame");
     if (!s || !depth) return KF_ERR_ARG;
     cudaStream_t st = as_stream(stream);
     KF_TRY(session_enqueue(s, depth, is_device_ptr, st));
@@ -1021,6 +1045,7 @@ kf_status kf_process_frame(kf_session* s, const uint16_t* depth, int is_device_p
 }
 
 kf_status kf_process_frame_async(kf_session* s, const uint16_t* depth_device, void* stream) {
+    NvtxRange nvtx_("kf_process_frame_async");
     if (!s || !depth_device) return KF_ERR_ARG;
     cudaStream_t st = as_stream(stream);
     KF_TRY(session_enqueue(s, depth_device, 1, st));
@@ -1258,6 +1283,7 @@ kf_status kf_float_channel_to_rgba(const float* src, int w, int h, float scale, 
 }
 
 kf_status kf_render(kf_session* s, int mode, const float pose_in[16], uint8_t* rgba, int to_host, void* stream) {
+    NvtxRange nvtx_("kf_render");
     if (!s || !rgba || (mode != KF_RENDER_NORMALS && mode != KF_RENDER_SHADING)) return KF_ERR_ARG;
     Slot& sl = s->sl();
     if (sl.external) return KF_ERR_STATE;
@@ -1376,6 +1402,7 @@ kf_status kf_initialize_grid(const kf_volume* vol, void* stream, float* elapsed_
 
 kf_status kf_fuse(const float* depth_m, int w, int h, const float cam_k[9], const kf_volume* vol, const float pose[16],
                   float min_depth, float max_depth, void* stream, float* elapsed_ms) {
+    NvtxRange nvtx_("kf_fuse");
     if (!depth_m || !cam_k || !pose || w <= 0 || h <= 0) return KF_ERR_ARG;
     KF_TRY(check_volume(vol));
     std::vector<float> xs(vol->n), zs(vol->n);
@@ -1397,6 +1424,7 @@ kf_status kf_fuse(const float* depth_m, int w, int h, const float cam_k[9], cons
 kf_status kf_raycast(const kf_volume* vol, const float pose[16], const float inv_cam_k[9], float* vertex, int w, int h,
                      float* normal, int nw, int nh, float min_depth, float max_depth, float step_large,
                      float step_small, void* stream, float* elapsed_ms) {
+    NvtxRange nvtx_("kf_raycast");
     if (!pose || !inv_cam_k || !vertex || !normal || w <= 0 || h <= 0) return KF_ERR_ARG;
     KF_TRY(check_volume(vol));
     if (w != nw || h != nh) return KF_ERR_SHAPE;   // project/src/raycast.cu:155-158
@@ -1468,6 +1496,7 @@ kf_status kf_solve_linear_least_squares(const float* mat_a, const float* vec_b, 
 kf_status kf_compute_pose(const float* const* vertex, const float* const* target_vertex,
                           const float* const* target_normal, int w, int h, int levels, const kf_config* cfg,
                           const float pose[16], float pose_out[16], int iters_out[KF_MAX_LEVELS], void* stream) {
+    NvtxRange nvtx_("kf_compute_pose");
     if (!vertex || !target_vertex || !target_normal || !cfg || !pose || !pose_out) return KF_ERR_ARG;
     if (levels < 1 || levels > KF_MAX_LEVELS) return KF_ERR_ARG;
     kf_config c = *cfg;
@@ -1571,6 +1600,7 @@ kf_status kf_batch_destroy(kf_batch* b) {
 }
 
 kf_status kf_batch_step(kf_batch* b, const uint16_t* const* depth, int is_device_ptr, void* stream, float* poses_out) {
+    NvtxRange nvtx_("kf_batch_step");
     if (!b || !depth) return KF_ERR_ARG;
     cudaStream_t st = as_stream(stream);
     std::vector<StepDev> want(b->n);
@@ -1597,6 +1627,7 @@ kf_status kf_batch_step(kf_batch* b, const uint16_t* const* depth, int is_device
 }
 
 kf_status kf_batch_step_async(kf_batch* b, const int* active, void* stream) {
+    NvtxRange nvtx_("kf_batch_step_async");
     if (!b || !active) return KF_ERR_ARG;
     cudaStream_t st = as_stream(stream);
     std::vector<StepDev> want(b->n);
@@ -1674,6 +1705,7 @@ kf_status kf_batch_session(kf_batch* b, int i, kf_session** out) {
 // Volumes and poses are saved first and restored afterwards, so tuning leaves the sessions
 // exactly as they were.  Every session must have processed at least one frame.
 kf_status kf_batch_autotune(kf_batch* b, void* stream, char* report, size_t report_bytes) {
+    NvtxRange nvtx_("kf_batch_autotune");
     if (!b) return KF_ERR_ARG;
     Engine& e = b->eng;
     cudaStream_t st = as_stream(stream);
@@ -1830,6 +1862,7 @@ kf_status kf_server_destroy(kf_server* s) {
 }
 
 kf_status kf_server_open(kf_server* s, const kf_config* cfg, int* id) {
+    NvtxRange nvtx_("kf_server_open");
     if (!s || !cfg || !id) return KF_ERR_ARG;
     KF_TRY(validate(*cfg));
     const size_t need = footprint(*cfg) + size_t(cfg->width) * cfg->height * 2 * 2;
@@ -1950,6 +1983,7 @@ kf_status kf_server_reserve(kf_server* s, const kf_config* cfg, int count) {
 }
 
 kf_status kf_server_close(kf_server* s, int id) {
+    NvtxRange nvtx_("kf_server_close");
     if (!s) return KF_ERR_ARG;
     int slot;
     {
@@ -1992,6 +2026,7 @@ kf_status kf_server_submit(kf_server* s, int id, const uint16_t* depth, double t
 }
 
 kf_status kf_server_step(kf_server* s, int* served) {
+    NvtxRange nvtx_("kf_server_step");
     if (!s) return KF_ERR_ARG;
     std::lock_guard<std::mutex> g(s->gpu_mu);
     const int cap = s->max_slots;
@@ -2127,11 +2162,9 @@ kf_status kf_session_stage_times(kf_session* s, float ms[4]) {
     return s->eng->stage_times(ms);
 }
 
-kf_status kf_session_set_debug(kf_session* s, int flags) {
-    if (!s || (flags & ~KF_DEBUG_RAY_TRACE)) return KF_ERR_ARG;
-    Slot& sl = s->sl();
+// debug modes of one slot's session (traces) and of its engine (plain launches)
+static kf_status slot_set_debug(Engine& e, Slot& sl, int flags) {
     if (sl.external) return KF_ERR_STATE;
-    KF_CK(cudaDeviceSynchronize());
     const bool want = (flags & KF_DEBUG_RAY_TRACE) != 0;
     for (int l = 0; l < sl.cfg.levels; ++l) {
         if (want && !sl.d.trace[l]) {
@@ -2146,7 +2179,26 @@ kf_status kf_session_set_debug(kf_session* s, int flags) {
             sl.d.trace[l] = nullptr;
         }
     }
-    s->eng->tables_dirty = true;   // the session record on the device carries the pointers
+    e.tables_dirty = true;   // the session record on the device carries the pointers
+    const bool graph = (flags & KF_DEBUG_NO_GRAPH) == 0;
+    if (graph != e.use_graph) {
+        e.use_graph = graph;
+        e.graph_dirty = true;
+    }
+    return KF_OK;
+}
+
+kf_status kf_session_set_debug(kf_session* s, int flags) {
+    if (!s || (flags & ~(KF_DEBUG_RAY_TRACE | KF_DEBUG_NO_GRAPH))) return KF_ERR_ARG;
+    KF_CK(cudaDeviceSynchronize());
+    return slot_set_debug(*s->eng, s->sl(), flags);
+}
+
+kf_status kf_batch_set_debug(kf_batch* b, int flags) {
+    if (!b || (flags & ~(KF_DEBUG_RAY_TRACE | KF_DEBUG_NO_GRAPH))) return KF_ERR_ARG;
+    KF_CK(cudaDeviceSynchronize());
+    for (Slot& sl : b->eng.slots)
+        if (sl.used) KF_TRY(slot_set_debug(b->eng, sl, flags));
     return KF_OK;
 }
 

@@ -19,7 +19,7 @@ import os
 import numpy as np
 
 from . import _lib
-from ._lib import (KF_DEBUG_RAY_TRACE, KF_ERR_ARG, KF_ERR_CAPACITY, KF_ERR_CUDA, KF_ERR_NONFINITE, KF_ERR_OOM_BUDGET, KF_ERR_SHAPE,
+from ._lib import (KF_DEBUG_NO_GRAPH, KF_DEBUG_RAY_TRACE, KF_ERR_ARG, KF_ERR_CAPACITY, KF_ERR_CUDA, KF_ERR_NONFINITE, KF_ERR_OOM_BUDGET, KF_ERR_SHAPE,
                    KF_ERR_STATE, KF_ERR_TIMEOUT, KF_MAX_LEVELS, KF_OK, KF_RENDER_NORMALS, KF_RENDER_SHADING,
                    KF_TSDF_F16U16, KF_TSDF_F32F32, KF_WEIGHT_SCALE, KfConfig, KfError, KfFrameStats, KfServerStats,
                    KfVolume, check, lib)
@@ -317,7 +317,8 @@ class KinectFusion:
         return list(ms)
 
     def set_debug(self, flags):
-        """Debug modes (KF_DEBUG_RAY_TRACE: record march decision traces)."""
+        """Debug modes (KF_DEBUG_RAY_TRACE: record march decision traces; KF_DEBUG_NO_GRAPH:
+        plain launches per stage inside NVTX ranges instead of the captured graph)."""
         check(lib.kf_session_set_debug(self._s, int(flags)), "kf_session_set_debug")
 
     def ray_trace(self, level=0):
@@ -629,6 +630,10 @@ class Batch:
         ms = (ctypes.c_float * 4)()
         check(lib.kf_batch_stage_times(self._b, ms))
         return list(ms)
+
+    def set_debug(self, flags):
+        """Debug modes for every session of the batch (see KinectFusion.set_debug)."""
+        check(lib.kf_batch_set_debug(self._b, int(flags)), "kf_batch_set_debug")
 
 
 def selftest_bounded_wait(timeout_ms=50):

@@ -27,6 +27,7 @@ KF_LLS_NOALLOC_MAX_ROWS = 1048576   # row limit of kf_solve_linear_least_squares
 KF_RENDER_NORMALS = 0
 KF_RENDER_SHADING = 1
 KF_DEBUG_RAY_TRACE = 1
+KF_DEBUG_NO_GRAPH = 2
 
 KF_TSDF_F32F32 = 0
 KF_TSDF_F16U16 = 1
@@ -155,6 +156,7 @@ SIGNATURES = {
     "kf_session_set_profiling": (_I, [_P, _I]),
     "kf_session_stage_times": (_I, [_P, _FP]),
     "kf_session_set_debug": (_I, [_P, _I]),
+    "kf_batch_set_debug": (_I, [_P, _I]),
     "kf_get_ray_trace": (_I, [_P, _I, _P, _I]),
     "kf_batch_set_profiling": (_I, [_P, _I]),
     "kf_batch_stage_times": (_I, [_P, _FP]),

@@ -282,3 +282,20 @@ def test_bilateral_radius_zero_and_single_level(kf, orc):
         assert a <= 1e-4 and d <= 1e-4
     np.testing.assert_allclose(s.depth(0), s.depth(-1), rtol=0)   # a 1x1 window is the identity
     s.close()
+
+
+def test_debug_modes_change_no_result(kf, run_small):
+    """Plain launches per stage (KF_DEBUG_NO_GRAPH, the mode for profiling a stage) and the
+    decision-trace recording give the same poses as the replayed graph, bit for bit."""
+    cfg, imgs, s, P, rows = run_small
+    s2 = kf.KinectFusion(cfg)
+    s2.set_debug(kf.KF_DEBUG_NO_GRAPH | kf.KF_DEBUG_RAY_TRACE)
+    for i in range(5):
+        st, pose = s2.process_frame(imgs[i])
+        np.testing.assert_array_equal(pose, rows[i][2])
+    s2.set_debug(0)
+    st, pose = s2.process_frame(imgs[5])
+    np.testing.assert_array_equal(pose, rows[5][2])
+    with pytest.raises(kf.KfError):
+        s2.ray_trace(0)   # recording is off again
+    s2.close()
