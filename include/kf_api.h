@@ -147,6 +147,20 @@ kf_status kf_session_reset(kf_session* s);
  * The call synchronizes the stream before returning. */
 kf_status kf_process_frame(kf_session* s, const uint16_t* depth, int is_device_ptr,
                            void* stream, float pose_out[16]);
+/* Streaming form of kf_process_frame: submit queues a frame (host memory, or device memory
+ * when is_device_ptr = 1) and returns without waiting; wait returns the oldest submitted
+ * frame's pose and statistics (and its status), blocking until that frame is done.  Up to
+ * KF_MAX_FRAMES_IN_FLIGHT frames may be submitted and not yet waited for (KF_ERR_CAPACITY
+ * beyond); a host frame must stay unchanged until its wait returns.  Submitting frame k + 1
+ * before waiting for frame k hides the host's share of a frame (the call overhead, the copy
+ * set-up, the wake-up after the result) behind the device's work on frame k; the frames run
+ * in order on the stream, with the same results as kf_process_frame.  kf_process_frame
+ * returns KF_ERR_STATE while submitted frames are outstanding; kf_session_reset drops them.
+ * No counterpart in the reference (its frame loop is synchronous,
+ * project/src/kinect_fusion.cpp:55-72). */
+#define KF_MAX_FRAMES_IN_FLIGHT 4
+kf_status kf_process_frame_submit(kf_session* s, const uint16_t* depth, int is_device_ptr, void* stream);
+kf_status kf_process_frame_wait(kf_session* s, float pose_out[16], kf_frame_stats* stats);
 /* Enqueue one frame from device memory without synchronizing (for graph-replay drivers);
  * results are valid once the stream reaches this point. */
 kf_status kf_process_frame_async(kf_session* s, const uint16_t* depth_device, void* stream);

@@ -580,7 +580,7 @@ struct Engine {
         for (int l = 0; l < c.levels; ++l) {
             const LevelDev& Lv = d.lv[l];
             ray += (long long)((Lv.cw + kRayTileW - 1) / kRayTileW) * ((Lv.ch + kRayTileH - 1) / kRayTileH);
-            itiles += (long long)grid_icp * kIcpTilesPerBlock + 1;   // at most that many per level
+            itiles += (long long)kIcpGroups * kIcpTilesPerBlock + 1;   // at most that many per level
         }
         // reservations add up: every kind reserved so far may be open at once
         const long long k = count;
@@ -649,8 +649,8 @@ struct Engine {
                 // round robin, which evens out tiles of mostly invalid pixels), each at least
                 // one pipelined step of the block (kIcpMinTile pixels): small levels get few
                 // tiles, so a pass over many sessions stores few partials
-                const int per_block = std::max(1, std::min(kIcpTilesPerBlock, np / (grid_icp * kIcpMinTile)));
-                const int ntiles = grid_icp * per_block;
+                const int per_block = std::max(1, std::min(kIcpTilesPerBlock, np / (kIcpGroups * kIcpMinTile)));
+                const int ntiles = kIcpGroups * per_block;
                 int tile = (np + ntiles - 1) / ntiles;
                 tile = std::max(kIcpMinTile, (tile + 31) / 32 * 32);
                 IcpRange rg;
@@ -907,10 +907,35 @@ void level_intrinsics(const kf_config& c, int level, float k[9], float ik[9]) {
 // C ABI
 // ------------------------------------------------------------------------------------------
 // a session is a slot of an engine: its own (kf_session_create) or a batch's / server's
+// frames of one session queued by kf_process_frame_submit and not yet collected by
+// kf_process_frame_wait: each has its own pinned copy of the step's result and an event
+struct FrameRing {
+    static constexpr int kDepth = KF_MAX_FRAMES_IN_FLIGHT;
+    OutDev* out = nullptr;                 // kDepth pinned result blocks
+    GridSync* sync = nullptr;              // kDepth pinned copies of the step's wait record
+    cudaEvent_t done[kDepth] = {};
+    int head = 0, count = 0;               // oldest in-flight entry, entries in flight
+    kf_status init() {
+        KF_CK(cudaMallocHost(&out, sizeof(OutDev) * kDepth));
+        KF_CK(cudaMallocHost(&sync, sizeof(GridSync) * kDepth));
+        for (cudaEvent_t& e : done) KF_CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+        return KF_OK;
+    }
+    void destroy() {
+        if (out) cudaFreeHost(out);
+        if (sync) cudaFreeHost(sync);
+        out = nullptr;
+        sync = nullptr;
+        for (cudaEvent_t& e : done)
+            if (e) cudaEventDestroy(e);
+    }
+};
+
 struct kf_session {
     Engine* eng = nullptr;
     int slot = 0;
     bool owns = false;
+    FrameRing* ring = nullptr;   // created by the first kf_process_frame_submit
     Slot& sl() { return eng->slots[slot]; }
 };
 
@@ -1004,6 +1029,10 @@ kf_status kf_session_destroy(kf_session* s) {
     if (!s) return KF_ERR_ARG;
     if (!s->owns) return KF_ERR_STATE;   // batch / server members go with their owner
     cudaDeviceSynchronize();
+    if (s->ring) {
+        s->ring->destroy();
+        delete s->ring;
+    }
     s->eng->destroy();
     delete s->eng;
     delete s;
@@ -1013,6 +1042,7 @@ kf_status kf_session_destroy(kf_session* s) {
 kf_status kf_session_reset(kf_session* s) {
     if (!s) return KF_ERR_ARG;
     KF_CK(cudaDeviceSynchronize());
+    if (s->ring) s->ring->head = s->ring->count = 0;   // results of submitted frames are dropped
     return slot_reset(s->sl());
 }
 
@@ -1034,6 +1064,7 @@ static kf_status session_enqueue(kf_session* s, const uint16_t* depth, int is_de
 kf_status kf_process_frame(kf_session* s, const uint16_t* depth, int is_device_ptr, void* stream, float pose_out[16]) {
     NvtxRange nvtx_("kf_process_frame");
     if (!s || !depth) return KF_ERR_ARG;
+    if (s->ring && s->ring->count) return KF_ERR_STATE;   // collect submitted frames first
     cudaStream_t st = as_stream(stream);
     KF_TRY(session_enqueue(s, depth, is_device_ptr, st));
     KF_CK(cudaStreamSynchronize(st));
@@ -1042,6 +1073,54 @@ kf_status kf_process_frame(kf_session* s, const uint16_t* depth, int is_device_p
     kf_status r = s->eng->collect(want);
     if (pose_out) std::memcpy(pose_out, s->sl().pose, sizeof(float) * 16);
     return r;
+}
+
+kf_status kf_process_frame_submit(kf_session* s, const uint16_t* depth, int is_device_ptr, void* stream) {
+    NvtxRange nvtx_("kf_process_frame_submit");
+    if (!s || !depth) return KF_ERR_ARG;
+    if (!s->owns) return KF_ERR_STATE;   // a batch's or server's session steps with its owner
+    if (!s->ring) {
+        FrameRing* r = new (std::nothrow) FrameRing;
+        if (!r) return KF_ERR_ARG;
+        const kf_status st = r->init();
+        if (st != KF_OK) { r->destroy(); delete r; return st; }
+        s->ring = r;
+    }
+    FrameRing& r = *s->ring;
+    if (r.count == FrameRing::kDepth) return KF_ERR_CAPACITY;
+    cudaStream_t st = as_stream(stream);
+    const int frame_no = s->sl().frames;
+    KF_TRY(session_enqueue(s, depth, is_device_ptr, st));
+    // this frame's result, read back before a later frame's step overwrites it on the device
+    const int k = (r.head + r.count) % FrameRing::kDepth;
+    KF_CK(cudaMemcpyAsync(&r.out[k], s->eng->d_out + s->slot, sizeof(OutDev), cudaMemcpyDeviceToHost, st));
+    KF_CK(cudaMemcpyAsync(&r.sync[k], s->eng->d_sync, sizeof(GridSync), cudaMemcpyDeviceToHost, st));
+    KF_CK(cudaEventRecord(r.done[k], st));
+    r.count += 1;
+    s->sl().frames = frame_no + 1;
+    return KF_OK;
+}
+
+kf_status kf_process_frame_wait(kf_session* s, float pose_out[16], kf_frame_stats* stats_out) {
+    NvtxRange nvtx_("kf_process_frame_wait");
+    if (!s) return KF_ERR_ARG;
+    if (!s->ring || s->ring->count == 0) return KF_ERR_STATE;
+    FrameRing& r = *s->ring;
+    const int k = r.head;
+    KF_CK(cudaEventSynchronize(r.done[k]));
+    const OutDev& o = r.out[k];
+    Slot& sl = s->sl();
+    kf_frame_stats fs{};
+    fs.frame = o.frame - 1;
+    fs.status = r.sync[k].abort != 0 ? KF_ERR_TIMEOUT : o.status;
+    for (int l = 0; l < KF_MAX_LEVELS; ++l) fs.icp_iters[l] = o.iters[l];
+    r.head = (r.head + 1) % FrameRing::kDepth;
+    r.count -= 1;
+    sl.stats = fs;
+    std::memcpy(sl.pose, o.pose, sizeof(sl.pose));
+    if (pose_out) std::memcpy(pose_out, o.pose, sizeof(float) * 16);
+    if (stats_out) *stats_out = fs;
+    return kf_status(fs.status);
 }
 
 kf_status kf_process_frame_async(kf_session* s, const uint16_t* depth_device, void* stream) {

@@ -420,9 +420,10 @@ __device__ void icp_solve(const EngineView& v, int s, int level, int begin, int 
         for (int t = g; t < cnt; t += 9 * kGroups) {
             float4 p[9];
 #pragma unroll
-            for (int u = 0; u < 9; ++u)
-                p[u] = t + kGroups * u < cnt ? __ldcg(src + size_t(t + kGroups * u) * (kIcpPartialStride / 4))
-                                             : make_float4(0.f, 0.f, 0.f, 0.f);
+            for (int u = 0; u < 9; ++u) {
+                const float4* a = src + size_t(t + kGroups * u) * (kIcpPartialStride / 4);
+                p[u] = t + kGroups * u < cnt ? __ldcg(a) : make_float4(0.f, 0.f, 0.f, 0.f);
+            }
 #pragma unroll
             for (int u = 0; u < 9; ++u)
                 if (t + kGroups * u < cnt) {
@@ -592,14 +593,56 @@ __device__ void block_inclusive_scan(int* a, int n, int* warp_tot) {
 constexpr int kIcpMaxSessionsSmem = 1024;
 constexpr int kIcpPixelsPerStep = 4;   // pixels a thread carries through one pipelined step
 
+// Phase A of one group: tiles g, g + G, ... of a session at one level, accumulated by the whole
+// block in tile order (each thread its pixels p0 + tid, p0 + tid + 256, ... of each tile), then
+// reduced to one compensated partial at `out`.  The partial depends on the group's tiles only,
+// not on which block or launch computes it.
+__device__ __forceinline__ void icp_group(const EngineView& v, int s, int lvl, int tile0, int ntiles, int g, int G,
+                                          const float* mats, float* red, float* out) {
+    float acc[32];
+#pragma unroll
+    for (int q = 0; q < 32; ++q) acc[q] = 0.f;
+    const SessionDev* S = &v.sess[s];
+    const LevelDev& Lv = S->lv[lvl];
+    const float4* vm = S->vmap[lvl];
+    const float4* tv = S->pv[lvl];
+    const float4* tn = S->pn[lvl];
+    uint8_t* mask = S->mask[lvl];
+    const float dist = S->dist_th, ang = S->angle_cos;
+    const IcpMats m{mats, mats + 9, mats + 12, mats + 21};
+    for (int j = g; j < ntiles; j += G) {
+        const IcpTile T = v.itiles[tile0 + j];
+        const int pend = T.p0 + T.np;
+#pragma unroll 1
+        for (int p = T.p0 + threadIdx.x; p < pend; p += kIcpPixelsPerStep * kIcpThreads)
+            icp_multi<kIcpPixelsPerStep>(vm, tv, tn, Lv.w, Lv.h, Lv.icw, p, pend, m, dist, ang, mask,
+                                         [&](const float (&a)[6], float b) { accumulate_products(acc, a, b); });
+    }
+    block_reduce_store(acc, red, out);
+}
+
+// thread 0: the block-local state goes back to the session's pose block
+__device__ void store_local_state(PoseDev* P, const IcpLocal& L, bool first) {
+    if (!first) {   // a first frame has no estimate (fusion only)
+        for (int q = 0; q < 9; ++q) P->R[q] = L.R[q];
+        for (int q = 0; q < 3; ++q) P->t[q] = L.t[q];
+    }
+    for (int l = 0; l < kMaxLevels; ++l) P->iters[l] = L.iters[l];
+    P->it = L.it;
+    P->level = L.level;
+    P->cont = L.cont;
+    P->status = L.status;
+}
+
 template <bool local>
 __global__ void __launch_bounds__(kIcpThreads, 1) icp_kernel(EngineView v) {
     __shared__ float red[8 * 32 * 2];
     __shared__ double dsm[(kIcpThreads / 14 + 1) * 28];
     __shared__ float mats[24];
-    __shared__ int s_pre[kIcpMaxSessionsSmem + 1];   // tiles of sessions before s in this pass
+    __shared__ int s_pre[kIcpMaxSessionsSmem + 1];   // groups of sessions before s in this pass
     __shared__ short s_lvl[kIcpMaxSessionsSmem];
     __shared__ int s_beg[kIcpMaxSessionsSmem];
+    __shared__ int s_cnt[kIcpMaxSessionsSmem];       // tiles of session s at its level
     __shared__ int s_wtot[kIcpThreads / 32];
     __shared__ IcpLocal loc;
     const int tid = threadIdx.x;
@@ -624,12 +667,13 @@ __global__ void __launch_bounds__(kIcpThreads, 1) icp_kernel(EngineView v) {
 
     for (int pass = 0; pass < kIcpMaxPasses; ++pass) {
         float* const parts = (local && (pass & 1)) ? v.partials2 : v.partials;
-        // which sessions iterate in this pass, at which level, with which tiles
+        // which sessions iterate in this pass, at which level, with which tiles and groups
         for (int s = tid; s < S_cap; s += blockDim.x) {
             const int4 e = local ? loc.sched : __ldcg(v.icp_sched + s);
             s_lvl[s] = short(e.x);
             s_beg[s] = e.y;
-            s_pre[s + 1] = e.x >= 0 ? e.z : 0;
+            s_cnt[s] = e.z;
+            s_pre[s + 1] = e.x >= 0 ? min(e.z, kIcpGroups) : 0;
         }
         if (tid == 0) s_pre[0] = 0;
         __syncthreads();
@@ -637,64 +681,38 @@ __global__ void __launch_bounds__(kIcpThreads, 1) icp_kernel(EngineView v) {
         const int total = s_pre[S_cap];
         if (total == 0) break;   // block-uniform: every block reads the same schedule
 
-        // phase A: tiles of every iterating session, round robin over the grid.  A block
-        // accumulates all its tiles of a session and stores one partial, in slot j mod grid
-        // of the session (j: the session's tile index), so a session's partials and their
-        // summation order depend on its own tiles only, not on the other sessions of a batch.
+        // phase A: the groups of every iterating session, round robin over the grid; group g of
+        // session s stores its partial in slot g of the session's tiles
         {
-            int run_s = -1, run_slot = 0;
-            float acc[32];
-#pragma unroll
-            for (int q = 0; q < 32; ++q) acc[q] = 0.f;
+            int cur_s = -1;
             for (int vt = blockIdx.x; vt < total; vt += gridDim.x) {
                 int lo = 0, hi = S_cap;
                 while (hi - lo > 1) {
                     const int mid = (lo + hi) >> 1;
                     if (s_pre[mid] <= vt) lo = mid; else hi = mid;
                 }
-                const int s = lo, lvl = s_lvl[s];
-                if (s != run_s) {
-                    if (run_s >= 0) {
-                        block_reduce_store(acc, red, parts + size_t(s_beg[run_s] + run_slot) * kIcpPartialStride);
-#pragma unroll
-                        for (int q = 0; q < 32; ++q) acc[q] = 0.f;
-                    }
-                    run_s = s;
-                    run_slot = vt - s_pre[s];
+                const int s = lo, lvl = s_lvl[s], g = vt - s_pre[s];
+                if (s != cur_s) {
+                    cur_s = s;
+                    __syncthreads();   // the previous group's threads are done with mats
                     if (tid < 24) mats[tid] = local ? loc.mats[tid] : ldcg(v.icp_mats + size_t(s) * 24 + tid);
                     __syncthreads();
                 }
-                const IcpTile T = v.itiles[s_beg[s] + (vt - s_pre[s])];
-                const SessionDev* S = &v.sess[s];
-                const LevelDev& Lv = S->lv[lvl];
-                const float4* vm = S->vmap[lvl];
-                const float4* tv = S->pv[lvl];
-                const float4* tn = S->pn[lvl];
-                uint8_t* mask = S->mask[lvl];
-                const float dist = S->dist_th, ang = S->angle_cos;
-                const IcpMats m{mats, mats + 9, mats + 12, mats + 21};
-                const int pend = T.p0 + T.np;
-#pragma unroll 1
-                for (int p = T.p0 + tid; p < pend; p += kIcpPixelsPerStep * kIcpThreads)
-                    icp_multi<kIcpPixelsPerStep>(vm, tv, tn, Lv.w, Lv.h, Lv.icw, p, pend, m, dist, ang, mask,
-                                                 [&](const float (&a)[6], float b) { accumulate_products(acc, a, b); });
+                icp_group(v, s, lvl, s_beg[s], s_cnt[s], g, kIcpGroups, mats, red,
+                                 parts + size_t(s_beg[s] + g) * kIcpPartialStride);
             }
-            if (run_s >= 0)
-                block_reduce_store(acc, red, parts + size_t(s_beg[run_s] + run_slot) * kIcpPartialStride);
         }
         if (!grid_barrier(v.sync, nb, epoch)) return;
 
         if constexpr (local) {
             // phase B in every block, on its own copy of the state
-            if (s_lvl[0] >= 0)
-                icp_solve<true>(v, 0, s_lvl[0], s_beg[0], min(s_pre[1] - s_pre[0], int(gridDim.x)), dsm, parts, &loc);
+            if (s_lvl[0] >= 0) icp_solve<true>(v, 0, s_lvl[0], s_beg[0], s_pre[1], dsm, parts, &loc);
             __syncthreads();
         } else {
             // phase B: the block that owns a session solves it
             for (int s = blockIdx.x; s < S_cap; s += gridDim.x) {
                 if (s_lvl[s] < 0) continue;
-                icp_solve<false>(v, s, s_lvl[s], s_beg[s], min(s_pre[s + 1] - s_pre[s], int(gridDim.x)), dsm,
-                                 parts, nullptr);
+                icp_solve<false>(v, s, s_lvl[s], s_beg[s], s_pre[s + 1] - s_pre[s], dsm, parts, nullptr);
                 __syncthreads();
             }
             if (!grid_barrier(v.sync, nb, epoch)) return;
@@ -704,16 +722,7 @@ __global__ void __launch_bounds__(kIcpThreads, 1) icp_kernel(EngineView v) {
     if constexpr (local) {
         // block 0 stores the state the rest of the frame and the host read
         if (blockIdx.x == 0 && tid == 0 && v.step[0].active) {
-            PoseDev* P = v.sess[0].pose;
-            if (!v.step[0].first) {   // a first frame has no estimate (fusion only)
-                for (int q = 0; q < 9; ++q) P->R[q] = loc.R[q];
-                for (int q = 0; q < 3; ++q) P->t[q] = loc.t[q];
-            }
-            for (int l = 0; l < kMaxLevels; ++l) P->iters[l] = loc.iters[l];
-            P->it = loc.it;
-            P->level = loc.level;
-            P->cont = loc.cont;
-            P->status = loc.status;
+            store_local_state(v.sess[0].pose, loc, v.step[0].first != 0);
             icp_finish(&v.sess[0], v.step[0], v.out);
         }
     } else {

@@ -173,22 +173,43 @@ __device__ __forceinline__ float raw_to_half_value(uint16_t u) {
 __device__ __forceinline__ float load_f(const float* f, size_t i) { return __ldg(f + i); }
 __device__ __forceinline__ float load_f(const __half* f, size_t i) { return __half2float(__ldg(f + i)); }
 
-// trilinear sample of the distance array at texel coordinates (x, y, z) (already
-// uvw * n - 0.5), taps clamped to [0, n-1]: what tex3D<float2>(...).x returns with
-// normalized coordinates, linear filtering and clamp addressing
-// (project/src/voxel_grid.cpp:24-33), computed with exact float weights.
-template <class TF>
-__device__ __forceinline__ float trilinear(const TF* f, int n, float x, float y, float z) {
+// The base voxel of a trilinear sample at texel coordinates (x, y, z) (already uvw * n - 0.5):
+// the low taps clamped to [0, n-1], the fractional weights, and whether the high tap is the
+// next voxel along each axis or the same one (index below 0, or at n-1 and above, where
+// clamping makes both taps equal).
+struct TexelBase {
+    float ax, ay, az;
+    int x0, y0, z0;
+    bool hx, hy, hz;
+};
+
+__device__ __forceinline__ TexelBase texel_base(int n, float x, float y, float z) {
+    TexelBase b;
     const float fx = floorf(x), fy = floorf(y), fz = floorf(z);
-    const float ax = x - fx, ay = y - fy, az = z - fz;
+    b.ax = x - fx;
+    b.ay = y - fy;
+    b.az = z - fz;
     const int ix = int(fx), iy = int(fy), iz = int(fz);
-    // the low tap clamps to [0, n-1]; the high tap is the next voxel, or the same one where
-    // clamping makes both taps equal (index below 0 or at n-1 and above)
-    const int x0 = min(max(ix, 0), n - 1), y0 = min(max(iy, 0), n - 1), z0 = min(max(iz, 0), n - 1);
-    const int dx = unsigned(ix) < unsigned(n - 1) ? 1 : 0;
-    const int dy = unsigned(iy) < unsigned(n - 1) ? n : 0;
-    const int dz = unsigned(iz) < unsigned(n - 1) ? n * n : 0;
-    const TF* p00 = f + ((size_t(z0) * unsigned(n) + unsigned(y0)) * unsigned(n) + unsigned(x0));
+    b.x0 = min(max(ix, 0), n - 1);
+    b.y0 = min(max(iy, 0), n - 1);
+    b.z0 = min(max(iz, 0), n - 1);
+    b.hx = unsigned(ix) < unsigned(n - 1);
+    b.hy = unsigned(iy) < unsigned(n - 1);
+    b.hz = unsigned(iz) < unsigned(n - 1);
+    return b;
+}
+
+// trilinear sample of the distance array from its base voxel: what tex3D<float2>(...).x
+// returns with normalized coordinates, linear filtering and clamp addressing
+// (project/src/voxel_grid.cpp:24-33), computed with exact float weights.  n^3 < 2^32, so the
+// offsets are 32-bit.
+template <class TF>
+__device__ __forceinline__ float trilinear_at(const TF* f, int n, const TexelBase& b) {
+    const unsigned int un = unsigned(n);
+    const TF* p00 = f + ((unsigned(b.z0) * un + unsigned(b.y0)) * un + unsigned(b.x0));
+    const int dx = b.hx ? 1 : 0;
+    const unsigned int dy = b.hy ? un : 0u;
+    const unsigned int dz = b.hz ? un * un : 0u;
     const TF* p10 = p00 + dy;
     const TF* p01 = p00 + dz;
     const TF* p11 = p01 + dy;
@@ -198,14 +219,20 @@ __device__ __forceinline__ float trilinear(const TF* f, int n, float x, float y,
     const float v011 = load_f(p11, 0), v111 = load_f(p11, dx);
     // each lerp a (1 - w) + b w as one rounded product and one fused multiply-add, spelled
     // out so every kernel that samples the volume rounds identically
-    const float bx = __fsub_rn(1.f, ax), by = __fsub_rn(1.f, ay), bz = __fsub_rn(1.f, az);
-    const float c00 = __fmaf_rn(v100, ax, __fmul_rn(v000, bx));
-    const float c10 = __fmaf_rn(v110, ax, __fmul_rn(v010, bx));
-    const float c01 = __fmaf_rn(v101, ax, __fmul_rn(v001, bx));
-    const float c11 = __fmaf_rn(v111, ax, __fmul_rn(v011, bx));
-    const float c0 = __fmaf_rn(c10, ay, __fmul_rn(c00, by));
-    const float c1 = __fmaf_rn(c11, ay, __fmul_rn(c01, by));
-    return __fmaf_rn(c1, az, __fmul_rn(c0, bz));
+    const float bx = __fsub_rn(1.f, b.ax), by = __fsub_rn(1.f, b.ay), bz = __fsub_rn(1.f, b.az);
+    const float c00 = __fmaf_rn(v100, b.ax, __fmul_rn(v000, bx));
+    const float c10 = __fmaf_rn(v110, b.ax, __fmul_rn(v010, bx));
+    const float c01 = __fmaf_rn(v101, b.ax, __fmul_rn(v001, bx));
+    const float c11 = __fmaf_rn(v111, b.ax, __fmul_rn(v011, bx));
+    const float c0 = __fmaf_rn(c10, b.ay, __fmul_rn(c00, by));
+    const float c1 = __fmaf_rn(c11, b.ay, __fmul_rn(c01, by));
+    return __fmaf_rn(c1, b.az, __fmul_rn(c0, bz));
+}
+
+// trilinear sample at texel coordinates (x, y, z)
+template <class TF>
+__device__ __forceinline__ float trilinear(const TF* f, int n, float x, float y, float z) {
+    return trilinear_at(f, n, texel_base(n, x, y, z));
 }
 
 // globaltimer (ns) for bounded waits

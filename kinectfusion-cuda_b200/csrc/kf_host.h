@@ -58,7 +58,12 @@ constexpr int kRayTileW = 8, kRayTileH = 4;   // one warp per ray tile
 constexpr int kIcpThreads = 256;
 constexpr int kIcpPxPerThread = 8;
 constexpr int kIcpTilePx = kIcpThreads * kIcpPxPerThread;   // rows per block of the LLS stage
-constexpr int kIcpTilesPerBlock = 4;  // ICP tiles per session-level per block of the grid
+constexpr int kIcpTilesPerBlock = 4;  // ICP tiles per session-level per group
+// A session-level's ICP tiles form kIcpGroups groups (group g: tiles g, g + G, g + 2 G, ...);
+// each group is accumulated by one block into one partial, and the partials are combined in
+// group order.  G is a constant -- not the launch's grid -- so that a session's arithmetic is
+// the same in any grid, batch or tuning.
+constexpr int kIcpGroups = 148;
 constexpr int kIcpMinTile = kIcpThreads * 4;   // smallest ICP tile: 4 pixels per thread
 constexpr int kIcpPartialStride = 56; // floats per ICP tile partial: 27 (sum, compensation) pairs + pad
 constexpr int kIcpMaxPasses = 64;     // hard cap on ICP passes per frame

@@ -212,6 +212,25 @@ class KinectFusion:
             raise KfError(st, "kf_process_frame")
         return st, from_colmajor(pose, 4)
 
+    def submit_frame(self, depth, stream=None):
+        """Queue a frame without waiting (kf_process_frame_submit): an (h, w) uint16 numpy
+        array that stays unchanged until its wait_frame returns, or a torch CUDA tensor."""
+        if hasattr(depth, "is_cuda") and depth.is_cuda:
+            st = lib.kf_process_frame_submit(self._s, _dev_ptr(depth), 1, _stream(stream))
+        else:
+            if depth.shape != (self.h, self.w) or depth.dtype != np.uint16 or not depth.flags.c_contiguous:
+                raise ValueError("depth frame must be a contiguous %dx%d uint16 array" % (self.h, self.w))
+            st = lib.kf_process_frame_submit(self._s, _np_ptr(depth), 0, _stream(stream))
+        check(st, "kf_process_frame_submit")
+
+    def wait_frame(self):
+        """(status, pose 4x4) of the oldest submitted frame (kf_process_frame_wait)."""
+        pose = (ctypes.c_float * 16)()
+        st = lib.kf_process_frame_wait(self._s, pose, None)
+        if st not in (KF_OK, KF_ERR_NONFINITE):
+            raise KfError(st, "kf_process_frame_wait")
+        return st, from_colmajor(pose, 4)
+
     def startTracking(self, frames):
         """Run every frame of an iterable (the reference reads them from a dataset,
         project/src/kinect_fusion.cpp:44-73); returns the list of poses."""

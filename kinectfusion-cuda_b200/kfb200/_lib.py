@@ -28,6 +28,7 @@ KF_RENDER_NORMALS = 0
 KF_RENDER_SHADING = 1
 KF_DEBUG_RAY_TRACE = 1
 KF_DEBUG_NO_GRAPH = 2
+KF_MAX_FRAMES_IN_FLIGHT = 4
 
 KF_TSDF_F32F32 = 0
 KF_TSDF_F16U16 = 1
@@ -96,6 +97,8 @@ SIGNATURES = {
     "kf_session_reset": (_I, [_P]),
     "kf_process_frame": (_I, [_P, _P, _I, _P, _FP]),
     "kf_process_frame_async": (_I, [_P, _P, _P]),
+    "kf_process_frame_submit": (_I, [_P, _P, _I, _P]),
+    "kf_process_frame_wait": (_I, [_P, _FP, ctypes.POINTER(KfFrameStats)]),
     "kf_get_pose": (_I, [_P, _FP]),
     "kf_set_pose": (_I, [_P, _FP]),
     "kf_get_frame_stats": (_I, [_P, ctypes.POINTER(KfFrameStats)]),

@@ -299,3 +299,34 @@ def test_debug_modes_change_no_result(kf, run_small):
     with pytest.raises(kf.KfError):
         s2.ray_trace(0)   # recording is off again
     s2.close()
+
+
+def test_submitted_frames_equal_synchronous_frames(kf, cuda, run_small):
+    """Frames queued with kf_process_frame_submit (host and device frames, up to the in-flight
+    limit ahead) give the poses of kf_process_frame, bit for bit, in order; one frame beyond the
+    limit is refused, and a synchronous call waits for the queue to be collected."""
+    cfg, imgs, s, P, rows = run_small
+    s2 = kf.KinectFusion(cfg)
+    pinned = [cuda.from_numpy(im.view(np.int16)).pin_memory() for im in imgs]
+    host = [p.numpy().view(np.uint16) for p in pinned]
+    depth = kf._lib.KF_MAX_FRAMES_IN_FLIGHT
+    got, nxt = [], 0
+    for _ in range(depth):
+        s2.submit_frame(host[nxt] if nxt % 2 == 0 else cuda.from_numpy(imgs[nxt].view(np.int16)).cuda())
+        nxt += 1
+    with pytest.raises(kf.KfError) as e:
+        s2.submit_frame(host[nxt])
+    assert e.value.status == kf.KF_ERR_CAPACITY
+    with pytest.raises(kf.KfError) as e:
+        s2.process_frame(host[nxt])
+    assert e.value.status == kf.KF_ERR_STATE
+    while len(got) < len(imgs):
+        got.append(s2.wait_frame()[1])
+        if nxt < len(imgs):
+            s2.submit_frame(host[nxt])
+            nxt += 1
+    for i, pose in enumerate(got):
+        np.testing.assert_array_equal(pose, rows[i][2])
+    assert s2.frame_stats()["frame"] == len(imgs) - 1
+    st, pose = s2.process_frame(host[0])   # the queue is empty again
+    s2.close()
