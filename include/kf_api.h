@@ -340,8 +340,23 @@ kf_status kf_batch_step_async(kf_batch* b, const int* active, void* stream);
 /* Device address of session i's uint16 input frame buffer (w*h elements). */
 kf_status kf_batch_input_buffer(kf_batch* b, int i, uint16_t** dev_ptr);
 kf_status kf_batch_session(kf_batch* b, int i, kf_session** out);
-/* Choose block shapes per stage by timing candidates on this batch's own data. */
-kf_status kf_batch_autotune(kf_batch* b, void* stream, char* report, size_t report_bytes);
+/* Tune the batch's launch shapes on its own live steps.  The shapes are the persistent grid of
+ * every stage, the raycast kernel's form (3 or 4 blocks per SM), the number of march iterations
+ * a lane takes before it hands a long ray to a warp, the ray tile (8 x 4, 16 x 2 or 4 x 8
+ * pixels per warp) and how fusion splits its queue entries; none of them changes a result, bit
+ * for bit.  After this call each kf_batch_step runs one candidate shape and its stage times
+ * (device events) are recorded; a walk over the parameters, one at a time, keeps the fastest
+ * candidate of each, and after the last step of the walk the batch keeps the chosen shape.
+ * cache_path (may be NULL): a JSON file of chosen shapes keyed by the batch's session mix
+ * (frame sizes, volumes, formats, counts) and the device's SM count; if it holds an entry for
+ * this mix, that shape is applied at once and no step is spent tuning, else the walk's result
+ * is added to it.  kf_batch_step_async steps do not advance the walk.  The reference has no
+ * counterpart (its launch shapes are fixed 8 x 8 blocks). */
+kf_status kf_batch_autotune_start(kf_batch* b, const char* cache_path);
+/* Steps the walk still needs (0 when done or not started) and a JSON report: the mix key, the
+ * source of the shape ("tuned" or "cache") and the shape, with each parameter's winning stage
+ * time when tuned. */
+kf_status kf_batch_autotune_status(kf_batch* b, int* steps_left, char* report, size_t report_bytes);
 
 /* ------------------------------------------------------------------------------------------ */
 /* server: continuous batching of concurrent sessions with HBM-budget admission              */

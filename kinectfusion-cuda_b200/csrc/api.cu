@@ -385,6 +385,52 @@ kf_status grow(T*& ptr, int& cap, int need) {
     return KF_OK;
 }
 
+// Launch shapes of a step.  Every value gives the same results bit for bit -- they only change
+// which block or lane does which part of the work -- so they can be tuned on live steps.
+struct Shape {
+    int grid_pre = 0, grid_ray = 0, grid_fuse = 0, grid_brick = 0, grid_icp = 0;
+    int ray_form = 0;     // 0: by the ray-tile count (many_ray_tiles); 3 or 4: the raycast kernel's
+                          // form with that many blocks per SM
+    int ray_budget = 0;   // 0: by the ray-tile count (serial_budget); else march iterations a lane
+                          // takes before queueing its ray for a warp
+    int ray_tw = kRayTileW;   // ray tile width (32 / ray_tw rows)
+    int fuse_split = 0;   // 0: by the queue length (fuse_split); 1, 2, 4: entries whole, halves, quarters
+    bool operator==(const Shape& o) const {
+        return grid_pre == o.grid_pre && grid_ray == o.grid_ray && grid_fuse == o.grid_fuse &&
+               grid_brick == o.grid_brick && grid_icp == o.grid_icp && ray_form == o.ray_form &&
+               ray_budget == o.ray_budget && ray_tw == o.ray_tw && fuse_split == o.fuse_split;
+    }
+    bool operator!=(const Shape& o) const { return !(*this == o); }
+};
+
+// The autotuner's walk over the shapes: coordinate descent, one parameter at a time, each
+// candidate run on kReps live steps and timed by the stage events of those steps (the smallest
+// time counts); the winner of each parameter is kept for the next.
+struct Tuner {
+    static constexpr int kReps = 2;
+    struct Param {
+        const char* name;
+        int stage;            // 0 preprocess, 1 raycast, 2 ICP, 3 fusion
+        int Shape::*field;
+        std::vector<int> cand;
+    };
+    bool active = false;
+    bool done = false;
+    bool was_profiling = false;
+    std::string cache_path, key;
+    std::vector<Param> params;
+    int pi = 0, ci = 0, rep = 0;
+    std::vector<float> best;      // per candidate of the current parameter
+    Shape base;                   // the shape the walk has settled on so far
+    std::string report;           // JSON of the chosen shape and the stage times behind it
+    int steps_left() const {
+        if (!active) return 0;
+        int n = (int(params[pi].cand.size()) - ci) * kReps - rep;
+        for (size_t q = pi + 1; q < params.size(); ++q) n += int(params[q].cand.size()) * kReps;
+        return n;
+    }
+};
+
 struct Engine {
     int sms = 148;
     int cap = 0;
@@ -423,7 +469,8 @@ struct Engine {
     Tables tb{};
     bool tables_dirty = true;
     bool step_dirty = true;
-    int grid_pre = 1, grid_ray = 1, grid_icp = 1, grid_fuse = 1, grid_brick = 1;
+    Shape shape;
+    Tuner tuner;
     // graph
     bool use_graph = true;
     bool graph_dirty = true;
@@ -438,7 +485,7 @@ struct Engine {
     // ev_input (an external event wait node), recorded after every step's copies
     bool input_wait = true;
     bool capturing = false;   // record() runs inside a stream capture (the wait becomes a node)
-    bool ray_many = false;    // the step has many ray tiles: the raycast kernel's 4-block form
+    bool ray_many = false;    // the raycast kernel's 4-block form (shape.ray_form, else the tile-count rule)
     cudaStream_t h2d_stream = nullptr;
     cudaEvent_t ev_input = nullptr, ev_prev = nullptr;
     bool stages[4] = {true, true, true, true};
@@ -484,12 +531,12 @@ struct Engine {
         KF_CK(cudaStreamCreateWithFlags(&h2d_stream, cudaStreamNonBlocking));
         KF_CK(cudaEventCreateWithFlags(&ev_input, cudaEventDisableTiming));
         KF_CK(cudaEventCreateWithFlags(&ev_prev, cudaEventDisableTiming));
-        // persistent grids (kf_batch_autotune may replace the first, second and fourth)
-        grid_pre = sms * 4;
-        grid_ray = sms * 6;
-        grid_fuse = sms * 4;
-        grid_brick = sms * 4;
-        grid_icp = icp_max_grid(sms);
+        // persistent grids (the autotuner may replace them)
+        shape.grid_pre = sms * 4;
+        shape.grid_ray = sms * 6;
+        shape.grid_fuse = sms * 4;
+        shape.grid_brick = sms * 4;
+        shape.grid_icp = icp_max_grid(sms);
         return KF_OK;
     }
 
@@ -514,6 +561,16 @@ struct Engine {
         if (profile != on) graph_dirty = true;
         profile = on;
         return KF_OK;
+    }
+
+    // switch to launch shape `to` for the next steps (callers hold the engine, stream idle)
+    void set_shape(const Shape& to) {
+        if (to == shape) return;
+        if (to.ray_tw != shape.ray_tw || to.ray_budget != shape.ray_budget || to.fuse_split != shape.fuse_split ||
+            to.ray_form != shape.ray_form)
+            tables_dirty = true;
+        shape = to;
+        graph_dirty = true;
     }
 
     // durations of the four stages of the last completed step (ms); the preprocess runs beside
@@ -579,7 +636,8 @@ struct Engine {
         pre = (long long)((c.width + kPreTileSize - 1) / kPreTileSize) * ((c.height + kPreTileSize - 1) / kPreTileSize);
         for (int l = 0; l < c.levels; ++l) {
             const LevelDev& Lv = d.lv[l];
-            ray += (long long)((Lv.cw + kRayTileW - 1) / kRayTileW) * ((Lv.ch + kRayTileH - 1) / kRayTileH);
+            // tiles of the narrowest shape the tuner tries (4 x 8) bound every shape's count
+            ray += (long long)((Lv.cw + 3) / 4) * ((Lv.ch + 7) / 8);
             itiles += (long long)kIcpGroups * kIcpTilesPerBlock + 1;   // at most that many per level
         }
         // reservations add up: every kind reserved so far may be open at once
@@ -635,8 +693,9 @@ struct Engine {
                     for (int x = 0; x < c.width; x += kPreTileSize) pre.push_back(PreTile{s, x, y});
                 for (int l = 0; l < c.levels; ++l) {
                     const LevelDev& Lv = sl.d.lv[l];
-                    for (int y = 0; y < Lv.ch; y += kRayTileH)
-                        for (int x = 0; x < Lv.cw; x += kRayTileW) ray.push_back(RayTile{s, l, x, y});
+                    const int tw = shape.ray_tw, th = 32 / shape.ray_tw;
+                    for (int y = 0; y < Lv.ch; y += th)
+                        for (int x = 0; x < Lv.cw; x += tw) ray.push_back(RayTile{s, l, x, y});
                 }
                 fprefix[s + 1] += fuse_units(c.volume_n);
                 bprefix[s + 1] += (long long)sl.d.nb * sl.d.nb * sl.d.nb;
@@ -697,9 +756,12 @@ struct Engine {
         tb.S = cap;
         tb.n_pre = int(pre.size());
         tb.n_ray = int(ray.size());
-        tb.ray_budget = serial_budget(tb.n_ray);
-        if (ray_many != many_ray_tiles(tb.n_ray)) graph_dirty = true;
-        ray_many = many_ray_tiles(tb.n_ray);
+        tb.ray_budget = shape.ray_budget ? shape.ray_budget : serial_budget(tb.n_ray);
+        tb.ray_tw = shape.ray_tw;
+        tb.fuse_split = shape.fuse_split;
+        const bool many = shape.ray_form ? shape.ray_form == 4 : many_ray_tiles(tb.n_ray);
+        if (ray_many != many) graph_dirty = true;
+        ray_many = many;
         for (int l = 0; l < KF_MAX_LEVELS; ++l) {
             tb.n_itiles[l] = int(it[l].size());
             tb.icp_off[l] = off[l];
@@ -726,30 +788,30 @@ struct Engine {
             KF_CK(cudaStreamWaitEvent(aux_stream, ev_fork, 0));
             if (input_wait) KF_CK(cudaStreamWaitEvent(aux_stream, ev_input, capturing ? cudaEventWaitExternal : 0));
             NvtxRange r("kf.preprocess");
-            KF_CK(launch_preprocess(v, grid_pre, aux_stream));
+            KF_CK(launch_preprocess(v, shape.grid_pre, aux_stream));
             if (profile) KF_CK(cudaEventRecordWithFlags(ev[1], aux_stream, cudaEventRecordExternal));
             KF_CK(cudaEventRecord(ev_join, aux_stream));
         } else {
             if (stages[0] && input_wait) KF_CK(cudaStreamWaitEvent(st, ev_input, capturing ? cudaEventWaitExternal : 0));
             NvtxRange r("kf.preprocess");
-            if (stages[0]) KF_CK(launch_preprocess(v, grid_pre, st));
+            if (stages[0]) KF_CK(launch_preprocess(v, shape.grid_pre, st));
             if (profile) KF_CK(cudaEventRecordWithFlags(ev[1], st, cudaEventRecordExternal));
         }
         {
             NvtxRange r("kf.raycast");
-            if (stages[1]) KF_CK(launch_raycast(v, grid_ray, st, ray_many));
+            if (stages[1]) KF_CK(launch_raycast(v, shape.grid_ray, st, ray_many));
         }
         if (fork) KF_CK(cudaStreamWaitEvent(st, ev_join, 0));
         if (profile) KF_CK(cudaEventRecordWithFlags(ev[2], st, cudaEventRecordExternal));
         {
             NvtxRange r("kf.icp");
-            if (stages[2]) KF_CK(launch_icp(v, grid_icp, st, cap == 1));
+            if (stages[2]) KF_CK(launch_icp(v, shape.grid_icp, st, cap == 1));
         }
         if (profile) KF_CK(cudaEventRecordWithFlags(ev[3], st, cudaEventRecordExternal));
         {
             NvtxRange r("kf.fusion");
-            if (stages[3]) KF_CK(launch_fuse(v, grid_fuse, st));
-            if (stages[3]) KF_CK(launch_bricks(v, grid_brick, st));
+            if (stages[3]) KF_CK(launch_fuse(v, shape.grid_fuse, st));
+            if (stages[3]) KF_CK(launch_bricks(v, shape.grid_brick, st));
         }
         if (profile) KF_CK(cudaEventRecordWithFlags(ev[4], st, cudaEventRecordExternal));
         KF_CK(cudaMemcpyAsync(h_out, d_out, sizeof(OutDev) * cap, cudaMemcpyDeviceToHost, st));
@@ -832,6 +894,10 @@ struct Engine {
         return worst;
     }
 };
+
+// the batch autotuner's step hooks (defined with the batch API below)
+kf_status tuner_before_step(Engine& e);
+kf_status tuner_after_step(Engine& e);
 
 kf_status record_ms(cudaStream_t st, cudaEvent_t a, cudaEvent_t b, float* ms) {
     KF_CK(cudaEventRecord(b, st));
@@ -1623,7 +1689,7 @@ kf_status kf_compute_pose(const float* const* vertex, const float* const* target
     StepDev step{1, 0};
     e = cudaMemcpy(eng.d_step, &step, sizeof(step), cudaMemcpyHostToDevice);
     if (e == cudaSuccess) e = cudaMemsetAsync(eng.d_sync, 0, sizeof(GridSync), s);
-    if (e == cudaSuccess) e = launch_icp(eng.view(), eng.grid_icp, s, eng.cap == 1);
+    if (e == cudaSuccess) e = launch_icp(eng.view(), eng.shape.grid_icp, s, eng.cap == 1);
     if (e == cudaSuccess) e = cudaMemcpyAsync(eng.h_out, eng.d_out, sizeof(OutDev), cudaMemcpyDeviceToHost, s);
     if (e == cudaSuccess) e = cudaMemcpyAsync(eng.h_sync, eng.d_sync, sizeof(GridSync), cudaMemcpyDeviceToHost, s);
     if (e == cudaSuccess) e = cudaStreamSynchronize(s);
@@ -1688,6 +1754,7 @@ kf_status kf_batch_step(kf_batch* b, const uint16_t* const* depth, int is_device
         want[i] = StepDev{depth[i] ? 1 : 0, sl.frames == 0 ? 1 : 0};
     }
     KF_TRY(b->eng.set_step(want, st));
+    KF_TRY(tuner_before_step(b->eng));
     cudaStream_t cs = st;
     KF_TRY(b->eng.begin_inputs(!is_device_ptr, st, &cs));
     for (int i = 0; i < b->n; ++i) {
@@ -1700,6 +1767,7 @@ kf_status kf_batch_step(kf_batch* b, const uint16_t* const* depth, int is_device
     KF_TRY(b->eng.enqueue(st));
     KF_CK(cudaStreamSynchronize(st));
     kf_status r = b->eng.collect(want);
+    KF_TRY(tuner_after_step(b->eng));
     if (poses_out)
         for (int i = 0; i < b->n; ++i) std::memcpy(poses_out + 16 * size_t(i), b->eng.slots[i].pose, sizeof(float) * 16);
     return r;
@@ -1731,32 +1799,161 @@ kf_status kf_batch_input_buffer(kf_batch* b, int i, uint16_t** dev_ptr) {
 // ------------------------------------------------------------------------------------------
 namespace {
 
-// time one stage of a step (ms, device events) with the given grid
-kf_status time_stage(Engine& e, int stage, int grid, cudaStream_t st, int reps, float* ms) {
-    const int saved[4] = {e.grid_pre, e.grid_ray, e.grid_icp, e.grid_fuse};
-    int* target = stage == 0 ? &e.grid_pre : stage == 1 ? &e.grid_ray : stage == 2 ? &e.grid_icp : &e.grid_fuse;
-    *target = grid;
-    bool keep[4];
-    for (int q = 0; q < 4; ++q) { keep[q] = e.stages[q]; e.stages[q] = (q == stage); }
-    const bool ug = e.use_graph;
-    e.use_graph = false;
-    cudaEvent_t a, b;
-    cudaEventCreate(&a);
-    cudaEventCreate(&b);
-    kf_status r = e.record(st);   // warm-up
-    cudaEventRecord(a, st);
-    for (int i = 0; i < reps && r == KF_OK; ++i) r = e.record(st);
-    cudaEventRecord(b, st);
-    cudaEventSynchronize(b);
-    float t = 0.f;
-    cudaEventElapsedTime(&t, a, b);
-    *ms = t / float(reps);
-    cudaEventDestroy(a);
-    cudaEventDestroy(b);
-    for (int q = 0; q < 4; ++q) e.stages[q] = keep[q];
-    e.use_graph = ug;
-    e.grid_pre = saved[0]; e.grid_ray = saved[1]; e.grid_icp = saved[2]; e.grid_fuse = saved[3];
-    return r;
+// the batch's session mix: what the tuned shapes depend on (frame sizes, volumes, formats,
+// how many of each) and the device's SM count
+std::string mix_key(const Engine& e) {
+    std::vector<std::string> kinds;
+    for (const Slot& sl : e.slots) {
+        if (!sl.used) continue;
+        char buf[96];
+        std::snprintf(buf, sizeof(buf), "%dx%d/%d/%s/L%d", sl.cfg.width, sl.cfg.height, sl.cfg.volume_n,
+                      sl.cfg.tsdf_format == KF_TSDF_F16U16 ? "f16u16" : "f32f32", sl.cfg.levels);
+        kinds.emplace_back(buf);
+    }
+    std::sort(kinds.begin(), kinds.end());
+    std::string key = std::to_string(e.sms) + "sm";
+    for (size_t i = 0; i < kinds.size();) {
+        size_t j = i;
+        while (j < kinds.size() && kinds[j] == kinds[i]) ++j;
+        key += " " + kinds[i] + "*" + std::to_string(j - i);
+        i = j;
+    }
+    return key;
+}
+
+const char* const kShapeFields[] = {"grid_pre", "grid_ray", "grid_fuse", "grid_brick", "grid_icp",
+                                    "ray_form", "ray_budget", "ray_tw", "fuse_split"};
+int Shape::* const kShapeMembers[] = {&Shape::grid_pre, &Shape::grid_ray, &Shape::grid_fuse, &Shape::grid_brick,
+                                      &Shape::grid_icp, &Shape::ray_form, &Shape::ray_budget, &Shape::ray_tw,
+                                      &Shape::fuse_split};
+constexpr int kShapeFieldCount = 9;
+
+std::string shape_json(const Shape& sh) {
+    std::string j = "{";
+    for (int q = 0; q < kShapeFieldCount; ++q) {
+        j += std::string(q ? ", " : "") + "\"" + kShapeFields[q] + "\": " + std::to_string(sh.*kShapeMembers[q]);
+    }
+    return j + "}";
+}
+
+// The cache file is a JSON object with one line per session mix:
+//   "<mix key>": {"grid_pre": 592, "grid_ray": 888, ...},
+// Returns true and fills `out` when `key` has an entry.
+bool cache_lookup(const std::string& path, const std::string& key, Shape& out) {
+    FILE* f = std::fopen(path.c_str(), "r");
+    if (!f) return false;
+    char line[1024];
+    bool found = false;
+    const std::string head = "\"" + key + "\": {";
+    while (!found && std::fgets(line, sizeof(line), f)) {
+        const char* p = std::strstr(line, head.c_str());
+        if (!p) continue;
+        Shape sh = out;
+        int got = 0;
+        for (int q = 0; q < kShapeFieldCount; ++q) {
+            const std::string name = "\"" + std::string(kShapeFields[q]) + "\": ";
+            const char* v = std::strstr(p + head.size(), name.c_str());
+            int x = 0;
+            if (v && std::sscanf(v + name.size(), "%d", &x) == 1) {
+                sh.*kShapeMembers[q] = x;
+                ++got;
+            }
+        }
+        if (got == kShapeFieldCount) {
+            out = sh;
+            found = true;
+        }
+    }
+    std::fclose(f);
+    return found;
+}
+
+// add or replace the entry of `key` (other mixes' entries are kept)
+bool cache_store(const std::string& path, const std::string& key, const Shape& sh) {
+    std::vector<std::string> entries;
+    const std::string head = "\"" + key + "\": {";
+    if (FILE* f = std::fopen(path.c_str(), "r")) {
+        char line[1024];
+        while (std::fgets(line, sizeof(line), f)) {
+            std::string l(line);
+            while (!l.empty() && (l.back() == '\n' || l.back() == ',' || l.back() == ' ')) l.pop_back();
+            if (l.find("\": {") == std::string::npos || l.find(head) != std::string::npos) continue;
+            size_t start = l.find('"');
+            entries.push_back(l.substr(start));
+        }
+        std::fclose(f);
+    }
+    entries.push_back("\"" + key + "\": " + shape_json(sh));
+    const std::string tmp = path + ".tmp";
+    FILE* f = std::fopen(tmp.c_str(), "w");
+    if (!f) return false;
+    std::fprintf(f, "{\n");
+    for (size_t i = 0; i < entries.size(); ++i)
+        std::fprintf(f, "  %s%s\n", entries[i].c_str(), i + 1 < entries.size() ? "," : "");
+    std::fprintf(f, "}\n");
+    if (std::fclose(f) != 0) return false;
+    return std::rename(tmp.c_str(), path.c_str()) == 0;
+}
+
+// the candidates the walk tries, in order (grids as multiples of the SM count)
+std::vector<Tuner::Param> tuner_params(int sms) {
+    std::vector<Tuner::Param> p;
+    p.push_back({"grid_ray", 1, &Shape::grid_ray, {2 * sms, 4 * sms, 6 * sms, 8 * sms, 12 * sms, 16 * sms}});
+    p.push_back({"ray_form", 1, &Shape::ray_form, {3, 4}});
+    p.push_back({"ray_budget", 1, &Shape::ray_budget, {24, 32, 40, 48, 64, 96}});
+    p.push_back({"ray_tw", 1, &Shape::ray_tw, {8, 16, 4}});
+    p.push_back({"grid_pre", 0, &Shape::grid_pre, {1 * sms, 2 * sms, 4 * sms, 8 * sms}});
+    p.push_back({"grid_icp", 2, &Shape::grid_icp, {sms / 2, sms}});
+    p.push_back({"grid_fuse", 3, &Shape::grid_fuse, {2 * sms, 4 * sms, 6 * sms, 8 * sms}});
+    p.push_back({"fuse_split", 3, &Shape::fuse_split, {1, 2, 4}});
+    p.push_back({"grid_brick", 3, &Shape::grid_brick, {2 * sms, 4 * sms, 8 * sms}});
+    return p;
+}
+
+// before a batch step: the shape of the tuner's current candidate
+kf_status tuner_before_step(Engine& e) {
+    Tuner& t = e.tuner;
+    if (!t.active) return KF_OK;
+    Shape sh = t.base;
+    sh.*(t.params[t.pi].field) = t.params[t.pi].cand[t.ci];
+    e.set_shape(sh);
+    return KF_OK;
+}
+
+// after a batch step finished: record its stage time for the candidate and move on
+kf_status tuner_after_step(Engine& e) {
+    Tuner& t = e.tuner;
+    if (!t.active) return KF_OK;
+    float ms[4];
+    KF_TRY(e.stage_times(ms));
+    const Tuner::Param& p = t.params[t.pi];
+    t.best[t.ci] = std::min(t.best[t.ci], ms[p.stage]);
+    if (++t.rep < Tuner::kReps) return KF_OK;
+    t.rep = 0;
+    if (++t.ci < int(p.cand.size())) return KF_OK;
+    // the parameter's winner
+    int w = 0;
+    for (int c = 1; c < int(p.cand.size()); ++c)
+        if (t.best[c] < t.best[w]) w = c;
+    t.base.*(p.field) = p.cand[w];
+    char buf[96];
+    std::snprintf(buf, sizeof(buf), "%s\"%s\": [%d, %.5f]", t.report.size() > 1 ? ", " : "", p.name, p.cand[w],
+                  t.best[w]);
+    t.report += buf;
+    t.ci = 0;
+    if (++t.pi < int(t.params.size())) {
+        t.best.assign(t.params[t.pi].cand.size(), 1e30f);
+        return KF_OK;
+    }
+    // done: keep the walk's shape and remember it
+    t.active = false;
+    t.done = true;
+    e.set_shape(t.base);
+    KF_TRY(e.set_profile(t.was_profiling));
+    t.report = "{\"mix\": \"" + t.key + "\", \"source\": \"tuned\", \"shape\": " + shape_json(t.base) +
+               ", \"stage_ms\": " + t.report + "}}";
+    if (!t.cache_path.empty()) cache_store(t.cache_path, t.key, t.base);
+    return KF_OK;
 }
 
 }  // namespace
@@ -1780,82 +1977,43 @@ kf_status kf_batch_session(kf_batch* b, int i, kf_session** out) {
     return KF_OK;
 }
 
-// Pick the persistent grid of each stage by timing candidates on this batch's own frames.
-// Volumes and poses are saved first and restored afterwards, so tuning leaves the sessions
-// exactly as they were.  Every session must have processed at least one frame.
-kf_status kf_batch_autotune(kf_batch* b, void* stream, char* report, size_t report_bytes) {
-    NvtxRange nvtx_("kf_batch_autotune");
+kf_status kf_batch_autotune_start(kf_batch* b, const char* cache_path) {
+    NvtxRange nvtx_("kf_batch_autotune_start");
     if (!b) return KF_ERR_ARG;
     Engine& e = b->eng;
-    cudaStream_t st = as_stream(stream);
-    for (int i = 0; i < b->n; ++i)
-        if (e.slots[i].frames == 0) return KF_ERR_STATE;
-    KF_CK(cudaStreamSynchronize(st));
-    if (e.tables_dirty) KF_TRY(e.build_tables());
-    // all sessions take part, none on its first frame
-    std::vector<StepDev> want(b->n, StepDev{1, 0});
-    for (int s = 0; s < b->n; ++s) e.h_step[s] = want[s];
-    KF_CK(cudaMemcpy(e.d_step, e.h_step, sizeof(StepDev) * b->n, cudaMemcpyHostToDevice));
-    e.step_dirty = false;
-    // snapshot volumes and pose state
-    std::vector<void*> saved;
-    std::vector<size_t> sizes;
-    for (int i = 0; i < b->n; ++i) {
-        const Slot& sl = e.slots[i];
-        const size_t n3 = size_t(sl.cfg.volume_n) * sl.cfg.volume_n * sl.cfg.volume_n;
-        const size_t es = sl.d.fmt == KF_TSDF_F16U16 ? 2 : 4;
-        void* p = nullptr;
-        KF_CK(cudaMalloc(&p, 2 * n3 * es + sizeof(PoseDev)));
-        KF_CK(cudaMemcpy(p, sl.d.tf, n3 * es, cudaMemcpyDeviceToDevice));
-        KF_CK(cudaMemcpy(static_cast<char*>(p) + n3 * es, sl.d.tw, n3 * es, cudaMemcpyDeviceToDevice));
-        KF_CK(cudaMemcpy(static_cast<char*>(p) + 2 * n3 * es, sl.d.pose, sizeof(PoseDev), cudaMemcpyDeviceToDevice));
-        saved.push_back(p);
-        sizes.push_back(n3 * es);
-    }
-    std::string rep = "{";
-    const int sms = e.sms;
-    const int cand_pre[] = {1, 2, 4, 8};
-    const int cand_ray[] = {2, 4, 6, 8, 12, 16};
-    const int cand_fuse[] = {4, 8, 12, 16, 24};
-    const char* names[4] = {"preprocess", "raycast", "icp", "fuse"};
-    kf_status r = KF_OK;
-    for (int stage = 0; stage < 4 && r == KF_OK; ++stage) {
-        if (stage == 2) continue;   // the cooperative ICP grid is one block per SM
-        const int* cand = stage == 0 ? cand_pre : stage == 1 ? cand_ray : cand_fuse;
-        const int nc = stage == 0 ? 4 : stage == 1 ? 6 : 5;
-        float best = 1e30f;
-        int best_g = 0;
-        char buf[160];
-        for (int c = 0; c < nc && r == KF_OK; ++c) {
-            float ms = 0.f;
-            r = time_stage(e, stage, sms * cand[c], st, 5, &ms);
-            if (ms < best) { best = ms; best_g = sms * cand[c]; }
-        }
-        if (r != KF_OK) break;
-        if (stage == 0) e.grid_pre = best_g;
-        if (stage == 1) e.grid_ray = best_g;
-        if (stage == 3) e.grid_fuse = best_g;
-        snprintf(buf, sizeof(buf), "%s\"%s\": {\"grid\": %d, \"ms\": %.5f}", rep.size() > 1 ? ", " : "", names[stage],
-                 best_g, best);
-        rep += buf;
-    }
-    rep += "}";
-    // restore
-    for (int i = 0; i < b->n; ++i) {
-        const Slot& sl = e.slots[i];
-        cudaMemcpy(sl.d.tf, saved[i], sizes[i], cudaMemcpyDeviceToDevice);
-        cudaMemcpy(sl.d.tw, static_cast<char*>(saved[i]) + sizes[i], sizes[i], cudaMemcpyDeviceToDevice);
-        cudaMemcpy(sl.d.pose, static_cast<char*>(saved[i]) + 2 * sizes[i], sizeof(PoseDev), cudaMemcpyDeviceToDevice);
-        cudaFree(saved[i]);
-        launch_rebuild_bricks(sl.d.tf, sl.d.fmt, sl.cfg.volume_n, sl.d.bmin, sl.d.bdil, sl.d.sdil, 0);
-    }
+    Tuner& t = e.tuner;
     KF_CK(cudaDeviceSynchronize());
-    e.graph_dirty = true;
+    t = Tuner{};
+    t.key = mix_key(e);
+    t.cache_path = cache_path ? cache_path : "";
+    Shape cached = e.shape;
+    if (!t.cache_path.empty() && cache_lookup(t.cache_path, t.key, cached)) {
+        e.set_shape(cached);
+        t.base = cached;
+        t.done = true;
+        t.report = "{\"mix\": \"" + t.key + "\", \"source\": \"cache\", \"shape\": " + shape_json(cached) + "}";
+        return KF_OK;
+    }
+    t.params = tuner_params(e.sms);
+    t.base = e.shape;
+    t.best.assign(t.params[0].cand.size(), 1e30f);
+    t.was_profiling = e.profile;
+    KF_TRY(e.set_profile(true));
+    t.report = "{";
+    t.active = true;
+    return KF_OK;
+}
+
+kf_status kf_batch_autotune_status(kf_batch* b, int* steps_left, char* report, size_t report_bytes) {
+    if (!b) return KF_ERR_ARG;
+    const Tuner& t = b->eng.tuner;
+    if (steps_left) *steps_left = t.steps_left();
     if (report && report_bytes) {
-        std::strncpy(report, rep.c_str(), report_bytes - 1);
+        const std::string r = t.done ? t.report : t.active ? std::string("{\"source\": \"tuning\"}") : std::string("{}");
+        std::strncpy(report, r.c_str(), report_bytes - 1);
         report[report_bytes - 1] = 0;
     }
-    return r;
+    return KF_OK;
 }
 
 }  // extern "C"

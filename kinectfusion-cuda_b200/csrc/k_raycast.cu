@@ -38,6 +38,7 @@ constexpr int kSerialBudgetMany = 64;
 constexpr int kManyRayTiles = 25000;   // more ray tiles than this in a step: kSerialBudgetMany
 
 bool many_ray_tiles(int ray_tiles) { return ray_tiles > kManyRayTiles; }
+int serial_budget_many() { return kSerialBudgetMany; }
 int serial_budget(int ray_tiles) { return many_ray_tiles(ray_tiles) ? kSerialBudgetMany : kSerialBudgetSingle; }
 
 struct RayGeo {
@@ -476,7 +477,8 @@ __global__ void __launch_bounds__(256, kBlocksPerSm) raycast_kernel(EngineView v
     const int lane = threadIdx.x & 31;
     const int ntiles = v.tb->n_ray;
     const int budget = v.tb->ray_budget;
-    const int lx = lane & 7, ly = lane >> 3;
+    const int tw = v.tb->ray_tw;
+    const int lx = lane % tw, ly = lane / tw;
     while (true) {
         int t = 0;
         if (lane == 0) t = int(atomicAdd(&v.counters[0], 1u));

@@ -322,7 +322,7 @@ __global__ void __launch_bounds__(256, 4) fuse_kernel(EngineView v) {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int S_cap = v.tb->S;
     const unsigned int blocks = min(__ldcg(&v.counters[4]), unsigned(v.fuseq_cap));
-    const int split = fuse_split(blocks), rows = 64 / split;
+    const int split = v.tb->fuse_split ? v.tb->fuse_split : fuse_split(blocks), rows = 64 / split;
     const unsigned int items = blocks * unsigned(split);
     FuseCtx& c = ctx[warp];
     int cur_s = -1;

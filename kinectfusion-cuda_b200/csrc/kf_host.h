@@ -18,6 +18,9 @@ struct Tables {
     int icp_off[kMaxLevels]; // offset of each level's tiles in the ICP tile array
     int max_levels;
     int ray_budget;          // march iterations a lane takes before handing its ray to a warp
+    int ray_tw;              // ray tile width (a warp's 32 rays are ray_tw x 32 / ray_tw pixels)
+    int fuse_split;          // 0: fusion takes queue entries by the rule of fuse_split(); 1, 2, 4:
+                             // whole, in halves or in quarters
     long long fuse_total;    // fusion segments over all slots
     long long brick_total;   // bricks over all slots
     long long super_total;   // super-bricks over all slots
@@ -54,7 +57,7 @@ struct EngineView {
 };
 
 constexpr int kPreTileSize = 32;
-constexpr int kRayTileW = 8, kRayTileH = 4;   // one warp per ray tile
+constexpr int kRayTileW = 8;   // default ray tile width; one warp per 32-ray tile
 constexpr int kIcpThreads = 256;
 constexpr int kIcpPxPerThread = 8;
 constexpr int kIcpTilePx = kIcpThreads * kIcpPxPerThread;   // rows per block of the LLS stage
@@ -72,6 +75,7 @@ constexpr int kIcpMaxPasses = 64;     // hard cap on ICP passes per frame
 cudaError_t launch_preprocess(const EngineView& v, int grid, cudaStream_t st);
 // many: a step of more than kManyRayTiles ray tiles (serial_budget's rule)
 cudaError_t launch_raycast(const EngineView& v, int grid, cudaStream_t st, bool many);
+int serial_budget_many();   // the lane budget of the raycast's many-tile form
 // single: an engine of one slot (the kernel keeps that session's state per block)
 cudaError_t launch_icp(const EngineView& v, int grid, cudaStream_t st, bool single);
 cudaError_t launch_fuse(const EngineView& v, int grid, cudaStream_t st);

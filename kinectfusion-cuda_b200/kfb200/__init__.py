@@ -637,10 +637,19 @@ class Batch:
         arr = (ctypes.c_int * len(self.configs))(*[int(bool(a)) for a in active])
         check(lib.kf_batch_step_async(self._b, arr, _stream(stream)), "kf_batch_step_async")
 
-    def autotune(self, stream=None):
-        buf = ctypes.create_string_buffer(1024)
-        check(lib.kf_batch_autotune(self._b, _stream(stream), buf, 1024), "kf_batch_autotune")
-        return buf.value.decode()
+    def autotune_start(self, cache_path=None):
+        """Start tuning the launch shapes on the next steps (kf_batch_autotune_start); with a
+        cache file holding this session mix, the cached shape applies at once."""
+        check(lib.kf_batch_autotune_start(self._b, os.fsencode(cache_path) if cache_path else None),
+              "kf_batch_autotune_start")
+
+    def autotune_status(self):
+        """(steps the tuning still needs, report dict)."""
+        left = ctypes.c_int(0)
+        buf = ctypes.create_string_buffer(4096)
+        check(lib.kf_batch_autotune_status(self._b, ctypes.byref(left), buf, 4096), "kf_batch_autotune_status")
+        import json
+        return left.value, json.loads(buf.value.decode() or "{}")
 
     def set_profiling(self, on=True):
         check(lib.kf_batch_set_profiling(self._b, int(bool(on))))

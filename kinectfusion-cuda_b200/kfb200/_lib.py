@@ -129,7 +129,8 @@ SIGNATURES = {
     "kf_batch_step_async": (_I, [_P, _IP, _P]),
     "kf_batch_input_buffer": (_I, [_P, _I, ctypes.POINTER(_P)]),
     "kf_batch_session": (_I, [_P, _I, ctypes.POINTER(_P)]),
-    "kf_batch_autotune": (_I, [_P, _P, ctypes.c_char_p, ctypes.c_size_t]),
+    "kf_batch_autotune_start": (_I, [_P, ctypes.c_char_p]),
+    "kf_batch_autotune_status": (_I, [_P, _IP, ctypes.c_char_p, ctypes.c_size_t]),
     "kf_server_create": (_I, [_I, ctypes.c_size_t, ctypes.POINTER(_P)]),
     "kf_server_destroy": (_I, [_P]),
     "kf_server_open": (_I, [_P, _CFG, _IP]),

@@ -1,7 +1,7 @@
 """Batched and served forms: every session's result is the same whether it runs alone or in
 a mix of uneven sessions (bit-identical: each session's pixels, tiles and reduction order
-do not depend on the other sessions), admission follows the HBM budget, and tuning leaves
-the sessions untouched."""
+do not depend on the other sessions), admission follows the HBM budget, and the launch shapes
+the tuner tries change no result."""
 import threading
 
 import numpy as np
@@ -90,18 +90,48 @@ def test_batch_skipped_session_is_untouched(kf, mix):
     b.close()
 
 
-def test_autotune_leaves_state_unchanged(kf, mix):
-    cfgs, seqs, alone = mix
+def test_autotune_on_live_steps_changes_no_result_and_is_cached(kf, tmp_path):
+    """The tuner tries a different launch shape on each live step (grids, raycast form, lane
+    budget, ray tile, fusion split): every step's poses equal the untuned sessions' bit for bit.
+    The chosen shape goes to the cache file, and a new batch of the same mix takes it from there
+    without spending a step."""
+    from kfb200 import synth
+    cfgs = [kf.config_small(), kf.config_small(volume_n=96, tsdf_format=kf.KF_TSDF_F16U16)]
+    nframes = 80
+    seqs = [synth.sequence(c, nframes, seed=120 + i)[0] for i, c in enumerate(cfgs)]
+    alone = []
+    for c, seq in zip(cfgs, seqs):
+        s = kf.KinectFusion(c)
+        alone.append([s.process_frame(img)[1] for img in seq])
+        s.close()
+    cache = str(tmp_path / "shapes.json")
     b = kf.Batch(cfgs)
-    for f in range(3):
-        b.step([seq[f] for seq in seqs])
-    report = b.autotune()
-    assert "raycast" in report and "fuse" in report
-    for f in range(3, 5):
+    b.step([seq[0] for seq in seqs])
+    b.autotune_start(cache)
+    left0, rep = b.autotune_status()
+    assert left0 > 0 and rep["source"] == "tuning"
+    f = 1
+    while True:
         _, poses = b.step([seq[f] for seq in seqs])
         for i in range(len(cfgs)):
-            np.testing.assert_array_equal(poses[i], alone[i][0][f])
+            np.testing.assert_array_equal(poses[i], alone[i][f])
+        f += 1
+        left, rep = b.autotune_status()
+        if left == 0:
+            break
+        assert f < nframes
+    assert f - 1 == left0
+    assert rep["source"] == "tuned" and set(rep["shape"]) >= {"grid_ray", "ray_budget", "ray_tw", "fuse_split"}
+    for g in range(f, f + 3):   # the chosen shape keeps the results too
+        _, poses = b.step([seq[g] for seq in seqs])
+        for i in range(len(cfgs)):
+            np.testing.assert_array_equal(poses[i], alone[i][g])
     b.close()
+    b2 = kf.Batch(cfgs)
+    b2.autotune_start(cache)
+    left, rep2 = b2.autotune_status()
+    assert left == 0 and rep2["source"] == "cache" and rep2["shape"] == rep["shape"]
+    b2.close()
 
 
 def test_server_alone_vs_mix(kf, mix):
