@@ -167,7 +167,9 @@ __device__ __forceinline__ bool ray_start(const SessionDev* S, const RayGeo& g, 
 }
 
 // t at which the base voxel of the march leaves the voxel box [lo, hi) per axis (0.01 texel
-// inside its faces); faces on the volume's edge do not bound (coordinates clamp there)
+// inside its faces); faces on the volume's edge do not bound (coordinates clamp there).  The
+// margin absorbs the rounding of the affine form to + td t: a skip that stops early only
+// evaluates samples it could have skipped; it never passes a sample outside the box.
 __device__ __forceinline__ float box_exit(const RayGeo& g, int n, int lox, int hix, int loy, int hiy, int loz, int hiz,
                                           float t_far) {
     float t = t_far;
@@ -182,15 +184,13 @@ __device__ __forceinline__ float box_exit(const RayGeo& g, int n, int lox, int h
 
 // Samples whose base voxel lies in a cell whose distance lower bound is at or above the
 // current threshold (0.991 during large steps, 0.001 during small steps) cannot change the
-// march.  If the sample at st.t is such a sample, advance st past every following sample in the
-// same cell -- its 32^3 super-brick when that one qualifies, else its 8^3 brick -- to the first
-// sample index whose position is at or past the cell's exit, and return true.
-__device__ __forceinline__ bool skip_cell(const SessionDev* S, const RayGeo& g, RayState& st, float x, float y, float z,
+// march.  If the sample at st.t, with base voxel (vx, vy, vz), is such a sample, advance st past
+// every following sample in the same cell -- its 32^3 super-brick when that one qualifies, else
+// its 8^3 brick -- to the first sample index whose position is at or past the cell's exit, and
+// return true.
+__device__ __forceinline__ bool skip_cell(const SessionDev* S, const RayGeo& g, RayState& st, int vx, int vy, int vz,
                                           float inc) {
     const int n = S->n;
-    const int vx = min(max(int(floorf(x)), 0), n - 1);
-    const int vy = min(max(int(floorf(y)), 0), n - 1);
-    const int vz = min(max(int(floorf(z)), 0), n - 1);
     // order-preserving int keys of the two thresholds
     const int thr = st.small ? __float_as_int(0.001f) : __float_as_int(0.991f);
     int lo[3], hi[3];
@@ -238,8 +238,9 @@ __device__ int march_serial(const SessionDev* S, const RayGeo& g, const TF* f, R
         const float inc = st.small ? small : large;
         float x, y, z;
         texel(g, st.t, x, y, z);
-        if (bdil && skip_cell(S, g, st, x, y, z, inc)) continue;
-        const float tsdf = trilinear(f, n, x, y, z);
+        const TexelBase tb = texel_base(n, x, y, z);
+        if (bdil && skip_cell(S, g, st, tb.x0, tb.y0, tb.z0, inc)) continue;
+        const float tsdf = trilinear_at(f, n, tb);
         ++st.guard;
         if (tsdf < 0.0f) {
             if (st.t != st.near_d) {
@@ -288,7 +289,8 @@ __device__ void march_coop(const SessionDev* S, const RayGeo& g, const TF* f, Ra
         if (S->bdil) {
             float x, y, z;
             texel(g, st.t, x, y, z);
-            if (skip_cell(S, g, st, x, y, z, inc)) {   // every lane takes the same steps
+            const TexelBase tb = texel_base(S->n, x, y, z);
+            if (skip_cell(S, g, st, tb.x0, tb.y0, tb.z0, inc)) {   // every lane takes the same steps
                 wide = false;
                 continue;
             }
