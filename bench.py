@@ -604,6 +604,84 @@ def run_served(kf, torch, seconds, seed=11):
             "vs_alone": check}
 
 
+def run_served_load(kf, torch, sessions, seconds, fps=30.0, seed=13):
+    """Serving at load: full-size sessions (640x480, 512^3 f16+u16) admitted against an HBM budget
+    sized for `sessions` of them, then more opens than fit (the surplus is refused by the budget);
+    every admitted session streams frames with Poisson arrivals at `fps` for `seconds`.  The offered
+    rate is close to the batch's capacity, so the GPU is busy and each step serves the frames that
+    arrived during the last one (continuous batching).  Latency: arrival to result ready."""
+    import threading
+    from kfb200 import synth
+    rng = np.random.default_rng(seed)
+    cfg = kf.config_full(tsdf_format=kf.KF_TSDF_F16U16)
+    seqs = [synth.sequence(cfg, synth.LOOP_FRAMES, seed=400 + q, kind=synth.LOOP)[0] for q in range(8)]
+    import ctypes
+    fp = ctypes.c_size_t(0)
+    kf.check(kf.lib.kf_session_footprint(ctypes.byref(cfg), ctypes.byref(fp)))
+    # a session holds its footprint and two pinned-staging-sized frame buffers of the budget
+    budget = sessions * (int(fp.value) + 4 * cfg.width * cfg.height) + (64 << 20)
+    srv = kf.Server(sessions + 32, budget)
+    srv.reserve(cfg, sessions)
+    ids, refused = [], 0
+    for i in range(sessions + 16):
+        sid = srv.try_open(cfg)
+        if sid is None:
+            refused += 1
+        else:
+            ids.append(sid)
+    progress("served at load: %d sessions admitted, %d refused" % (len(ids), refused))
+    n = len(ids)
+    pos = [int(rng.integers(0, synth.LOOP_FRAMES)) for _ in range(n)]
+    for k in range(2):   # first frames (fusion only) and graph capture outside the window
+        for j in range(n):
+            srv.submit(ids[j], seqs[j % 8][pos[j]])
+            pos[j] += 1
+        srv.step()
+    srv.reset_stats()
+    stop = threading.Event()
+
+    def gpu_loop():
+        while not stop.is_set():
+            if srv.step() == 0:
+                time.sleep(0.0002)
+
+    th = threading.Thread(target=gpu_loop, daemon=True)
+    t0 = kf.Server.now_ms()
+    nxt = [t0 + float(rng.exponential(1000.0 / fps)) for _ in range(n)]
+    backlog = [[] for _ in range(n)]
+    th.start()
+    offered = 0
+    while True:
+        now = kf.Server.now_ms()
+        if now - t0 > seconds * 1000.0:
+            break
+        for j in range(n):
+            while nxt[j] <= now:
+                backlog[j].append(nxt[j])
+                nxt[j] += float(rng.exponential(1000.0 / fps))
+                offered += 1
+            if backlog[j] and srv.submit(ids[j], seqs[j % 8][pos[j] % synth.LOOP_FRAMES], backlog[j][0]) == kf.KF_OK:
+                backlog[j].pop(0)
+                pos[j] += 1
+        time.sleep(0.0002)
+    stop.set()
+    th.join(timeout=30)
+    wall = (kf.Server.now_ms() - t0) / 1000.0
+    st = srv.stats()
+    srv.close()
+    return {"workload": "%d full-size sessions (640x480, 512^3 f16+u16) streaming %g fps Poisson arrivals each for "
+                        "%.0f s; HBM budget sized for %d sessions, %d opens attempted" % (n, fps, seconds, sessions,
+                                                                                       sessions + 16),
+            "value": round(st["frames_done"] / wall, 2), "unit": "frames/s",
+            "offered_fps": round(offered / wall, 2),
+            "p50_ms": round(st["p50_ms"], 3), "p99_ms": round(st["p99_ms"], 3), "max_ms": round(st["max_ms"], 3),
+            "frames": int(st["frames_done"]), "steps": int(st["steps"]),
+            "frames_per_step": round(st["frames_done"] / max(1, st["steps"]), 2),
+            "admitted": n, "refused_at_open": refused, "max_active": int(st["max_active_sessions"]),
+            "hbm_budget_gb": round(budget / 1e9, 2),
+            "latency": "arrival of the frame (client queueing included) to result ready"}
+
+
 def served_vs_alone(kf, cfgs, frames):
     """Serve the sessions together, a different subset of them stepping each time, then run each
     alone through a plain session: the largest pose difference per frame and whether the final
@@ -947,6 +1025,14 @@ def run_ours(args, world, rank, local):
             out["batched"] = run_batched(kf, torch, min(steps, 150), value)
         if not args.no_served:
             out["served"] = run_served(kf, torch, args.served_seconds)
+            torch.cuda.empty_cache()
+            loads = [int(x) for x in str(args.load_sessions).split(",") if int(x) > 0]
+            if loads:
+                rows = []
+                for k in loads:
+                    rows.append(run_served_load(kf, torch, k, args.load_seconds))
+                    torch.cuda.empty_cache()
+                out["served_at_load"] = rows
         if not args.no_accuracy:
             progress("accuracy: start")
             out["accuracy"] = run_accuracy(kf)
@@ -1004,8 +1090,11 @@ def main():
     ap.add_argument("--no-batched", action="store_true", help="skip the batched-form measurement")
     ap.add_argument("--no-served", action="store_true", help="skip the served-form measurement")
     ap.add_argument("--no-accuracy", action="store_true", help="skip the error report against the FP64 oracle")
-    ap.add_argument("--served-seconds", type=float, default=20.0,
-                    help="length of the served run (the 64-session schedule is scaled to it)")
+    ap.add_argument("--served-seconds", type=float, default=60.0,
+                    help="length of the served run (the 64-session schedule of 60 s is scaled to it)")
+    ap.add_argument("--load-sessions", default="96,144,192",
+                    help="comma-separated session counts of the served-at-load runs (0: skip them)")
+    ap.add_argument("--load-seconds", type=float, default=10.0, help="length of each served-at-load run")
     ap.add_argument("--profile-frames", type=int, default=0,
                     help="run this many frames of the workload through kf_process_frame and exit, "
                          "printing no measurement (a short command for ncu captures of one kernel)")

@@ -385,6 +385,10 @@ kf_status grow(T*& ptr, int& cap, int need) {
     return KF_OK;
 }
 
+// The long-ray queue holds 1 / kLongRayShare of a step's rays (about 4 % of a frame's rays take
+// the long-ray path; more than the queue holds finish in their lane).
+constexpr int kLongRayShare = 16;
+
 // Launch shapes of a step.  Every value gives the same results bit for bit -- they only change
 // which block or lane does which part of the work -- so they can be tuned on live steps.
 struct Shape {
@@ -651,7 +655,7 @@ struct Engine {
         for (int l = 0; l < KF_MAX_LEVELS; ++l) cur_it += tb.n_itiles[l];
         const long long need_it = cur_it + res_it;
         const long long need_fq = tb.fuse_total + res_fq;
-        if (need_pre > INT32_MAX || need_ray * 32 / 4 > INT32_MAX / long_ray_bytes() ||
+        if (need_pre > INT32_MAX || need_ray * 32 / kLongRayShare > INT32_MAX / long_ray_bytes() ||
             need_it * kIcpPartialStride > INT32_MAX || need_fq > (1 << 29))
             return KF_ERR_CAPACITY;
         const int old_pre = cap_pre, old_ray = cap_ray, old_it = cap_it, old_part = cap_part, old_lq = cap_longq,
@@ -660,7 +664,7 @@ struct Engine {
         KF_TRY(grow(d_ray, cap_ray, int(need_ray)));
         KF_TRY(grow(d_itiles, cap_it, int(need_it)));
         KF_TRY(grow(d_partials, cap_part, 2 * int(need_it) * kIcpPartialStride));
-        KF_TRY(grow(d_longq, cap_longq, std::max<int>(1024, int(need_ray) * 32 / 4) * long_ray_bytes()));
+        KF_TRY(grow(d_longq, cap_longq, std::max<int>(1024, int(need_ray) * 32 / kLongRayShare) * long_ray_bytes()));
         KF_TRY(grow(d_fuseq, cap_fuseq, int(need_fq)));
         if (old_pre != cap_pre || old_ray != cap_ray || old_it != cap_it || old_part != cap_part || old_lq != cap_longq ||
             old_fq != cap_fuseq) {
@@ -740,8 +744,7 @@ struct Engine {
         KF_TRY(grow(d_ray, cap_ray, std::max<int>(1, int(ray.size()))));
         KF_TRY(grow(d_itiles, cap_it, std::max<int>(1, int(all.size()))));
         KF_TRY(grow(d_partials, cap_part, 2 * std::max<int>(1, int(all.size())) * kIcpPartialStride));
-        // room for a quarter of all rays to take the long-ray path (more fall back to the lane)
-        KF_TRY(grow(d_longq, cap_longq, std::max<int>(1024, int(ray.size()) * 32 / 4) * long_ray_bytes()));
+        KF_TRY(grow(d_longq, cap_longq, std::max<int>(1024, int(ray.size()) * 32 / kLongRayShare) * long_ray_bytes()));
         if (old_pre != cap_pre || old_ray != cap_ray || old_it != cap_it || old_part != cap_part || old_lq != cap_longq ||
             old_fq != cap_fuseq)
             graph_dirty = true;
