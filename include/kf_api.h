@@ -98,6 +98,13 @@ typedef struct kf_config {
                                     (reference: project/src/raycast.cu:61-73 returns early) */
     int export_icp_mask;         /* record per-pixel correspondence masks of the last iteration */
     float initial_pose[16];      /* camera->world, column-major */
+    /* Visualization volume: the reference's second voxel grid (project/src/kinect_fusion.cpp:19,
+     * :179-203), which it fuses every frame at the frame's pose and raycasts for display only.
+     * vis_volume_n = 0: none.  Else an n^3 grid (n a multiple of 8, format tsdf_format) over a
+     * cube of vis_volume_width metres, truncation vis_mu metres; kf_render raycasts it. */
+    int vis_volume_n;
+    float vis_volume_width;
+    float vis_mu;
 } kf_config;
 
 /* A TSDF volume in device memory, for the per-stage calls. */
@@ -179,6 +186,10 @@ kf_status kf_get_icp_mask(kf_session* s, int level, uint8_t* dst, int to_host);
 kf_status kf_get_tsdf(kf_session* s, void* dst, size_t dst_bytes, int layout, int to_host);
 kf_status kf_set_tsdf(kf_session* s, const void* src, size_t src_bytes, int layout, int from_host);
 kf_status kf_get_volume(kf_session* s, kf_volume* out);
+/* The visualization volume (KF_ERR_STATE when the session has none), as kf_get_tsdf /
+ * kf_get_volume do for the tracking volume. */
+kf_status kf_get_vis_tsdf(kf_session* s, void* dst, size_t dst_bytes, int layout, int to_host);
+kf_status kf_get_vis_volume(kf_session* s, kf_volume* out);
 
 /* ------------------------------------------------------------------------------------------ */
 /* stages: the reference's kernel:: wrappers, on device pointers                            */
@@ -272,6 +283,10 @@ kf_status kf_pose_error(const float pose_1[16], const float pose_2[16], float ou
  * sessions convert to and from float. */
 kf_status kf_save_tsdf_file(kf_session* s, const char* path);
 kf_status kf_load_tsdf_file(kf_session* s, const char* path);
+/* The same for the visualization volume, the grid the reference's KinectFusion::saveTSDF /
+ * loadTSDF write and read (project/src/kinect_fusion.cpp:327-335); KF_ERR_STATE without one. */
+kf_status kf_save_vis_tsdf_file(kf_session* s, const char* path);
+kf_status kf_load_vis_tsdf_file(kf_session* s, const char* path);
 /* Checkpoint: the .bin TSDF at `path` plus `path`.pose (text: frame count and the
  * column-major camera->world pose).  After a load the session resumes tracking as frame
  * `frames` of its sequence.  No counterpart in the reference beyond the .bin file. */
@@ -297,10 +312,10 @@ kf_status kf_shading_to_rgba(const float* normal, int w, int h, const float pose
 kf_status kf_float_channel_to_rgba(const float* src, int w, int h, float scale, uint8_t* rgba,
                                    void* stream, float* elapsed_ms);
 /* KinectFusion::visualizeCurrentModel (project/src/kinect_fusion.cpp:185-203), headless: raycast
- * the session's volume at level 0 from `pose` (NULL: the current pose; the reference's static
- * view passes the initial pose) into the session's own render maps, then the display kernel of
- * `mode` into rgba (w * h * 4 bytes; host memory when to_host = 1).  Tracking maps are not
- * touched.  Synchronizes `stream`. */
+ * the session's visualization volume (the tracking volume when it has none) at level 0 from
+ * `pose` (NULL: the current pose; the reference's static view passes the initial pose) into the
+ * session's own render maps, then the display kernel of `mode` into rgba (w * h * 4 bytes; host
+ * memory when to_host = 1).  Tracking maps are not touched.  Synchronizes `stream`. */
 kf_status kf_render(kf_session* s, int mode, const float pose[16], uint8_t* rgba, int to_host,
                     void* stream);
 

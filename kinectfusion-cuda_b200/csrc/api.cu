@@ -71,6 +71,9 @@ kf_status validate(const kf_config& c) {
     // a march step must still advance t in float at the far end of the range
     if (!(c.min_depth >= 0.f) || !(c.max_depth > c.min_depth) || !(c.max_depth < 1000.f)) return KF_ERR_ARG;
     if (!(c.mu * c.step_small > c.max_depth * 1e-6f)) return KF_ERR_ARG;
+    if (c.vis_volume_n != 0 &&
+        (c.vis_volume_n < 8 || c.vis_volume_n % 8 || !(c.vis_volume_width > 0.f) || !(c.vis_mu > 0.f)))
+        return KF_ERR_ARG;
     int total = 0;
     for (int l = 0; l < c.levels; ++l) {
         if (c.iters[l] < 0) return KF_ERR_ARG;
@@ -95,6 +98,11 @@ size_t footprint(const kf_config& c) {
     const size_t nb = size_t(c.volume_n / 8), ns = (nb + 3) / 4;
     b += nb * nb * nb * 2 * sizeof(int) + ns * ns * ns * sizeof(int);
     b += sizeof(float) * size_t((c.width + 15) / 16) * ((c.height + 15) / 16);
+    if (c.vis_volume_n) {   // the visualization volume: grid, axes, brick and super-brick bounds
+        const size_t vn = size_t(c.vis_volume_n), vnb = vn / 8, vns = (vnb + 3) / 4;
+        b += vn * vn * vn * (c.tsdf_format == KF_TSDF_F16U16 ? 4 : 8) + sizeof(float) * 2 * vn;
+        b += vnb * vnb * vnb * 2 * sizeof(int) + vns * vns * vns * sizeof(int);
+    }
     return b;
 }
 
@@ -339,10 +347,43 @@ kf_status slot_create(Slot& s, const kf_config& c, cudaStream_t st = nullptr) {
     KF_ALLOC(d.bmin, int*, sizeof(int) * size_t(nbricks));
     KF_ALLOC(d.bdil, int*, sizeof(int) * size_t(nbricks));
     KF_ALLOC(d.sdil, int*, sizeof(int) * size_t(nsuper));
+    std::vector<float> vhx, vhz;   // alive until the stream sync below
+    if (c.vis_volume_n) {
+        VisDev& V = d.vis;
+        V.n = c.vis_volume_n;
+        V.nb = V.n / 8;
+        V.ns = (V.nb + 3) / 4;
+        V.vol_w = c.vis_volume_width;
+        V.mu = c.vis_mu;
+        const size_t vn3 = size_t(V.n) * V.n * V.n;
+        KF_ALLOC(V.tf, void*, vn3 * es);
+        KF_ALLOC(V.tw, void*, vn3 * es);
+        float* vxs;
+        float* vzs;
+        KF_ALLOC(vxs, float*, sizeof(float) * V.n);
+        KF_ALLOC(vzs, float*, sizeof(float) * V.n);
+        vhx.resize(V.n);
+        vhz.resize(V.n);
+        voxel_axes(V.n, V.vol_w, vhx.data(), vhz.data());
+        err = cudaMemcpyAsync(vxs, vhx.data(), sizeof(float) * V.n, cudaMemcpyHostToDevice, st);
+        if (err == cudaSuccess) err = cudaMemcpyAsync(vzs, vhz.data(), sizeof(float) * V.n, cudaMemcpyHostToDevice, st);
+        if (err != cudaSuccess) { g_last_cuda = err; s.release(); return KF_ERR_CUDA; }
+        V.xs = vxs;
+        V.zs = vzs;
+        const size_t vnb3 = size_t(V.nb) * V.nb * V.nb, vns3 = size_t(V.ns) * V.ns * V.ns;
+        KF_ALLOC(V.bmin, int*, sizeof(int) * vnb3);
+        KF_ALLOC(V.bdil, int*, sizeof(int) * vnb3);
+        KF_ALLOC(V.sdil, int*, sizeof(int) * vns3);
+    }
 #undef KF_ALLOC
     // grid {f = 2, w = 0} and pose = initial_pose (project/src/kinect_fusion.cpp:33-36, :80)
     err = launch_init_volume(d.tf, d.tw, (long long)n3, d.fmt, st);
     if (err == cudaSuccess) err = launch_init_bricks(d.bmin, d.bdil, d.sdil, c.volume_n, st);
+    if (err == cudaSuccess && d.vis.n) {
+        const long long vn3 = (long long)d.vis.n * d.vis.n * d.vis.n;
+        err = launch_init_volume(d.vis.tf, d.vis.tw, vn3, d.fmt, st);
+        if (err == cudaSuccess) err = launch_init_bricks(d.vis.bmin, d.vis.bdil, d.vis.sdil, d.vis.n, st);
+    }
     const PoseDev P = make_pose_dev(c.initial_pose);
     if (err == cudaSuccess) err = cudaMemcpyAsync(d.pose, &P, sizeof(P), cudaMemcpyHostToDevice, st);
     if (err == cudaSuccess) err = cudaStreamSynchronize(st);
@@ -360,6 +401,11 @@ kf_status slot_reset(Slot& s) {
     const size_t n3 = size_t(c.volume_n) * c.volume_n * c.volume_n;
     KF_CK(launch_init_volume(s.d.tf, s.d.tw, (long long)n3, s.d.fmt, 0));
     KF_CK(launch_init_bricks(s.d.bmin, s.d.bdil, s.d.sdil, c.volume_n, 0));
+    if (s.d.vis.n) {
+        const long long vn3 = (long long)s.d.vis.n * s.d.vis.n * s.d.vis.n;
+        KF_CK(launch_init_volume(s.d.vis.tf, s.d.vis.tw, vn3, s.d.fmt, 0));
+        KF_CK(launch_init_bricks(s.d.vis.bmin, s.d.vis.bdil, s.d.vis.sdil, s.d.vis.n, 0));
+    }
     PoseDev P = make_pose_dev(c.initial_pose);
     KF_CK(cudaMemcpy(s.d.pose, &P, sizeof(P), cudaMemcpyHostToDevice));
     KF_CK(cudaDeviceSynchronize());
@@ -451,21 +497,27 @@ struct Engine {
     long long* d_fprefix = nullptr;
     long long* d_bprefix = nullptr;
     long long* d_sprefix = nullptr;
+    long long* d_vfprefix = nullptr;   // the same three over the visualization volumes
+    long long* d_vbprefix = nullptr;
+    long long* d_vsprefix = nullptr;
     float* d_partials = nullptr;
     int4* d_icp_sched = nullptr;
     float* d_icp_mats = nullptr;
     GridSync* d_sync = nullptr;
     unsigned int* d_ctr = nullptr;
-    static constexpr int kCounters = 8;
+    static constexpr int kCounters = 12;
     int cap_pre = 0, cap_ray = 0, cap_it = 0, cap_part = 0;
     // long-ray queue of the raycaster (bytes; entries = bytes / long_ray_bytes())
     char* d_longq = nullptr;
     int cap_longq = 0;
-    // fusion queue (one entry per block of every slot at most)
+    // fusion queue (one entry per block of every slot at most), and the visualization volumes'
     unsigned int* d_fuseq = nullptr;
     int cap_fuseq = 0;
+    unsigned int* d_vfuseq = nullptr;
+    int cap_vfuseq = 0;
+    bool has_vis = false;      // some slot has a visualization volume: the step fuses it too
     // work-list entries reserved ahead for sessions not open yet (reserve_work)
-    long long res_pre = 0, res_ray = 0, res_it = 0, res_fq = 0;
+    long long res_pre = 0, res_ray = 0, res_it = 0, res_fq = 0, res_vfq = 0;
     // pinned host
     StepDev* h_step = nullptr;
     OutDev* h_out = nullptr;
@@ -516,6 +568,9 @@ struct Engine {
         KF_CK(cudaMalloc(&d_fprefix, sizeof(long long) * (capacity + 1)));
         KF_CK(cudaMalloc(&d_bprefix, sizeof(long long) * (capacity + 1)));
         KF_CK(cudaMalloc(&d_sprefix, sizeof(long long) * (capacity + 1)));
+        KF_CK(cudaMalloc(&d_vfprefix, sizeof(long long) * (capacity + 1)));
+        KF_CK(cudaMalloc(&d_vbprefix, sizeof(long long) * (capacity + 1)));
+        KF_CK(cudaMalloc(&d_vsprefix, sizeof(long long) * (capacity + 1)));
         KF_CK(cudaMalloc(&d_icp_sched, sizeof(int4) * capacity));
         KF_CK(cudaMemset(d_icp_sched, 0, sizeof(int4) * capacity));
         KF_CK(cudaMalloc(&d_icp_mats, sizeof(float) * 24 * capacity));
@@ -596,6 +651,7 @@ struct Engine {
             if (e) cudaEventDestroy(e);
         cudaFree(d_sess); cudaFree(d_step); cudaFree(d_out); cudaFree(d_tb); cudaFree(d_pre); cudaFree(d_ray);
         cudaFree(d_itiles); cudaFree(d_iranges); cudaFree(d_fprefix); cudaFree(d_bprefix); cudaFree(d_sprefix);
+        cudaFree(d_vfprefix); cudaFree(d_vbprefix); cudaFree(d_vsprefix); cudaFree(d_vfuseq);
         cudaFree(d_partials);
         cudaFree(d_icp_sched);
         cudaFree(d_icp_mats);
@@ -627,6 +683,11 @@ struct Engine {
         v.longq_cap = cap_longq / long_ray_bytes();
         v.fuseq = d_fuseq;
         v.fuseq_cap = cap_fuseq;
+        v.vis_fuse_prefix = d_vfprefix;
+        v.vis_brick_prefix = d_vbprefix;
+        v.vis_super_prefix = d_vsprefix;
+        v.vis_fuseq = d_vfuseq;
+        v.vis_fuseq_cap = cap_vfuseq;
         return v;
     }
 
@@ -650,13 +711,15 @@ struct Engine {
         res_ray += k * ray;
         res_it += k * itiles;
         res_fq += k * fuse_units(c.volume_n);
+        res_vfq += k * (c.vis_volume_n ? fuse_units(c.vis_volume_n) : 0);
         const long long need_pre = tb.n_pre + res_pre, need_ray = tb.n_ray + res_ray;
         long long cur_it = 0;
         for (int l = 0; l < KF_MAX_LEVELS; ++l) cur_it += tb.n_itiles[l];
         const long long need_it = cur_it + res_it;
         const long long need_fq = tb.fuse_total + res_fq;
+        const long long need_vfq = tb.vis_fuse_total + res_vfq;
         if (need_pre > INT32_MAX || need_ray * 32 / kLongRayShare > INT32_MAX / long_ray_bytes() ||
-            need_it * kIcpPartialStride > INT32_MAX || need_fq > (1 << 29))
+            need_it * kIcpPartialStride > INT32_MAX || need_fq > (1 << 29) || need_vfq > (1 << 29))
             return KF_ERR_CAPACITY;
         const int old_pre = cap_pre, old_ray = cap_ray, old_it = cap_it, old_part = cap_part, old_lq = cap_longq,
                   old_fq = cap_fuseq;
@@ -666,8 +729,10 @@ struct Engine {
         KF_TRY(grow(d_partials, cap_part, 2 * int(need_it) * kIcpPartialStride));
         KF_TRY(grow(d_longq, cap_longq, std::max<int>(1024, int(need_ray) * 32 / kLongRayShare) * long_ray_bytes()));
         KF_TRY(grow(d_fuseq, cap_fuseq, int(need_fq)));
+        const int old_vfq = cap_vfuseq;
+        if (need_vfq > 0) KF_TRY(grow(d_vfuseq, cap_vfuseq, int(need_vfq)));
         if (old_pre != cap_pre || old_ray != cap_ray || old_it != cap_it || old_part != cap_part || old_lq != cap_longq ||
-            old_fq != cap_fuseq) {
+            old_fq != cap_fuseq || old_vfq != cap_vfuseq) {
             graph_dirty = true;
             tables_dirty = true;
         }
@@ -681,6 +746,7 @@ struct Engine {
         std::vector<IcpTile> it[KF_MAX_LEVELS];
         std::vector<IcpRange> ranges(size_t(KF_MAX_LEVELS) * cap, IcpRange{0, 0});
         std::vector<long long> fprefix(cap + 1, 0), bprefix(cap + 1, 0), sprefix(cap + 1, 0);
+        std::vector<long long> vfprefix(cap + 1, 0), vbprefix(cap + 1, 0), vsprefix(cap + 1, 0);
         std::vector<SessionDev> sess(cap);
         int max_levels = 1;
         for (int s = 0; s < cap; ++s) {
@@ -688,6 +754,9 @@ struct Engine {
             fprefix[s + 1] = fprefix[s];
             bprefix[s + 1] = bprefix[s];
             sprefix[s + 1] = sprefix[s];
+            vfprefix[s + 1] = vfprefix[s];
+            vbprefix[s + 1] = vbprefix[s];
+            vsprefix[s + 1] = vsprefix[s];
             if (!sl.used) { std::memset(&sess[s], 0, sizeof(SessionDev)); continue; }
             sess[s] = sl.d;
             const kf_config& c = sl.cfg;
@@ -704,6 +773,12 @@ struct Engine {
                 fprefix[s + 1] += fuse_units(c.volume_n);
                 bprefix[s + 1] += (long long)sl.d.nb * sl.d.nb * sl.d.nb;
                 sprefix[s + 1] += (long long)sl.d.ns * sl.d.ns * sl.d.ns;
+                if (sl.d.vis.n) {
+                    const VisDev& V = sl.d.vis;
+                    vfprefix[s + 1] += fuse_units(V.n);
+                    vbprefix[s + 1] += (long long)V.nb * V.nb * V.nb;
+                    vsprefix[s + 1] += (long long)V.ns * V.ns * V.ns;
+                }
             }
             for (int l = 0; l < c.levels; ++l) {
                 const LevelDev& Lv = sl.d.lv[l];
@@ -738,8 +813,14 @@ struct Engine {
         const int old_pre = cap_pre, old_ray = cap_ray, old_it = cap_it, old_part = cap_part, old_lq = cap_longq,
                   old_fq = cap_fuseq;
         // fusion queue entries are 32-bit and each is taken in 4 parts counted in 32 bits
-        if (fprefix[cap] > (long long)(1 << 29)) return KF_ERR_CAPACITY;
+        if (fprefix[cap] > (long long)(1 << 29) || vfprefix[cap] > (long long)(1 << 29)) return KF_ERR_CAPACITY;
         KF_TRY(grow(d_fuseq, cap_fuseq, std::max<int>(1, int(fprefix[cap]))));
+        const int old_vfq = cap_vfuseq;
+        KF_TRY(grow(d_vfuseq, cap_vfuseq, std::max<int>(1, int(vfprefix[cap]))));
+        if (old_vfq != cap_vfuseq) graph_dirty = true;
+        const bool vis = vfprefix[cap] > 0;
+        if (vis != has_vis) graph_dirty = true;   // the step launches the visualization fusion or not
+        has_vis = vis;
         KF_TRY(grow(d_pre, cap_pre, std::max<int>(1, int(pre.size()))));
         KF_TRY(grow(d_ray, cap_ray, std::max<int>(1, int(ray.size()))));
         KF_TRY(grow(d_itiles, cap_it, std::max<int>(1, int(all.size()))));
@@ -755,6 +836,9 @@ struct Engine {
         KF_CK(cudaMemcpy(d_fprefix, fprefix.data(), sizeof(long long) * fprefix.size(), cudaMemcpyHostToDevice));
         KF_CK(cudaMemcpy(d_bprefix, bprefix.data(), sizeof(long long) * bprefix.size(), cudaMemcpyHostToDevice));
         KF_CK(cudaMemcpy(d_sprefix, sprefix.data(), sizeof(long long) * sprefix.size(), cudaMemcpyHostToDevice));
+        KF_CK(cudaMemcpy(d_vfprefix, vfprefix.data(), sizeof(long long) * vfprefix.size(), cudaMemcpyHostToDevice));
+        KF_CK(cudaMemcpy(d_vbprefix, vbprefix.data(), sizeof(long long) * vbprefix.size(), cudaMemcpyHostToDevice));
+        KF_CK(cudaMemcpy(d_vsprefix, vsprefix.data(), sizeof(long long) * vsprefix.size(), cudaMemcpyHostToDevice));
         KF_CK(cudaMemcpy(d_sess, sess.data(), sizeof(SessionDev) * cap, cudaMemcpyHostToDevice));
         tb.S = cap;
         tb.n_pre = int(pre.size());
@@ -773,6 +857,9 @@ struct Engine {
         tb.fuse_total = fprefix[cap];
         tb.brick_total = bprefix[cap];
         tb.super_total = sprefix[cap];
+        tb.vis_fuse_total = vfprefix[cap];
+        tb.vis_brick_total = vbprefix[cap];
+        tb.vis_super_total = vsprefix[cap];
         KF_CK(cudaMemcpy(d_tb, &tb, sizeof(Tables), cudaMemcpyHostToDevice));
         tables_dirty = false;
         return KF_OK;
@@ -815,6 +902,13 @@ struct Engine {
             NvtxRange r("kf.fusion");
             if (stages[3]) KF_CK(launch_fuse(v, shape.grid_fuse, st));
             if (stages[3]) KF_CK(launch_bricks(v, shape.grid_brick, st));
+        }
+        if (has_vis && stages[3]) {
+            // the visualization volumes (the reference's second grid), after the tracking fusion
+            // and in the same stage time
+            NvtxRange r("kf.fusion_vis");
+            KF_CK(launch_fuse_vis(v, shape.grid_fuse, st));
+            KF_CK(launch_bricks_vis(v, shape.grid_brick, st));
         }
         if (profile) KF_CK(cudaEventRecordWithFlags(ev[4], st, cudaEventRecordExternal));
         KF_CK(cudaMemcpyAsync(h_out, d_out, sizeof(OutDev) * cap, cudaMemcpyDeviceToHost, st));
@@ -1068,6 +1162,11 @@ void kf_config_default(kf_config* c) {
     c->keep_on_miss = 1;
     c->export_icp_mask = 0;
     for (int i = 0; i < 16; ++i) c->initial_pose[i] = (i % 5 == 0) ? 1.0f : 0.0f;
+    // visualization grid: 512^3 over 5 m, mu = 2 voxels (project/src/main.cpp:25-26,
+    // project/src/kinect_fusion.cpp:19)
+    c->vis_volume_n = 512;
+    c->vis_volume_width = 5.0f;
+    c->vis_mu = 2.0f * (5.0f / 511.0f);
 }
 
 kf_status kf_session_footprint(const kf_config* cfg, size_t* bytes) {
@@ -1270,17 +1369,17 @@ kf_status kf_get_icp_mask(kf_session* s, int level, uint8_t* dst, int to_host) {
     return copy_out(dst, sl.d.mask[level], level_px(sl.cfg, level), to_host);
 }
 
-kf_status kf_get_tsdf(kf_session* s, void* dst, size_t dst_bytes, int layout, int to_host) {
-    if (!s || !dst) return KF_ERR_ARG;
-    const Slot& sl = s->sl();
-    const size_t n3 = size_t(sl.cfg.volume_n) * sl.cfg.volume_n * sl.cfg.volume_n;
-    const size_t es = sl.d.fmt == KF_TSDF_F16U16 ? 2 : 4;
+// a grid (distance and weight arrays of n^3) to dst in layout 0 (native) or 1 (.bin float2)
+static kf_status copy_grid_out(const void* tf, const void* tw, int n, int fmt, void* dst, size_t dst_bytes, int layout,
+                               int to_host) {
+    const size_t n3 = size_t(n) * n * n;
+    const size_t es = fmt == KF_TSDF_F16U16 ? 2 : 4;
     KF_CK(cudaDeviceSynchronize());
     const cudaMemcpyKind kind = to_host ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice;
     if (layout == 0) {
         if (dst_bytes < 2 * n3 * es) return KF_ERR_SHAPE;
-        KF_CK(cudaMemcpy(dst, sl.d.tf, n3 * es, kind));
-        KF_CK(cudaMemcpy(static_cast<char*>(dst) + n3 * es, sl.d.tw, n3 * es, kind));
+        KF_CK(cudaMemcpy(dst, tf, n3 * es, kind));
+        KF_CK(cudaMemcpy(static_cast<char*>(dst) + n3 * es, tw, n3 * es, kind));
         return KF_OK;
     }
     if (layout != 1) return KF_ERR_ARG;
@@ -1288,7 +1387,7 @@ kf_status kf_get_tsdf(kf_session* s, void* dst, size_t dst_bytes, int layout, in
     float* tmp = nullptr;
     if (to_host) KF_CK(cudaMalloc(&tmp, n3 * 8));
     float* target = to_host ? tmp : static_cast<float*>(dst);
-    cudaError_t e = launch_export_interleaved(sl.d.tf, sl.d.tw, (long long)n3, sl.d.fmt, target, 0);
+    cudaError_t e = launch_export_interleaved(tf, tw, (long long)n3, fmt, target, 0);
     if (e == cudaSuccess) e = cudaDeviceSynchronize();
     if (e == cudaSuccess && to_host) e = cudaMemcpy(dst, tmp, n3 * 8, cudaMemcpyDeviceToHost);
     if (tmp) cudaFree(tmp);
@@ -1296,17 +1395,31 @@ kf_status kf_get_tsdf(kf_session* s, void* dst, size_t dst_bytes, int layout, in
     return KF_OK;
 }
 
-kf_status kf_set_tsdf(kf_session* s, const void* src, size_t src_bytes, int layout, int from_host) {
-    if (!s || !src) return KF_ERR_ARG;
-    Slot& sl = s->sl();
-    const size_t n3 = size_t(sl.cfg.volume_n) * sl.cfg.volume_n * sl.cfg.volume_n;
-    const size_t es = sl.d.fmt == KF_TSDF_F16U16 ? 2 : 4;
+kf_status kf_get_vis_tsdf(kf_session* s, void* dst, size_t dst_bytes, int layout, int to_host) {
+    if (!s || !dst) return KF_ERR_ARG;
+    const Slot& sl = s->sl();
+    if (!sl.d.vis.n) return KF_ERR_STATE;
+    return copy_grid_out(sl.d.vis.tf, sl.d.vis.tw, sl.d.vis.n, sl.d.fmt, dst, dst_bytes, layout, to_host);
+}
+
+kf_status kf_get_tsdf(kf_session* s, void* dst, size_t dst_bytes, int layout, int to_host) {
+    if (!s || !dst) return KF_ERR_ARG;
+    const Slot& sl = s->sl();
+    return copy_grid_out(sl.d.tf, sl.d.tw, sl.cfg.volume_n, sl.d.fmt, dst, dst_bytes, layout, to_host);
+}
+
+// a grid (distance and weight arrays of n^3, with its brick bounds) from src in layout 0
+// (native) or 1 (.bin float2)
+static kf_status copy_grid_in(void* tf, void* tw, int n, int fmt, int* bmin, int* bdil, int* sdil, const void* src,
+                              size_t src_bytes, int layout, int from_host) {
+    const size_t n3 = size_t(n) * n * n;
+    const size_t es = fmt == KF_TSDF_F16U16 ? 2 : 4;
     KF_CK(cudaDeviceSynchronize());
     const cudaMemcpyKind kind = from_host ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice;
     if (layout == 0) {
         if (src_bytes < 2 * n3 * es) return KF_ERR_SHAPE;
-        KF_CK(cudaMemcpy(sl.d.tf, src, n3 * es, kind));
-        KF_CK(cudaMemcpy(sl.d.tw, static_cast<const char*>(src) + n3 * es, n3 * es, kind));
+        KF_CK(cudaMemcpy(tf, src, n3 * es, kind));
+        KF_CK(cudaMemcpy(tw, static_cast<const char*>(src) + n3 * es, n3 * es, kind));
     } else {
         if (layout != 1) return KF_ERR_ARG;
         if (src_bytes < n3 * 8) return KF_ERR_SHAPE;
@@ -1317,25 +1430,31 @@ kf_status kf_set_tsdf(kf_session* s, const void* src, size_t src_bytes, int layo
             KF_CK(cudaMemcpy(tmp, src, n3 * 8, cudaMemcpyHostToDevice));
             from = tmp;
         }
-        cudaError_t e = launch_import_interleaved(from, sl.d.tf, sl.d.tw, (long long)n3, sl.d.fmt, 0);
+        cudaError_t e = launch_import_interleaved(from, tf, tw, (long long)n3, fmt, 0);
         if (e == cudaSuccess) e = cudaDeviceSynchronize();
         if (tmp) cudaFree(tmp);
         KF_CK(e);
     }
     // the raycaster's brick minima follow the new volume
-    KF_CK(launch_rebuild_bricks(sl.d.tf, sl.d.fmt, sl.cfg.volume_n, sl.d.bmin, sl.d.bdil, sl.d.sdil, 0));
+    KF_CK(launch_rebuild_bricks(tf, fmt, n, bmin, bdil, sdil, 0));
     KF_CK(cudaDeviceSynchronize());
     return KF_OK;
 }
 
+kf_status kf_set_tsdf(kf_session* s, const void* src, size_t src_bytes, int layout, int from_host) {
+    if (!s || !src) return KF_ERR_ARG;
+    Slot& sl = s->sl();
+    return copy_grid_in(sl.d.tf, sl.d.tw, sl.cfg.volume_n, sl.d.fmt, sl.d.bmin, sl.d.bdil, sl.d.sdil, src, src_bytes,
+                        layout, from_host);
+}
+
 // ---- files: the reference's .bin TSDF layout, and checkpoints (TSDF + pose + frame index) ----
 
-kf_status kf_save_tsdf_file(kf_session* s, const char* path) {
-    if (!s || !path) return KF_ERR_ARG;
-    const Slot& sl = s->sl();
-    const size_t n3 = size_t(sl.cfg.volume_n) * sl.cfg.volume_n * sl.cfg.volume_n;
+// n^3 interleaved float {f, w} (VoxelGrid::saveVoxelGrid, project/src/voxel_grid.cpp:43-62)
+static kf_status save_grid_file(const void* tf, const void* tw, int n, int fmt, const char* path) {
+    const size_t n3 = size_t(n) * n * n;
     std::vector<float> host(n3 * 2);
-    KF_TRY(kf_get_tsdf(s, host.data(), n3 * 8, 1, 1));
+    KF_TRY(copy_grid_out(tf, tw, n, fmt, host.data(), n3 * 8, 1, 1));
     FILE* f = std::fopen(path, "wb");
     if (!f) return KF_ERR_ARG;
     const size_t wrote = std::fwrite(host.data(), 1, n3 * 8, f);
@@ -1343,18 +1462,45 @@ kf_status kf_save_tsdf_file(kf_session* s, const char* path) {
     return wrote == n3 * 8 && closed == 0 ? KF_OK : KF_ERR_ARG;
 }
 
-kf_status kf_load_tsdf_file(kf_session* s, const char* path) {
-    if (!s || !path) return KF_ERR_ARG;
-    const Slot& sl = s->sl();
-    const size_t n3 = size_t(sl.cfg.volume_n) * sl.cfg.volume_n * sl.cfg.volume_n;
+// VoxelGrid::loadVoxelGrid (project/src/voxel_grid.cpp:64-80); a file of another size is
+// KF_ERR_SHAPE
+static kf_status load_grid_file(void* tf, void* tw, int n, int fmt, int* bmin, int* bdil, int* sdil, const char* path) {
+    const size_t n3 = size_t(n) * n * n;
     FILE* f = std::fopen(path, "rb");
     if (!f) return KF_ERR_ARG;
     std::vector<float> host(n3 * 2);
     const size_t got = std::fread(host.data(), 1, n3 * 8, f);
     const bool extra = std::fgetc(f) != EOF;
     std::fclose(f);
-    if (got != n3 * 8 || extra) return KF_ERR_SHAPE;   // a .bin of another volume size
-    return kf_set_tsdf(s, host.data(), n3 * 8, 1, 1);
+    if (got != n3 * 8 || extra) return KF_ERR_SHAPE;
+    return copy_grid_in(tf, tw, n, fmt, bmin, bdil, sdil, host.data(), n3 * 8, 1, 1);
+}
+
+kf_status kf_save_tsdf_file(kf_session* s, const char* path) {
+    if (!s || !path) return KF_ERR_ARG;
+    const Slot& sl = s->sl();
+    return save_grid_file(sl.d.tf, sl.d.tw, sl.cfg.volume_n, sl.d.fmt, path);
+}
+
+kf_status kf_load_tsdf_file(kf_session* s, const char* path) {
+    if (!s || !path) return KF_ERR_ARG;
+    Slot& sl = s->sl();
+    return load_grid_file(sl.d.tf, sl.d.tw, sl.cfg.volume_n, sl.d.fmt, sl.d.bmin, sl.d.bdil, sl.d.sdil, path);
+}
+
+kf_status kf_save_vis_tsdf_file(kf_session* s, const char* path) {
+    if (!s || !path) return KF_ERR_ARG;
+    const Slot& sl = s->sl();
+    if (!sl.d.vis.n) return KF_ERR_STATE;
+    return save_grid_file(sl.d.vis.tf, sl.d.vis.tw, sl.d.vis.n, sl.d.fmt, path);
+}
+
+kf_status kf_load_vis_tsdf_file(kf_session* s, const char* path) {
+    if (!s || !path) return KF_ERR_ARG;
+    Slot& sl = s->sl();
+    if (!sl.d.vis.n) return KF_ERR_STATE;
+    return load_grid_file(sl.d.vis.tf, sl.d.vis.tw, sl.d.vis.n, sl.d.fmt, sl.d.vis.bmin, sl.d.vis.bdil, sl.d.vis.sdil,
+                          path);
 }
 
 kf_status kf_session_checkpoint_save(kf_session* s, const char* path) {
@@ -1450,16 +1596,26 @@ kf_status kf_render(kf_session* s, int mode, const float pose_in[16], uint8_t* r
     else KF_TRY(kf_get_pose(s, pose));
     float k[9], ik[9];
     level_intrinsics(c, 0, k, ik);
+    // the reference raycasts its visualization grid at level 0 into the predicted maps, then
+    // displays (KinectFusion::visualizeCurrentModel, project/src/kinect_fusion.cpp:185-203); the
+    // tracking maps are left alone here, and a session without a visualization volume renders
+    // its tracking volume
     kf_volume vol;
-    KF_TRY(kf_get_volume(s, &vol));
-    // the reference raycasts the model at level 0 into the predicted maps, then displays
-    // (KinectFusion::visualizeCurrentModel, project/src/kinect_fusion.cpp:185-203); the
-    // tracking maps are left alone here
+    SessionDev bounds = sl.d;   // the brick bounds the march may skip by
+    if (sl.d.vis.n) {
+        KF_TRY(kf_get_vis_volume(s, &vol));
+        bounds.bdil = sl.d.vis.bdil;
+        bounds.sdil = sl.d.vis.sdil;
+        bounds.nb = sl.d.vis.nb;
+        bounds.ns = sl.d.vis.ns;
+    } else {
+        KF_TRY(kf_get_volume(s, &vol));
+    }
     KF_CK(cudaStreamSynchronize(st));
     KF_CK(cudaMemsetAsync(sl.render_v, 0, size_t(w) * h * 16, st));
     KF_CK(cudaMemsetAsync(sl.render_n, 0, size_t(w) * h * 16, st));
     KF_CK(stage_raycast(&vol, pose, ik, sl.render_v, sl.render_n, w, h, c.min_depth, c.max_depth, c.step_large,
-                        c.step_small, st, &sl.d));
+                        c.step_small, st, &bounds));
     DispMats m{};
     if (mode == KF_RENDER_NORMALS) {
         for (int cc = 0; cc < 3; ++cc)
@@ -1485,6 +1641,20 @@ kf_status kf_get_volume(kf_session* s, kf_volume* out) {
     out->n = sl.cfg.volume_n;
     out->width = sl.cfg.volume_width;
     out->mu = sl.cfg.mu;
+    out->format = sl.cfg.tsdf_format;
+    out->max_weight = sl.cfg.max_weight;
+    return KF_OK;
+}
+
+kf_status kf_get_vis_volume(kf_session* s, kf_volume* out) {
+    if (!s || !out) return KF_ERR_ARG;
+    const Slot& sl = s->sl();
+    if (!sl.d.vis.n) return KF_ERR_STATE;
+    out->f = sl.d.vis.tf;
+    out->w = sl.d.vis.tw;
+    out->n = sl.d.vis.n;
+    out->width = sl.d.vis.vol_w;
+    out->mu = sl.d.vis.mu;
     out->format = sl.cfg.tsdf_format;
     out->max_weight = sl.cfg.max_weight;
     return KF_OK;

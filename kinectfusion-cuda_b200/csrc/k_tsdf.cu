@@ -246,33 +246,65 @@ __device__ __forceinline__ void fuse_rows(const FuseCtx& c, int x0, int j0, int 
         fuse_block<float, float>(c, x0, j0, k0, r_begin, r_end, lane);
 }
 
+// the fusion context of a session's tracking volume, or of its visualization volume (kVis):
+// the same depth map and pose, the other grid
+template <bool kVis>
 __device__ void load_ctx(const SessionDev* S, FuseCtx& c) {
     const PoseDev* P = S->pose;
     for (int q = 0; q < 9; ++q) c.iR[q] = P->iRf[q];
     for (int q = 0; q < 3; ++q) c.it[q] = P->itf[q];
     c.fx = S->lv[0].fx; c.fy = S->lv[0].fy; c.cx = S->lv[0].cx; c.cy = S->lv[0].cy;
-    c.min_d = S->min_d; c.max_d = S->max_d; c.mu = S->mu; c.max_w = S->max_w;
+    c.min_d = S->min_d; c.max_d = S->max_d; c.max_w = S->max_w;
     c.depth = S->depth_m;
     c.dmax = S->dmax16;
     c.t16w = S->t16w; c.t16h = S->t16h;
-    c.w = S->W; c.h = S->H; c.n = S->n; c.nb = S->nb; c.fmt = S->fmt;
-    c.F = S->tf; c.W = S->tw; c.xs = S->xs; c.zs = S->zs; c.bmin = S->bmin;
+    c.w = S->W; c.h = S->H; c.fmt = S->fmt;
+    if (kVis) {
+        const VisDev& V = S->vis;
+        c.mu = V.mu; c.n = V.n; c.nb = V.nb;
+        c.F = V.tf; c.W = V.tw; c.xs = V.xs; c.zs = V.zs; c.bmin = V.bmin;
+    } else {
+        c.mu = S->mu; c.n = S->n; c.nb = S->nb;
+        c.F = S->tf; c.W = S->tw; c.xs = S->xs; c.zs = S->zs; c.bmin = S->bmin;
+    }
 }
 
+// which tables a fusion launch walks: the tracking volumes' or the visualization volumes'
+template <bool kVis> struct FuseLists;
+template <> struct FuseLists<false> {
+    static __device__ long long total(const EngineView& v) { return v.tb->fuse_total; }
+    static __device__ const long long* prefix(const EngineView& v) { return v.fuse_prefix; }
+    static __device__ unsigned int* queue(const EngineView& v) { return v.fuseq; }
+    static __device__ int queue_cap(const EngineView& v) { return v.fuseq_cap; }
+    static constexpr int kQueued = 4, kTaken = 5;   // counters
+};
+template <> struct FuseLists<true> {
+    static __device__ long long total(const EngineView& v) { return v.tb->vis_fuse_total; }
+    static __device__ const long long* prefix(const EngineView& v) { return v.vis_fuse_prefix; }
+    static __device__ unsigned int* queue(const EngineView& v) { return v.vis_fuseq; }
+    static __device__ int queue_cap(const EngineView& v) { return v.vis_fuseq_cap; }
+    static constexpr int kQueued = 8, kTaken = 9;
+};
+
 // session of global fusion unit g (binary search over the per-slot prefix)
-__device__ __forceinline__ int unit_session(const EngineView& v, long long g, int S_cap) {
+__device__ __forceinline__ int unit_session(const long long* prefix, long long g, int S_cap) {
     int lo = 0, hi = S_cap;
     while (hi - lo > 1) {
         const int mid = (lo + hi) >> 1;
-        if (__ldg(v.fuse_prefix + mid) <= g) lo = mid; else hi = mid;
+        if (__ldg(prefix + mid) <= g) lo = mid; else hi = mid;
     }
     return lo;
 }
 
 // one thread per block of every stepping session: append the blocks that can update to the
-// queue (counters[4] = entries), one atomic per warp
+// queue (counters[4] = entries; [8] for the visualization volumes), one atomic per warp
+template <bool kVis>
 __global__ void __launch_bounds__(256) fuse_cull_kernel(EngineView v) {
-    const long long total = v.tb->fuse_total;
+    using Lists = FuseLists<kVis>;
+    const long long total = Lists::total(v);
+    const long long* prefix = Lists::prefix(v);
+    unsigned int* queue = Lists::queue(v);
+    const int queue_cap = Lists::queue_cap(v);
     const int S_cap = v.tb->S;
     const int lane = threadIdx.x & 31;
     const long long stride = (long long)gridDim.x * blockDim.x;
@@ -283,26 +315,26 @@ __global__ void __launch_bounds__(256) fuse_cull_kernel(EngineView v) {
         const long long g = base + lane;
         bool keep = false;
         if (g < total) {
-            const int s = unit_session(v, g, S_cap);
+            const int s = unit_session(prefix, g, S_cap);
             if (s != cur_s) {
                 cur_s = s;
                 const SessionDev* S = &v.sess[s];
                 live = v.step[s].active && S->pose->fuse_ok;
-                if (live) load_ctx(S, c);
+                if (live) load_ctx<kVis>(S, c);
             }
             if (live) {
                 int x0, j0, k0;
-                unit_origin(c.n, int(g - __ldg(v.fuse_prefix + s)), x0, j0, k0);
+                unit_origin(c.n, int(g - __ldg(prefix + s)), x0, j0, k0);
                 keep = !block_culled(c, x0, j0, k0);
             }
         }
         const unsigned int m = __ballot_sync(0xffffffffu, keep);
         if (m == 0) continue;
         unsigned int slot = 0;
-        if (lane == 0) slot = atomicAdd(&v.counters[4], unsigned(__popc(m)));
+        if (lane == 0) slot = atomicAdd(&v.counters[Lists::kQueued], unsigned(__popc(m)));
         slot = __shfl_sync(0xffffffffu, slot, 0);
         const unsigned int at = slot + __popc(m & ((1u << lane) - 1u));
-        if (keep && at < unsigned(v.fuseq_cap)) v.fuseq[at] = unsigned(g);   // capacity >= all blocks
+        if (keep && at < unsigned(queue_cap)) queue[at] = unsigned(g);   // capacity >= all blocks
     }
 }
 
@@ -317,39 +349,49 @@ __device__ __forceinline__ int fuse_split(unsigned int blocks) {
     return blocks >= 8u * warps ? 1 : blocks >= 4u * warps ? 2 : 4;
 }
 
+template <bool kVis>
 __global__ void __launch_bounds__(256, 4) fuse_kernel(EngineView v) {
+    using Lists = FuseLists<kVis>;
     __shared__ FuseCtx ctx[kFuseWarps];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int S_cap = v.tb->S;
-    const unsigned int blocks = min(__ldcg(&v.counters[4]), unsigned(v.fuseq_cap));
+    const long long* prefix = Lists::prefix(v);
+    const unsigned int* queue = Lists::queue(v);
+    const unsigned int blocks = min(__ldcg(&v.counters[Lists::kQueued]), unsigned(Lists::queue_cap(v)));
     const int split = v.tb->fuse_split ? v.tb->fuse_split : fuse_split(blocks), rows = 64 / split;
     const unsigned int items = blocks * unsigned(split);
     FuseCtx& c = ctx[warp];
     int cur_s = -1;
     while (true) {
         unsigned int i = 0;
-        if (lane == 0) i = atomicAdd(&v.counters[5], 1u);
+        if (lane == 0) i = atomicAdd(&v.counters[Lists::kTaken], 1u);
         i = __shfl_sync(0xffffffffu, i, 0);
         if (i >= items) break;
-        const long long g = __ldcg(v.fuseq + i / unsigned(split));
+        const long long g = __ldcg(queue + i / unsigned(split));
         const int part = int(i % unsigned(split));
-        const int s = unit_session(v, g, S_cap);
+        const int s = unit_session(prefix, g, S_cap);
         if (s != cur_s) {
             cur_s = s;
             __syncwarp();
-            if (lane == 0) load_ctx(&v.sess[s], c);
+            if (lane == 0) load_ctx<kVis>(&v.sess[s], c);
             __syncwarp();
         }
         int x0, j0, k0;
-        unit_origin(c.n, int(g - __ldg(v.fuse_prefix + s)), x0, j0, k0);
+        unit_origin(c.n, int(g - __ldg(prefix + s)), x0, j0, k0);
         fuse_rows(c, x0, j0, k0, part * rows, (part + 1) * rows, lane);
     }
 }
 
 cudaError_t launch_fuse(const EngineView& v, int grid, cudaStream_t st) {
     const int cull_grid = grid;   // grid-stride over all blocks of all sessions
-    fuse_cull_kernel<<<cull_grid, 256, 0, st>>>(v);
-    fuse_kernel<<<grid, 256, 0, st>>>(v);
+    fuse_cull_kernel<false><<<cull_grid, 256, 0, st>>>(v);
+    fuse_kernel<false><<<grid, 256, 0, st>>>(v);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_fuse_vis(const EngineView& v, int grid, cudaStream_t st) {
+    fuse_cull_kernel<true><<<grid, 256, 0, st>>>(v);
+    fuse_kernel<true><<<grid, 256, 0, st>>>(v);
     return cudaGetLastError();
 }
 
@@ -398,36 +440,52 @@ __device__ __forceinline__ int slot_of(const long long* prefix, long long g, int
 
 // bdil of every brick (the first half of the grid) and sdil of every super-brick (the second
 // half, one warp each) of the stepping sessions
+// the brick bounds of a session's tracking volume, or of its visualization volume (kVis)
+struct BrickView { int* bmin; int* bdil; int* sdil; int nb, ns; };
+template <bool kVis>
+__device__ __forceinline__ BrickView brick_view(const SessionDev* S) {
+    if (kVis) return BrickView{S->vis.bmin, S->vis.bdil, S->vis.sdil, S->vis.nb, S->vis.ns};
+    return BrickView{S->bmin, S->bdil, S->sdil, S->nb, S->ns};
+}
+
+template <bool kVis>
 __global__ void __launch_bounds__(256) bricks_kernel(EngineView v) {
     const int S_cap = v.tb->S;
     const int half = gridDim.x / 2;
+    const long long* bprefix = kVis ? v.vis_brick_prefix : v.brick_prefix;
+    const long long* sprefix = kVis ? v.vis_super_prefix : v.super_prefix;
     if (int(blockIdx.x) < half) {
-        const long long total = v.tb->brick_total;
+        const long long total = kVis ? v.tb->vis_brick_total : v.tb->brick_total;
         for (long long g = blockIdx.x * (long long)blockDim.x + threadIdx.x; g < total; g += (long long)half * blockDim.x) {
-            const int s = slot_of(v.brick_prefix, g, S_cap);
+            const int s = slot_of(bprefix, g, S_cap);
             if (!v.step[s].active) continue;
-            const SessionDev* S = &v.sess[s];
-            dilate_brick(S->bmin, S->bdil, S->nb, int(g - __ldg(v.brick_prefix + s)));
+            const BrickView B = brick_view<kVis>(&v.sess[s]);
+            dilate_brick(B.bmin, B.bdil, B.nb, int(g - __ldg(bprefix + s)));
         }
     } else {
-        const long long total = v.tb->super_total;
+        const long long total = kVis ? v.tb->vis_super_total : v.tb->super_total;
         const int lane = threadIdx.x & 31;
         const long long warp = ((blockIdx.x - half) * (long long)blockDim.x + threadIdx.x) >> 5;
         const long long nwarps = ((long long)(gridDim.x - half) * blockDim.x) >> 5;
         for (long long g = warp; g < total; g += nwarps) {
-            const int s = slot_of(v.super_prefix, g, S_cap);
+            const int s = slot_of(sprefix, g, S_cap);
             if (!v.step[s].active) continue;
-            const SessionDev* S = &v.sess[s];
-            const long long b = g - __ldg(v.super_prefix + s);
-            const int ns = S->ns;
-            const int k = superbrick_bound(S->bmin, S->nb, int(b % ns), int((b / ns) % ns), int(b / ((long long)ns * ns)), lane);
-            if (lane == 0) S->sdil[b] = k;
+            const BrickView B = brick_view<kVis>(&v.sess[s]);
+            const long long b = g - __ldg(sprefix + s);
+            const int ns = B.ns;
+            const int k = superbrick_bound(B.bmin, B.nb, int(b % ns), int((b / ns) % ns), int(b / ((long long)ns * ns)), lane);
+            if (lane == 0) B.sdil[b] = k;
         }
     }
 }
 
 cudaError_t launch_bricks(const EngineView& v, int grid, cudaStream_t st) {
-    bricks_kernel<<<grid, 256, 0, st>>>(v);
+    bricks_kernel<false><<<grid, 256, 0, st>>>(v);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_bricks_vis(const EngineView& v, int grid, cudaStream_t st) {
+    bricks_kernel<true><<<grid, 256, 0, st>>>(v);
     return cudaGetLastError();
 }
 

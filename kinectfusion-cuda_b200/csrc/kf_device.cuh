@@ -42,6 +42,20 @@ struct PoseDev {
     int fuse_ok;            // 1 when this frame's fusion runs
 };
 
+// a session's visualization volume (n = 0: none): a second TSDF in the session's format, fused
+// at the frame's pose from the same depth map, never raycast by the frame step
+struct VisDev {
+    int n, nb, ns;          // voxels, bricks and super-bricks per axis
+    float vol_w, mu;
+    void* tf;
+    void* tw;
+    const float* xs;
+    const float* zs;
+    int* bmin;
+    int* bdil;
+    int* sdil;
+};
+
 // everything a kernel needs about one session; an array of these lives in device memory
 struct SessionDev {
     int W, H, L;
@@ -85,6 +99,7 @@ struct SessionDev {
     float dist_th, angle_th, stop_a, stop_d;
     float angle_cos;       // cos(angle_th): the normal test compares cosines
     PoseDev* pose;
+    VisDev vis;
 };
 
 // per-step control, written by the host: which sessions take part and which are on their

@@ -24,6 +24,9 @@ struct Tables {
     long long fuse_total;    // fusion segments over all slots
     long long brick_total;   // bricks over all slots
     long long super_total;   // super-bricks over all slots
+    long long vis_fuse_total;  // the same three over the slots' visualization volumes
+    long long vis_brick_total;
+    long long vis_super_total;
 };
 
 struct LongRay;   // march state of a ray handed from a lane to a warp (k_raycast.cu)
@@ -43,17 +46,23 @@ struct EngineView {
     const long long* fuse_prefix;// S + 1 entries, in segments
     const long long* brick_prefix;// S + 1 entries, in bricks
     const long long* super_prefix;// S + 1 entries, in super-bricks
+    const long long* vis_fuse_prefix;   // the same three for the visualization volumes
+    const long long* vis_brick_prefix;
+    const long long* vis_super_prefix;
     float* partials;             // ICP tile partials, kIcpPartialStride floats per tile
     float* partials2;            // a second set: a single session's odd passes (see icp_kernel)
     int4* icp_sched;             // per slot: {level of the next ICP pass or -1, first tile, tiles, 0}
     float* icp_mats;             // per slot: 24 floats phase A reads (R, t, K_l R_prev^T, t_prev)
     GridSync* sync;
     unsigned int* counters;      // [0] raycast tiles, [4] fusion blocks queued, [5] fusion
-                                 // items taken, [6] long rays queued, [7] long rays taken
+                                 // items taken, [6] long rays queued, [7] long rays taken,
+                                 // [8], [9] the visualization volumes' [4], [5]
     LongRay* longq;              // long-ray queue
     int longq_cap;
     unsigned int* fuseq;         // fusion queue: global unit index of each block that can update
     int fuseq_cap;
+    unsigned int* vis_fuseq;     // the visualization volumes' fusion queue
+    int vis_fuseq_cap;
 };
 
 constexpr int kPreTileSize = 32;
@@ -79,9 +88,12 @@ int serial_budget_many();   // the lane budget of the raycast's many-tile form
 // single: an engine of one slot (the kernel keeps that session's state per block)
 cudaError_t launch_icp(const EngineView& v, int grid, cudaStream_t st, bool single);
 cudaError_t launch_fuse(const EngineView& v, int grid, cudaStream_t st);
+// the same for the sessions' visualization volumes (cull, fuse and bounds)
+cudaError_t launch_fuse_vis(const EngineView& v, int grid, cudaStream_t st);
 // widen the brick lower bounds to the 2 x 2 x 2 bricks the raycaster reads, and bound the
 // super-bricks (one launch)
 cudaError_t launch_bricks(const EngineView& v, int grid, cudaStream_t st);
+cudaError_t launch_bricks_vis(const EngineView& v, int grid, cudaStream_t st);
 // bounds = key(2), the initial distance; rebuild recomputes them exactly from a loaded volume
 cudaError_t launch_init_bricks(int* bmin, int* bdil, int* sdil, int n, cudaStream_t st);
 cudaError_t launch_rebuild_bricks(const void* f, int fmt, int n, int* bmin, int* bdil, int* sdil, cudaStream_t st);

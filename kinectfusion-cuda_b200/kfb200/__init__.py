@@ -103,22 +103,22 @@ def start_pose(cube_width):
 def config_small(**overrides):
     """Plain pipeline, small size: 320x240, fx = fy = 262.5, 128^3 float/float TSDF over a
     2 m cube, truncation 0.03 m, bilateral sigma_s 4.5 px / sigma_r 30 mm / 5x5, ICP 4/5/10
-    coarse to fine, 0.1 m / 20 degrees, depth in millimetres."""
+    coarse to fine, 0.1 m / 20 degrees, depth in millimetres; no visualization volume."""
     kw = dict(width=320, height=240, fx=262.5, fy=262.5, cx=159.5, cy=119.5, depth_scale=1e-3,
               iters=(10, 5, 4), dist_thresh=0.1, angle_thresh=float(np.deg2rad(20.0)),
               bilateral_sigma_s=4.5, bilateral_sigma_r=0.03, bilateral_radius=2,
-              volume_n=128, volume_width=2.0, mu=0.03, initial_pose=start_pose(2.0))
+              volume_n=128, volume_width=2.0, mu=0.03, initial_pose=start_pose(2.0), vis_volume_n=0)
     kw.update(overrides)
     return default_config(**kw)
 
 
 def config_full(**overrides):
     """Plain pipeline at full size: 640x480, fx = fy = 525, 512^3 float/float TSDF over a
-    3 m cube, truncation 0.02 m, ICP 4/5/10 coarse to fine."""
+    3 m cube, truncation 0.02 m, ICP 4/5/10 coarse to fine; no visualization volume."""
     kw = dict(width=640, height=480, fx=525.0, fy=525.0, cx=319.5, cy=239.5, depth_scale=1e-3,
               iters=(10, 5, 4), dist_thresh=0.1, angle_thresh=float(np.deg2rad(20.0)),
               bilateral_sigma_s=4.5, bilateral_sigma_r=0.03, bilateral_radius=2,
-              volume_n=512, volume_width=3.0, mu=0.02, initial_pose=start_pose(3.0))
+              volume_n=512, volume_width=3.0, mu=0.02, initial_pose=start_pose(3.0), vis_volume_n=0)
     kw.update(overrides)
     return default_config(**kw)
 
@@ -285,6 +285,18 @@ class KinectFusion:
         check(lib.kf_get_tsdf(self._s, _np_ptr(inter), inter.nbytes, 1, 1))
         return inter[..., 0].copy(), inter[..., 1].copy()
 
+    def vis_tsdf(self):
+        """The visualization volume's (f, w) float32 arrays (n, n, n) indexed [z, y, x]."""
+        n = self.config.vis_volume_n
+        inter = np.empty((n, n, n, 2), np.float32)
+        check(lib.kf_get_vis_tsdf(self._s, _np_ptr(inter), inter.nbytes, 1, 1), "kf_get_vis_tsdf")
+        return inter[..., 0].copy(), inter[..., 1].copy()
+
+    def vis_volume(self):
+        v = KfVolume()
+        check(lib.kf_get_vis_volume(self._s, ctypes.byref(v)), "kf_get_vis_volume")
+        return v
+
     def set_tsdf(self, f, w):
         n = self.config.volume_n
         inter = np.empty((n, n, n, 2), np.float32)
@@ -293,12 +305,22 @@ class KinectFusion:
         check(lib.kf_set_tsdf(self._s, _np_ptr(inter), inter.nbytes, 1, 1))
 
     def saveTSDF(self, path):
-        """VoxelGrid::saveVoxelGrid (project/src/voxel_grid.cpp:43-62): n^3 float2 {f, w}, x fastest."""
-        check(lib.kf_save_tsdf_file(self._s, os.fsencode(path)), "kf_save_tsdf_file")
+        """KinectFusion::saveTSDF (project/src/kinect_fusion.cpp:327-330): the visualization grid
+        when the session has one (as the reference), else the tracking volume, in the .bin layout
+        of VoxelGrid::saveVoxelGrid (project/src/voxel_grid.cpp:43-62): n^3 float2 {f, w}, x
+        fastest."""
+        if self.config.vis_volume_n:
+            check(lib.kf_save_vis_tsdf_file(self._s, os.fsencode(path)), "kf_save_vis_tsdf_file")
+        else:
+            check(lib.kf_save_tsdf_file(self._s, os.fsencode(path)), "kf_save_tsdf_file")
 
     def loadTSDF(self, path):
-        """VoxelGrid::loadVoxelGrid (project/src/voxel_grid.cpp:64-80)."""
-        check(lib.kf_load_tsdf_file(self._s, os.fsencode(path)), "kf_load_tsdf_file")
+        """KinectFusion::loadTSDF (project/src/kinect_fusion.cpp:332-335), the same grid as saveTSDF
+        (VoxelGrid::loadVoxelGrid, project/src/voxel_grid.cpp:64-80)."""
+        if self.config.vis_volume_n:
+            check(lib.kf_load_vis_tsdf_file(self._s, os.fsencode(path)), "kf_load_vis_tsdf_file")
+        else:
+            check(lib.kf_load_tsdf_file(self._s, os.fsencode(path)), "kf_load_tsdf_file")
 
     def saveCheckpoint(self, path):
         """TSDF (.bin at path) + pose and frame count (path + '.pose')."""

@@ -53,6 +53,7 @@ class KfConfig(ctypes.Structure):
         ("step_large", ctypes.c_float), ("step_small", ctypes.c_float),
         ("compat_trunc8", ctypes.c_int), ("keep_on_miss", ctypes.c_int), ("export_icp_mask", ctypes.c_int),
         ("initial_pose", ctypes.c_float * 16),
+        ("vis_volume_n", ctypes.c_int), ("vis_volume_width", ctypes.c_float), ("vis_mu", ctypes.c_float),
     ]
 
 
@@ -109,6 +110,8 @@ SIGNATURES = {
     "kf_get_tsdf": (_I, [_P, _P, ctypes.c_size_t, _I, _I]),
     "kf_set_tsdf": (_I, [_P, _P, ctypes.c_size_t, _I, _I]),
     "kf_get_volume": (_I, [_P, _VOL]),
+    "kf_get_vis_tsdf": (_I, [_P, _P, ctypes.c_size_t, _I, _I]),
+    "kf_get_vis_volume": (_I, [_P, _VOL]),
     "kf_convert_to_depth_meters": (_I, [_P, _I, _I, _P, _I, _I, _F, _I, _P, _FP]),
     "kf_apply_bilateral_filter": (_I, [_P, _I, _I, _P, _I, _I, _F, _F, _I, _P, _FP]),
     "kf_down_sample": (_I, [_P, _I, _I, _P, _I, _I, _F, _P, _FP]),
@@ -144,6 +147,8 @@ SIGNATURES = {
     "kf_server_reserve": (_I, [_P, _CFG, _I]),
     "kf_save_tsdf_file": (_I, [_P, ctypes.c_char_p]),
     "kf_load_tsdf_file": (_I, [_P, ctypes.c_char_p]),
+    "kf_save_vis_tsdf_file": (_I, [_P, ctypes.c_char_p]),
+    "kf_load_vis_tsdf_file": (_I, [_P, ctypes.c_char_p]),
     "kf_session_checkpoint_save": (_I, [_P, ctypes.c_char_p]),
     "kf_session_checkpoint_load": (_I, [_P, ctypes.c_char_p]),
     "kf_normal_map_to_rgba": (_I, [_P, _I, _I, _FP, _P, _P, _FP]),

@@ -129,3 +129,55 @@ def test_tum_sequence_drives_the_pipeline(kf, tracked):
             np.testing.assert_array_equal(p1, p2)
         s1.close()
         s2.close()
+
+
+def test_visualization_volume(kf, orc, cuda):
+    """The reference's second grid (project/src/kinect_fusion.cpp:19, :179-203): fused every frame
+    at the frame's pose from the unfiltered depth, as the oracle fuses it (max over touched
+    voxels but boundary flips within 1e-3 of its truncation); tracking is unchanged by it, bit for
+    bit; kf_render raycasts it (the stage raycast of that volume plus the display kernel)."""
+    import parity
+    from kfb200 import synth
+    cfg0 = kf.config_small()
+    vn, vw = 128, 3.0
+    cfg = kf.config_small(vis_volume_n=vn, vis_volume_width=vw, vis_mu=2.0 * vw / (vn - 1))
+    imgs, _ = synth.sequence(cfg, 5, seed=55)
+    xs, zs = orc.voxel_axes(vn, vw)
+    plain = kf.KinectFusion(cfg0)
+    s = kf.KinectFusion(cfg)
+    for img in imgs:
+        f0, w0 = s.vis_tsdf()
+        _, pose = s.process_frame(img)
+        np.testing.assert_array_equal(pose, plain.process_frame(img)[1])
+        f1, w1 = s.vis_tsdf()
+        fo, wo = f0.copy(), w0.copy()
+        depth_m = orc.convert(img, cfg.depth_scale)
+        orc.fuse(depth_m, kf.level_intrinsics(cfg, 0), fo, wo, vw, cfg.vis_mu, pose, prec=1)
+        vcfg = kf.config_small(volume_n=vn, volume_width=vw, mu=cfg.vis_mu)
+        t = parity.tsdf_frame_parity(vcfg, f0, w0, f1, w1, fo, wo, pose, depth_m, xs, zs)
+        assert t["touched"] > 1000 and t["max_nonflip"] <= 1e-3, t
+        assert t["boundary_flips"] <= 5e-3 * t["touched"], t
+    np.testing.assert_array_equal(s.tsdf()[0], plain.tsdf()[0])   # the tracking volume is the same
+    pose = s.pose()
+    ik = kf.level_inverse_intrinsics(cfg, 0)
+    vt = cuda.zeros((cfg.height, cfg.width, 4), dtype=cuda.float32, device="cuda")
+    nt = cuda.zeros_like(vt)
+    kf.kernel.raycast(s.vis_volume(), pose, ik, vt, nt, cfg.min_depth, cfg.max_depth, cfg.step_large, cfg.step_small)
+    nmap = nt.cpu().numpy()
+    assert np.mean(nmap[..., 3] == -1) > 0.2
+    close_rgba(s.render(kf.KF_RENDER_SHADING), orc.display_shading(nmap, pose, ik))
+    close_rgba(s.render(kf.KF_RENDER_NORMALS), orc.display_normals(nmap, pose[:3, :3].T))
+    # saveTSDF / loadTSDF write and read the visualization grid, as the reference's do
+    vf, vwt = s.vis_tsdf()
+    with tempfile.TemporaryDirectory() as d:
+        path = os.path.join(d, "vis.bin")
+        s.saveTSDF(path)
+        assert os.path.getsize(path) == vn ** 3 * 8
+        other = kf.KinectFusion(cfg)
+        other.loadTSDF(path)
+        f2, w2 = other.vis_tsdf()
+        np.testing.assert_array_equal(f2, vf)
+        np.testing.assert_array_equal(w2, vwt)
+        other.close()
+    plain.close()
+    s.close()

@@ -55,6 +55,22 @@ def test_default_config_is_the_reference_main(kf):
     assert c.step_large == pytest.approx(1.99) and c.step_small == pytest.approx(0.1)
     assert c.keep_on_miss == 1 and c.max_weight == 0.0 and c.tsdf_format == kf.KF_TSDF_F32F32
     assert list(c.initial_pose) == [1, 0, 0, 0, 0, 1, 0, 0, 0, 0, 1, 0, 0, 0, 0, 1]
+    # the visualization grid: 512^3 over 5 m, mu = 2 voxels (project/src/main.cpp:25-26,
+    # project/src/kinect_fusion.cpp:19)
+    assert c.vis_volume_n == 512 and c.vis_volume_width == 5.0 and abs(c.vis_mu - 2 * 5 / 511) < 1e-7
+
+
+def test_visualization_volume_counts_in_the_footprint(kf):
+    n = ctypes.c_size_t()
+    c = kf.config_small()
+    assert c.vis_volume_n == 0
+    kf.lib.kf_session_footprint(ctypes.byref(c), ctypes.byref(n))
+    base = n.value
+    cv = kf.config_small(vis_volume_n=256, vis_volume_width=5.0, vis_mu=2 * 5 / 255)
+    kf.lib.kf_session_footprint(ctypes.byref(cv), ctypes.byref(n))
+    assert n.value - base >= 256 ** 3 * 8
+    bad = kf.config_small(vis_volume_n=100, vis_volume_width=5.0, vis_mu=0.04)   # not a multiple of 8
+    assert kf.lib.kf_session_footprint(ctypes.byref(bad), ctypes.byref(n)) == kf.KF_ERR_ARG
 
 
 def test_status_strings(kf):
