@@ -293,6 +293,26 @@ def stage_rooflines(cfg, ab, stage_ms, peak, icp_iters, traffic, fps):
     return out
 
 
+def raycast_work(kf, cfg, dev_frames, nimg, stream, frames=12):
+    """The raycast's own work per frame on the timed frame sequence (KF_DEBUG_COUNTERS on a second
+    session, counts averaged over the frames after the second): rays, samples evaluated, skips,
+    samples skipped, gradient samples, long-ray hand-offs."""
+    import torch
+    s = kf.KinectFusion(cfg)
+    s.set_debug(kf.KF_DEBUG_COUNTERS)
+    acc, first = None, None
+    for i in range(frames):
+        s.process_frame(dev_frames[i % nimg], stream=stream)
+        if i == 1:
+            first = s.debug_counts()   # the frame the oracle's sample count is taken on
+        if i >= 2:
+            c = s.debug_counts()
+            acc = c if acc is None else {k: acc[k] + c[k] for k in c}
+    torch.cuda.synchronize()
+    s.close()
+    return {k: round(v / (frames - 2), 1) for k, v in acc.items()}, first
+
+
 def l2_read_gbs(kf):
     """Read bandwidth of an L2-resident buffer (64 MiB, under the 126 MB L2), 200 rounds in one
     launch (kf_measure_read_bandwidth): the on-box L2 figure beside the gather numbers."""
@@ -987,6 +1007,22 @@ def run_ours(args, world, rank, local):
         stages["raycast"]["l2_read_gbs"] = l2
         stages["raycast"]["frac_of_l2_read"] = (round(stages["raycast"]["achieved_gbs"] / l2, 4)
                                                 if stages["raycast"]["achieved_gbs"] and l2 else None)
+        # what the march itself does per frame: the samples it evaluates (8 taps of 4 B each) are
+        # the gather it issues, against the on-box L2 read (the taps are L1/L2 hits)
+        work, work1 = raycast_work(kf, cfg, dev_frames, nimg, stream)
+        evaluated = work["eval_large"] + work["eval_small"] + work["gradient"]
+        evaluated1 = work1["eval_large"] + work1["eval_small"] + work1["gradient"]
+        own = evaluated * 8 * 4 + sum((cfg.width >> l) * (cfg.height >> l) for l in range(cfg.levels)) * 32
+        rs = stage_ms[1] / 1000.0
+        stages["raycast"]["march_work_per_frame"] = work
+        stages["raycast"]["evaluated_samples_per_frame"] = round(evaluated, 1)
+        stages["raycast"]["reference_samples_frame1"] = int(samples)
+        stages["raycast"]["evaluated_samples_frame1"] = int(evaluated1)
+        stages["raycast"]["evaluated_vs_reference_frame1"] = round(evaluated1 / samples, 4) if samples else None
+        stages["raycast"]["evaluated_gather_bytes"] = int(own)
+        stages["raycast"]["evaluated_gather_gbs"] = round(own / rs / 1e9, 1) if rs > 0 else None
+        stages["raycast"]["evaluated_gather_frac_of_l2_read"] = (round(own / rs / 1e9 / l2, 4) if rs > 0 and l2
+                                                                 else None)
         roofline["stages"] = stages
         progress("plain: roofline sample done")
         cpu = None

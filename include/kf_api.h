@@ -441,9 +441,22 @@ kf_status kf_session_stage_times(kf_session* s, float ms[4]);
  * graph, each stage inside an NVTX range (kf.preprocess, kf.raycast, kf.icp, kf.fusion), so a
  * profiler can select a stage's launches.  Results are the same; steps are slower. */
 #define KF_DEBUG_NO_GRAPH 2
+/* KF_DEBUG_COUNTERS makes the raycast count its work in every step (kernels built with the
+ * counts; the plain kernels run otherwise): kf_session_debug_counts / kf_batch_debug_counts
+ * return, for the last step, [0] rays that marched, [1] samples evaluated during large steps,
+ * [2] during small steps, [3] cell skips, [4] samples the skips jumped over, [5] gradient
+ * samples, [6] rays handed to the long-ray warp kernel, [7] that kernel's warp rounds.  The
+ * counts cost time; results are the same. */
+#define KF_DEBUG_COUNTERS 4
+#define KF_RAY_COUNTS 8
 kf_status kf_session_set_debug(kf_session* s, int flags);
-/* The same for every session of a batch (KF_DEBUG_NO_GRAPH applies to the batch's steps). */
+/* The same for every session of a batch (KF_DEBUG_NO_GRAPH and KF_DEBUG_COUNTERS apply to the
+ * batch's steps). */
 kf_status kf_batch_set_debug(kf_batch* b, int flags);
+/* The raycast work counts of the last step (n entries, at most KF_RAY_COUNTS; KF_ERR_STATE
+ * unless KF_DEBUG_COUNTERS is on).  For a session of a batch the counts are the whole step's. */
+kf_status kf_session_debug_counts(kf_session* s, uint64_t* out, int n);
+kf_status kf_batch_debug_counts(kf_batch* b, uint64_t* out, int n);
 /* The traces of the last raycast at `level` (w * h uint64; host memory when to_host = 1).
  * KF_ERR_STATE unless KF_DEBUG_RAY_TRACE is on. */
 kf_status kf_get_ray_trace(kf_session* s, int level, uint64_t* dst, int to_host);

@@ -516,6 +516,8 @@ struct Engine {
     unsigned int* d_vfuseq = nullptr;
     int cap_vfuseq = 0;
     bool has_vis = false;      // some slot has a visualization volume: the step fuses it too
+    unsigned long long* d_ray_counts = nullptr;   // debug mode KF_DEBUG_COUNTERS: raycast work counts
+    bool count_rays = false;
     // work-list entries reserved ahead for sessions not open yet (reserve_work)
     long long res_pre = 0, res_ray = 0, res_it = 0, res_fq = 0, res_vfq = 0;
     // pinned host
@@ -652,6 +654,7 @@ struct Engine {
         cudaFree(d_sess); cudaFree(d_step); cudaFree(d_out); cudaFree(d_tb); cudaFree(d_pre); cudaFree(d_ray);
         cudaFree(d_itiles); cudaFree(d_iranges); cudaFree(d_fprefix); cudaFree(d_bprefix); cudaFree(d_sprefix);
         cudaFree(d_vfprefix); cudaFree(d_vbprefix); cudaFree(d_vsprefix); cudaFree(d_vfuseq);
+        cudaFree(d_ray_counts);
         cudaFree(d_partials);
         cudaFree(d_icp_sched);
         cudaFree(d_icp_mats);
@@ -688,6 +691,7 @@ struct Engine {
         v.vis_super_prefix = d_vsprefix;
         v.vis_fuseq = d_vfuseq;
         v.vis_fuseq_cap = cap_vfuseq;
+        v.ray_counts = count_rays ? d_ray_counts : nullptr;
         return v;
     }
 
@@ -870,6 +874,7 @@ struct Engine {
         const EngineView v = view();
         KF_CK(cudaMemsetAsync(d_ctr, 0, sizeof(unsigned int) * kCounters, st));
         KF_CK(cudaMemsetAsync(d_sync, 0, sizeof(GridSync), st));
+        if (count_rays) KF_CK(cudaMemsetAsync(d_ray_counts, 0, sizeof(unsigned long long) * ray_count_slots(), st));
         if (profile) KF_CK(cudaEventRecordWithFlags(ev[0], st, cudaEventRecordExternal));
         const bool fork = stages[0] && stages[1];
         if (fork) {
@@ -2595,21 +2600,50 @@ static kf_status slot_set_debug(Engine& e, Slot& sl, int flags) {
         e.use_graph = graph;
         e.graph_dirty = true;
     }
+    const bool count = (flags & KF_DEBUG_COUNTERS) != 0;
+    if (count && !e.d_ray_counts) {
+        KF_CK(cudaMalloc(&e.d_ray_counts, sizeof(unsigned long long) * ray_count_slots()));
+        KF_CK(cudaMemset(e.d_ray_counts, 0, sizeof(unsigned long long) * ray_count_slots()));
+    }
+    if (count != e.count_rays) {
+        e.count_rays = count;
+        e.graph_dirty = true;   // the step launches the counting or the plain kernels
+    }
+    return KF_OK;
+}
+
+static kf_status engine_counts(Engine& e, uint64_t* out, int n) {
+    if (!out || n <= 0) return KF_ERR_ARG;
+    if (!e.count_rays || !e.d_ray_counts) return KF_ERR_STATE;
+    std::vector<unsigned long long> c(ray_count_slots());
+    KF_CK(cudaDeviceSynchronize());
+    KF_CK(cudaMemcpy(c.data(), e.d_ray_counts, sizeof(unsigned long long) * c.size(), cudaMemcpyDeviceToHost));
+    for (int k = 0; k < n; ++k) out[k] = k < int(c.size()) ? c[k] : 0;
     return KF_OK;
 }
 
 kf_status kf_session_set_debug(kf_session* s, int flags) {
-    if (!s || (flags & ~(KF_DEBUG_RAY_TRACE | KF_DEBUG_NO_GRAPH))) return KF_ERR_ARG;
+    if (!s || (flags & ~(KF_DEBUG_RAY_TRACE | KF_DEBUG_NO_GRAPH | KF_DEBUG_COUNTERS))) return KF_ERR_ARG;
     KF_CK(cudaDeviceSynchronize());
     return slot_set_debug(*s->eng, s->sl(), flags);
 }
 
 kf_status kf_batch_set_debug(kf_batch* b, int flags) {
-    if (!b || (flags & ~(KF_DEBUG_RAY_TRACE | KF_DEBUG_NO_GRAPH))) return KF_ERR_ARG;
+    if (!b || (flags & ~(KF_DEBUG_RAY_TRACE | KF_DEBUG_NO_GRAPH | KF_DEBUG_COUNTERS))) return KF_ERR_ARG;
     KF_CK(cudaDeviceSynchronize());
     for (Slot& sl : b->eng.slots)
         if (sl.used) KF_TRY(slot_set_debug(b->eng, sl, flags));
     return KF_OK;
+}
+
+kf_status kf_session_debug_counts(kf_session* s, uint64_t* out, int n) {
+    if (!s) return KF_ERR_ARG;
+    return engine_counts(*s->eng, out, n);
+}
+
+kf_status kf_batch_debug_counts(kf_batch* b, uint64_t* out, int n) {
+    if (!b) return KF_ERR_ARG;
+    return engine_counts(b->eng, out, n);
 }
 
 kf_status kf_get_ray_trace(kf_session* s, int level, uint64_t* dst, int to_host) {

@@ -87,6 +87,35 @@ __device__ __forceinline__ unsigned long long ray_trace_code(const RayState& st,
            static_cast<unsigned long long>((st.sw & 3) << 4) | static_cast<unsigned long long>(end);
 }
 
+// Work counts of the march, kept only by the kernels' counting instantiation (debug mode
+// KF_DEBUG_COUNTERS); the production instantiation compiles every count away.
+enum RayCount {
+    kCntRays = 0,        // rays that marched
+    kCntEvalLarge,       // samples evaluated (trilinear) during large steps
+    kCntEvalSmall,       // samples evaluated during small steps
+    kCntSkips,           // cell skips (each jumps over one or more samples)
+    kCntSkipped,         // samples jumped over by the skips
+    kCntGrad,            // gradient samples of hits (six per refined hit)
+    kCntQueued,          // rays handed from a lane to the long-ray warp kernel
+    kCntRounds,          // warp rounds of the long-ray kernel (32 or 64 samples each)
+    kRayCounts
+};
+
+template <bool kOn> struct MarchCount {
+    __device__ __forceinline__ void add(int, unsigned int) {}
+    __device__ __forceinline__ void flush(unsigned long long*) {}
+};
+template <> struct MarchCount<true> {
+    unsigned int c[kRayCounts] = {};
+    __device__ __forceinline__ void add(int k, unsigned int x) { c[k] += x; }
+    __device__ __forceinline__ void flush(unsigned long long* dst) {
+        if (!dst) return;
+#pragma unroll
+        for (int k = 0; k < kRayCounts; ++k)
+            if (c[k]) atomicAdd(dst + k, static_cast<unsigned long long>(c[k]));
+    }
+};
+
 // a ray handed from a lane to a warp: where it is, its exact march state and its geometry (so
 // the warp neither reloads the pose nor divides again)
 struct __align__(16) LongRay {
@@ -226,9 +255,9 @@ __device__ __forceinline__ bool skip_cell(const SessionDev* S, const RayGeo& g, 
 // The reference's march loop for one lane (project/src/raycast.cu:75-117).  Returns 1 when
 // the ray is finished (precise = refined hit distance, 0 for none) and 0 when `budget`
 // iterations ran out with the ray still marching (state kept in st).
-template <class TF>
+template <class TF, class Cnt>
 __device__ int march_serial(const SessionDev* S, const RayGeo& g, const TF* f, RayState& st, int budget,
-                            float& precise) {
+                            float& precise, Cnt& cnt) {
     const int n = S->n;
     const float mu = S->mu, large = mu * S->step_l, small = mu * S->step_s;
     const int* __restrict__ bdil = S->bdil;
@@ -239,8 +268,14 @@ __device__ int march_serial(const SessionDev* S, const RayGeo& g, const TF* f, R
         float x, y, z;
         texel(g, st.t, x, y, z);
         const TexelBase tb = texel_base(n, x, y, z);
-        if (bdil && skip_cell(S, g, st, tb.x0, tb.y0, tb.z0, inc)) continue;
+        const int g0 = st.guard;
+        if (bdil && skip_cell(S, g, st, tb.x0, tb.y0, tb.z0, inc)) {
+            cnt.add(kCntSkips, 1u);
+            cnt.add(kCntSkipped, unsigned(st.guard - g0));
+            continue;
+        }
         const float tsdf = trilinear_at(f, n, tb);
+        cnt.add(st.small ? kCntEvalSmall : kCntEvalLarge, 1u);
         ++st.guard;
         if (tsdf < 0.0f) {
             if (st.t != st.near_d) {
@@ -278,9 +313,9 @@ __device__ int march_serial(const SessionDev* S, const RayGeo& g, const TF* f, R
 // A round that follows a round without any such sample takes two sets, samples k and 32 + k
 // (such rays are in a long run of samples that change nothing, a grazing ray in small steps
 // for instance); the first event in sample order is applied all the same.
-template <class TF>
+template <class TF, class Cnt>
 __device__ void march_coop(const SessionDev* S, const RayGeo& g, const TF* f, RayState& st, int lane,
-                           float& precise) {
+                           float& precise, Cnt& cnt) {
     const float mu = S->mu, large = mu * S->step_l, small = mu * S->step_s;
     const unsigned int full = 0xffffffffu;
     bool wide = false;   // the last round changed nothing
@@ -290,7 +325,12 @@ __device__ void march_coop(const SessionDev* S, const RayGeo& g, const TF* f, Ra
             float x, y, z;
             texel(g, st.t, x, y, z);
             const TexelBase tb = texel_base(S->n, x, y, z);
+            const int g0 = st.guard;
             if (skip_cell(S, g, st, tb.x0, tb.y0, tb.z0, inc)) {   // every lane takes the same steps
+                if (lane == 0) {
+                    cnt.add(kCntSkips, 1u);
+                    cnt.add(kCntSkipped, unsigned(st.guard - g0));
+                }
                 wide = false;
                 continue;
             }
@@ -304,7 +344,11 @@ __device__ void march_coop(const SessionDev* S, const RayGeo& g, const TF* f, Ra
             valid[j] = (j == 0 || wide) && tk[j] < st.far_d && st.guard + n < kMaxMarchSamples;
         }
 #pragma unroll
-        for (int j = 0; j < 2; ++j) fk[j] = valid[j] ? sample_at(S, g, f, tk[j]) : 0.0f;
+        for (int j = 0; j < 2; ++j) {
+            fk[j] = valid[j] ? sample_at(S, g, f, tk[j]) : 0.0f;
+            if (valid[j]) cnt.add(st.small ? kCntEvalSmall : kCntEvalLarge, 1u);
+        }
+        if (lane == 0) cnt.add(kCntRounds, 1u);
         unsigned int evm[2], valm[2];
 #pragma unroll
         for (int j = 0; j < 2; ++j) {
@@ -412,13 +456,14 @@ __device__ __forceinline__ void write_trace(const SessionDev* S, int level, int 
     if (tr) tr[size_t(j) * S->lv[level].w + i] = code;
 }
 
-template <class TF>
+template <class TF, class Cnt>
 __device__ void finish_ray(const SessionDev* S, const RayGeo& g, const TF* f, int level, int i, int j, float precise,
-                           const RayState& st) {
+                           const RayState& st, Cnt& cnt) {
     write_trace(S, level, i, j, ray_trace_code(st, precise));
     const HitGeo h = hit_geo(S, g, precise);
     float v[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
     if (precise != 0.0f) {
+        cnt.add(kCntGrad, 6u);
 #pragma unroll
         for (int q = 0; q < 6; ++q) v[q] = grad_sample(f, S->n, h, q);
     }
@@ -427,13 +472,16 @@ __device__ void finish_ray(const SessionDev* S, const RayGeo& g, const TF* f, in
 
 // the same for a ray carried by a whole warp: lanes 0-5 take one gradient sample each, lane 0
 // writes
-template <class TF>
+template <class TF, class Cnt>
 __device__ void finish_ray_warp(const SessionDev* S, const RayGeo& g, const TF* f, int level, int i, int j,
-                                float precise, int lane, const RayState& st) {
+                                float precise, int lane, const RayState& st, Cnt& cnt) {
     if (lane == 0) write_trace(S, level, i, j, ray_trace_code(st, precise));
     const HitGeo h = hit_geo(S, g, precise);
     float mine = 0.f;
-    if (precise != 0.0f && lane < 6) mine = grad_sample(f, S->n, h, lane);
+    if (precise != 0.0f && lane < 6) {
+        mine = grad_sample(f, S->n, h, lane);
+        cnt.add(kCntGrad, 1u);
+    }
     float v[6];
 #pragma unroll
     for (int q = 0; q < 6; ++q) v[q] = __shfl_sync(0xffffffffu, mine, q);
@@ -448,9 +496,9 @@ __device__ __forceinline__ void write_miss(const SessionDev* S, int level, int i
     S->pn[level][size_t(j) * w + i] = make_float4(0.f, 0.f, 0.f, kInvalid);
 }
 
-template <class TF>
+template <class TF, class Cnt>
 __device__ void serial_ray(const EngineView& v, const SessionDev* S, int s, const float* m, F3 o, int level, int i,
-                           int j, int budget) {
+                           int j, int budget, Cnt& cnt) {
     const TF* f = static_cast<const TF*>(S->tf);
     RayGeo g;
     make_geo(S, m, o, i, j, g);
@@ -459,23 +507,26 @@ __device__ void serial_ray(const EngineView& v, const SessionDev* S, int s, cons
         write_miss(S, level, i, j);
         return;
     }
+    cnt.add(kCntRays, 1u);
     float precise = 0.0f;
-    if (!march_serial(S, g, f, st, budget, precise)) {
+    if (!march_serial(S, g, f, st, budget, precise, cnt)) {
         const unsigned int slot = atomicAdd(&v.counters[6], 1u);
         if (slot < unsigned(v.longq_cap)) {
             v.longq[slot] = LongRay{s, level, i, j, st, g};
+            cnt.add(kCntQueued, 1u);
             return;
         }
-        march_serial(S, g, f, st, 0x7fffffff, precise);   // queue full: finish here
+        march_serial(S, g, f, st, 0x7fffffff, precise, cnt);   // queue full: finish here
     }
-    finish_ray(S, g, f, level, i, j, precise, st);
+    finish_ray(S, g, f, level, i, j, precise, st, cnt);
 }
 
 // Each warp pulls 8 x 4-ray tiles on its own (no block-wide barrier).  Steps of many ray tiles
 // run four blocks per SM (64 registers: more warps to hide the gathers behind); a single
 // session's step runs three (80 registers: fewer instructions per sample, a shorter tail).
-template <int kBlocksPerSm>
+template <int kBlocksPerSm, bool kCount>
 __global__ void __launch_bounds__(256, kBlocksPerSm) raycast_kernel(EngineView v) {
+    MarchCount<kCount> cnt;
     const int lane = threadIdx.x & 31;
     const int ntiles = v.tb->n_ray;
     const int budget = v.tb->ray_budget;
@@ -497,24 +548,27 @@ __global__ void __launch_bounds__(256, kBlocksPerSm) raycast_kernel(EngineView v
         F3 o;
         ray_matrix(S, Lv, m, o);
         if (S->fmt == KF_TSDF_F16U16)
-            serial_ray<__half>(v, S, T.s, m, o, T.level, i, j, budget);
+            serial_ray<__half>(v, S, T.s, m, o, T.level, i, j, budget, cnt);
         else
-            serial_ray<float>(v, S, T.s, m, o, T.level, i, j, budget);
+            serial_ray<float>(v, S, T.s, m, o, T.level, i, j, budget, cnt);
     }
+    cnt.flush(v.ray_counts);
 }
 
-template <class TF>
-__device__ void coop_ray(const SessionDev* S, const LongRay& L, int lane) {
+template <class TF, class Cnt>
+__device__ void coop_ray(const SessionDev* S, const LongRay& L, int lane, Cnt& cnt) {
     const TF* f = static_cast<const TF*>(S->tf);
     const RayGeo g = L.g;
     RayState st = L.st;
     float precise = 0.0f;
-    march_coop(S, g, f, st, lane, precise);
-    finish_ray_warp(S, g, f, L.level, L.i, L.j, precise, lane, st);
+    march_coop(S, g, f, st, lane, precise, cnt);
+    finish_ray_warp(S, g, f, L.level, L.i, L.j, precise, lane, st, cnt);
 }
 
 // the queued long rays, one warp each
+template <bool kCount>
 __global__ void __launch_bounds__(256) raycast_long_kernel(EngineView v) {
+    MarchCount<kCount> cnt;
     const int lane = threadIdx.x & 31;
     const int count = min(int(v.counters[6]), v.longq_cap);
     while (true) {
@@ -525,24 +579,32 @@ __global__ void __launch_bounds__(256) raycast_long_kernel(EngineView v) {
         const LongRay L = v.longq[idx];
         const SessionDev* S = &v.sess[L.s];
         if (S->fmt == KF_TSDF_F16U16)
-            coop_ray<__half>(S, L, lane);
+            coop_ray<__half>(S, L, lane, cnt);
         else
-            coop_ray<float>(S, L, lane);
+            coop_ray<float>(S, L, lane, cnt);
     }
+    cnt.flush(v.ray_counts);
 }
 
 int long_ray_bytes() { return int(sizeof(LongRay)); }
 
 cudaError_t launch_raycast(const EngineView& v, int grid, cudaStream_t st, bool many) {
-    if (many)
-        raycast_kernel<4><<<grid, 256, 0, st>>>(v);
-    else
-        raycast_kernel<3><<<grid, 256, 0, st>>>(v);
+    const bool count = v.ray_counts != nullptr;
+    if (count) {
+        if (many) raycast_kernel<4, true><<<grid, 256, 0, st>>>(v);
+        else raycast_kernel<3, true><<<grid, 256, 0, st>>>(v);
+    } else {
+        if (many) raycast_kernel<4, false><<<grid, 256, 0, st>>>(v);
+        else raycast_kernel<3, false><<<grid, 256, 0, st>>>(v);
+    }
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
-    raycast_long_kernel<<<grid, 256, 0, st>>>(v);
+    if (count) raycast_long_kernel<true><<<grid, 256, 0, st>>>(v);
+    else raycast_long_kernel<false><<<grid, 256, 0, st>>>(v);
     return cudaGetLastError();
 }
+
+int ray_count_slots() { return kRayCounts; }
 
 // ---- stage kernel: kernel::raycast on a caller volume ----
 
@@ -564,8 +626,9 @@ __global__ void raycast_stage_kernel(SessionDev S, RayStage rs, int w, int h) {
         return;
     }
     float precise = 0.0f;
-    march_serial(&S, g, f, st, 0x7fffffff, precise);
-    finish_ray(&S, g, f, 0, i, j, precise, st);
+    MarchCount<false> cnt;
+    march_serial(&S, g, f, st, 0x7fffffff, precise, cnt);
+    finish_ray(&S, g, f, 0, i, j, precise, st, cnt);
 }
 
 cudaError_t stage_raycast(const kf_volume* vol, const float* pose, const float* ik, float4* vtx, float4* nrm, int w,

@@ -63,6 +63,7 @@ struct EngineView {
     int fuseq_cap;
     unsigned int* vis_fuseq;     // the visualization volumes' fusion queue
     int vis_fuseq_cap;
+    unsigned long long* ray_counts;   // debug mode: the raycast's work counts (null: not counted)
 };
 
 constexpr int kPreTileSize = 32;
@@ -85,6 +86,7 @@ cudaError_t launch_preprocess(const EngineView& v, int grid, cudaStream_t st);
 // many: a step of more than kManyRayTiles ray tiles (serial_budget's rule)
 cudaError_t launch_raycast(const EngineView& v, int grid, cudaStream_t st, bool many);
 int serial_budget_many();   // the lane budget of the raycast's many-tile form
+int ray_count_slots();      // entries of the raycast's debug work counts
 // single: an engine of one slot (the kernel keeps that session's state per block)
 cudaError_t launch_icp(const EngineView& v, int grid, cudaStream_t st, bool single);
 cudaError_t launch_fuse(const EngineView& v, int grid, cudaStream_t st);

@@ -19,10 +19,11 @@ import os
 import numpy as np
 
 from . import _lib
-from ._lib import (KF_DEBUG_NO_GRAPH, KF_DEBUG_RAY_TRACE, KF_ERR_ARG, KF_ERR_CAPACITY, KF_ERR_CUDA, KF_ERR_NONFINITE, KF_ERR_OOM_BUDGET, KF_ERR_SHAPE,
-                   KF_ERR_STATE, KF_ERR_TIMEOUT, KF_MAX_LEVELS, KF_OK, KF_RENDER_NORMALS, KF_RENDER_SHADING,
-                   KF_TSDF_F16U16, KF_TSDF_F32F32, KF_WEIGHT_SCALE, KfConfig, KfError, KfFrameStats, KfServerStats,
-                   KfVolume, check, lib)
+from ._lib import (KF_DEBUG_COUNTERS, KF_DEBUG_NO_GRAPH, KF_DEBUG_RAY_TRACE, KF_ERR_ARG, KF_ERR_CAPACITY,
+                   KF_ERR_CUDA, KF_ERR_NONFINITE, KF_ERR_OOM_BUDGET, KF_ERR_SHAPE, KF_ERR_STATE, KF_ERR_TIMEOUT,
+                   KF_MAX_LEVELS, KF_OK, KF_RENDER_NORMALS, KF_RENDER_SHADING, KF_TSDF_F16U16, KF_TSDF_F32F32,
+                   KF_WEIGHT_SCALE, RAY_COUNT_NAMES, KfConfig, KfError, KfFrameStats, KfServerStats, KfVolume, check,
+                   lib)
 
 __all__ = [
     "KfConfig", "KfError", "default_config", "config_small", "config_full", "KinectFusion", "kernel", "ICP",
@@ -362,6 +363,12 @@ class KinectFusion:
         plain launches per stage inside NVTX ranges instead of the captured graph)."""
         check(lib.kf_session_set_debug(self._s, int(flags)), "kf_session_set_debug")
 
+    def debug_counts(self):
+        """The raycast's work counts of the last step (KF_DEBUG_COUNTERS), as a dict."""
+        c = np.zeros(len(RAY_COUNT_NAMES), np.uint64)
+        check(lib.kf_session_debug_counts(self._s, _np_ptr(c), len(c)), "kf_session_debug_counts")
+        return {k: int(v) for k, v in zip(RAY_COUNT_NAMES, c)}
+
     def ray_trace(self, level=0):
         """(h, w) int64 march decision traces of the last raycast at `level` (debug mode)."""
         w, h = self._lw(level)
@@ -684,6 +691,12 @@ class Batch:
     def set_debug(self, flags):
         """Debug modes for every session of the batch (see KinectFusion.set_debug)."""
         check(lib.kf_batch_set_debug(self._b, int(flags)), "kf_batch_set_debug")
+
+    def debug_counts(self):
+        """The raycast's work counts of the last step (KF_DEBUG_COUNTERS), as a dict."""
+        c = np.zeros(len(RAY_COUNT_NAMES), np.uint64)
+        check(lib.kf_batch_debug_counts(self._b, _np_ptr(c), len(c)), "kf_batch_debug_counts")
+        return {k: int(v) for k, v in zip(RAY_COUNT_NAMES, c)}
 
 
 def selftest_bounded_wait(timeout_ms=50):

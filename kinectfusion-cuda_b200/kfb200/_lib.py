@@ -28,6 +28,9 @@ KF_RENDER_NORMALS = 0
 KF_RENDER_SHADING = 1
 KF_DEBUG_RAY_TRACE = 1
 KF_DEBUG_NO_GRAPH = 2
+KF_DEBUG_COUNTERS = 4
+KF_RAY_COUNTS = 8
+RAY_COUNT_NAMES = ("rays", "eval_large", "eval_small", "skips", "skipped", "gradient", "queued", "long_rounds")
 KF_MAX_FRAMES_IN_FLIGHT = 4
 
 KF_TSDF_F32F32 = 0
@@ -166,6 +169,8 @@ SIGNATURES = {
     "kf_session_stage_times": (_I, [_P, _FP]),
     "kf_session_set_debug": (_I, [_P, _I]),
     "kf_batch_set_debug": (_I, [_P, _I]),
+    "kf_session_debug_counts": (_I, [_P, _P, _I]),
+    "kf_batch_debug_counts": (_I, [_P, _P, _I]),
     "kf_get_ray_trace": (_I, [_P, _I, _P, _I]),
     "kf_batch_set_profiling": (_I, [_P, _I]),
     "kf_batch_stage_times": (_I, [_P, _FP]),

@@ -285,14 +285,22 @@ def test_bilateral_radius_zero_and_single_level(kf, orc):
 
 
 def test_debug_modes_change_no_result(kf, run_small):
-    """Plain launches per stage (KF_DEBUG_NO_GRAPH, the mode for profiling a stage) and the
-    decision-trace recording give the same poses as the replayed graph, bit for bit."""
+    """Plain launches per stage (KF_DEBUG_NO_GRAPH, the mode for profiling a stage), the
+    decision-trace recording and the raycast's counting kernels give the same poses as the
+    replayed graph, bit for bit."""
     cfg, imgs, s, P, rows = run_small
     s2 = kf.KinectFusion(cfg)
-    s2.set_debug(kf.KF_DEBUG_NO_GRAPH | kf.KF_DEBUG_RAY_TRACE)
+    s2.set_debug(kf.KF_DEBUG_NO_GRAPH | kf.KF_DEBUG_RAY_TRACE | kf.KF_DEBUG_COUNTERS)
     for i in range(5):
         st, pose = s2.process_frame(imgs[i])
         np.testing.assert_array_equal(pose, rows[i][2])
+        c = s2.debug_counts()
+        if i == 0:
+            assert c["rays"] == 0   # the first frame fuses only
+        else:
+            # every pixel of every level marches; samples are evaluated, skipped or taken by warps
+            assert 0 < c["rays"] <= sum((cfg.width >> l) * (cfg.height >> l) for l in range(cfg.levels))
+            assert c["eval_large"] + c["eval_small"] > c["rays"] and c["skips"] > 0 and c["gradient"] % 6 == 0
     s2.set_debug(0)
     st, pose = s2.process_frame(imgs[5])
     np.testing.assert_array_equal(pose, rows[5][2])
