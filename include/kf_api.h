@@ -361,7 +361,8 @@ kf_status kf_batch_session(kf_batch* b, int i, kf_session** out);
  * pixels per warp) and how fusion splits its queue entries; none of them changes a result, bit
  * for bit.  After this call each kf_batch_step runs one candidate shape and its stage times
  * (device events) are recorded; a walk over the parameters, one at a time, keeps the fastest
- * candidate of each, and after the last step of the walk the batch keeps the chosen shape.
+ * candidate of each (by the step's device time), and after the last step of the walk the
+ * batch keeps the chosen shape.
  * cache_path (may be NULL): a JSON file of chosen shapes keyed by the batch's session mix
  * (frame sizes, volumes, formats, counts) and the device's SM count; if it holds an entry for
  * this mix, that shape is applied at once and no step is spent tuning, else the walk's result
@@ -369,8 +370,8 @@ kf_status kf_batch_session(kf_batch* b, int i, kf_session** out);
  * counterpart (its launch shapes are fixed 8 x 8 blocks). */
 kf_status kf_batch_autotune_start(kf_batch* b, const char* cache_path);
 /* Steps the walk still needs (0 when done or not started) and a JSON report: the mix key, the
- * source of the shape ("tuned" or "cache") and the shape, with each parameter's winning stage
- * time when tuned. */
+ * source of the shape ("tuned" or "cache") and the shape, with each parameter's winning step
+ * time (ms) when tuned. */
 kf_status kf_batch_autotune_status(kf_batch* b, int* steps_left, char* report, size_t report_bytes);
 
 /* ------------------------------------------------------------------------------------------ */
