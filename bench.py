@@ -9,9 +9,12 @@ Workload (one step = one frame through preprocess -> raycast -> ICP -> fusion):
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
---impl reference times the reference's algorithm on the host cores: the CPU restatement in
-oracle/ (the reference has no CPU path and its CUDA build needs glm, which is absent), float
-instantiation, OpenMP over all cores, on the same frames.  Under torchrun only rank 0 runs it.
+--impl reference times the reference's own pipeline: its CUDA kernels, ICP and least-squares
+code compiled from its sources for sm_100a (oracle/_ref, built by oracle/Makefile), driven frame
+by frame as its tracking loop drives them, on the same frames and configuration (the bilateral
+filter's constants are compiled into the reference and stay its own).  Where that build is
+absent the arm times the CPU restatement in oracle/ instead (float, OpenMP over all cores).
+Under torchrun only rank 0 runs it.
 Multi-GPU (torchrun, N ranks): each rank runs its own independent session (weak scaling, no
 collective in the data path); times are device events, max over ranks.
 """
@@ -203,7 +206,53 @@ def plain_config(world):
             "parallelism": "replicas" if world > 1 else "single"}
 
 
-REF_MAX_STEPS = 120   # timed frames of the CPU reference arm (about 25 s on 16 cores)
+REF_MAX_STEPS = 120    # timed frames of the CPU restatement (about 25 s on 16 cores)
+REF_GPU_MAX_STEPS = 3000   # timed frames of the reference's own pipeline (about 3 ms each)
+
+
+def reference_line(cfg, fps, steps, warmup, dt, cpu_baseline, note, **extra):
+    line = {
+        "impl": "reference", "metric": "frames/s", "value": round(fps, 4), "unit": "frames/s",
+        "n_gpus": extra.pop("n_gpus", 0), "steps": steps, "warmup": warmup, "ms_per_step": round(1000 * dt / steps, 4),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": plain_config(1), "cpu_baseline": cpu_baseline,
+        "e2e": {"value": round(fps, 4), "unit": "frames/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "note": note,
+    }
+    line.update(extra)
+    return line
+
+
+def run_reference_gpu(args, kf, cfg):
+    """The reference's own pipeline (oracle/_ref) on cuda:0: frame 0 as its initializeTracking,
+    then its loop's preprocess, raycast of every level, ICP::computePose and fusion, each frame
+    uploaded from host memory (DepthMap::update); wall-clock over the timed frames."""
+    import refpipe
+    steps, warmup = min(args.steps, REF_GPU_MAX_STEPS), args.warmup
+    imgs, _ = render_frames(kf, cfg, 300, seed=1)   # the closed loop; cycled frames stay continuous
+    frames = np.ascontiguousarray(np.stack(imgs))
+    R = refpipe.RefPipeline(cfg)
+    progress("reference pipeline: warm-up")
+    R.time_frames(frames, 1 + warmup)
+    before = R.stage_times()
+    progress("reference pipeline: %d timed frames" % steps)
+    dt, st = R.time_frames(np.roll(frames, -(1 + warmup), axis=0), steps)
+    stages = (R.stage_times() - before) / steps
+    R.close()
+    fps = steps / dt
+    names = ["preprocess", "raycast", "icp_residuals", "icp_solve_host", "fuse", "visualization"]
+    return reference_line(
+        cfg, fps, steps, warmup, dt,
+        {"value": round(fps, 4), "unit": "frames/s", "cores": 1, "kind": "reference",
+         "sample": "%d frames of the full-size workload after 1 + %d untimed, one host thread driving the "
+                   "reference's CUDA kernels on cuda:0" % (steps, warmup)},
+        "the reference's own pipeline: project/src kernels, ICP::computePose (cuBLAS + Eigen) and VoxelGrid "
+        "compiled from its sources for sm_100a with its Release flags (oracle/Makefile), driven as "
+        "KinectFusion::startTracking drives them (oracle/ref_harness.cpp), on one B200; its bilateral "
+        "filter keeps its compiled-in 4 px / 0.25 m / 7x7; no visualization grid (the plain line has none)",
+        n_gpus=1,
+        reference_stage_ms={k: round(float(v), 4) for k, v in zip(names, stages)},
+        frames_icp_nonfinite=int(np.sum(st == refpipe.NONFINITE)))
 
 
 def run_reference(args, world, rank):
@@ -211,6 +260,15 @@ def run_reference(args, world, rank):
         return
     import kfb200 as kf
     cfg = full_config(kf)
+    try:
+        import refpipe
+        import torch
+        gpu_ref = refpipe.available() and torch.cuda.is_available()
+    except Exception:
+        gpu_ref = False
+    if gpu_ref:
+        print(json.dumps(run_reference_gpu(args, kf, cfg)), flush=True)
+        return
     # a bounded sample of the same workload: at most REF_MAX_STEPS timed frames
     steps, warmup = min(args.steps, REF_MAX_STEPS), min(args.warmup, 3)
     imgs, _ = render_frames(kf, cfg, 1 + warmup + steps, seed=1)
@@ -224,19 +282,13 @@ def run_reference(args, world, rank):
         P.process_frame(imgs[1 + warmup + i])
     dt = time.perf_counter() - t0
     fps = steps / dt
-    cores = os.cpu_count()
-    line = {
-        "impl": "reference", "metric": "frames/s", "value": round(fps, 4), "unit": "frames/s", "n_gpus": 0,
-        "steps": steps, "warmup": warmup, "ms_per_step": round(1000 * dt / steps, 3), "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": plain_config(1),
-        "cpu_baseline": {"value": round(fps, 4), "unit": "frames/s", "cores": cores, "kind": "port",
-                         "sample": "%d timed frames of the full-size workload after 1 + %d untimed (at most %d "
-                                   "timed per run)" % (steps, warmup, REF_MAX_STEPS)},
-        "e2e": {"value": round(fps, 4), "unit": "frames/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
-        "note": "the reference's CUDA build needs glm (absent) and runs only on Windows; this arm is its "
-                "algorithm restated on the CPU (oracle/kf_oracle.cpp), float, OpenMP over all host cores",
-    }
+    line = reference_line(
+        cfg, fps, steps, warmup, dt,
+        {"value": round(fps, 4), "unit": "frames/s", "cores": os.cpu_count(), "kind": "port",
+         "sample": "%d timed frames of the full-size workload after 1 + %d untimed (at most %d timed per run)"
+                   % (steps, warmup, REF_MAX_STEPS)},
+        "the reference's own build (oracle/_ref) is absent here; this arm is its algorithm restated on the CPU "
+        "(oracle/kf_oracle.cpp), float, OpenMP over all host cores")
     print(json.dumps(line), flush=True)
 
 
@@ -851,7 +903,55 @@ def run_accuracy(kf, full_frames=6, small_frames=30, drift_frames=150, full_drif
     out["full_f16u16"] = synced_errors(kf, orc, f16, fimgs[:full_frames])
     if full_drift_frames > 0:
         out["full_f16u16_drift"] = drift(kf, orc, f16, fimgs[:full_drift_frames], fgts)
+    ref = reference_pipeline_errors(kf, orc)
+    if ref is not None:
+        out["reference_pipeline"] = ref
     return out
+
+
+def reference_pipeline_errors(kf, orc, frames=5):
+    """The library against the reference's own pipeline built here (oracle/_ref) and the FP64
+    oracle, synced per frame, at the reference's constants (refpipe.matching_config) with a
+    512^3 f32 volume over 3 m; None when that build is absent."""
+    import refpipe
+    import torch
+    from kfb200 import synth
+    if not refpipe.available():
+        return None
+    cfg = refpipe.matching_config(kf, depth_scale=1e-3, volume_n=512, volume_width=3.0,
+                                  initial_pose=kf.start_pose(3.0), vis_volume_n=0, keep_on_miss=0)
+    imgs, _ = synth.sequence(cfg, frames, seed=3, kind=synth.LOOP)
+    rows = refpipe.compare_synced(kf, orc, torch, cfg, imgs)
+    tracked = rows[1:]
+    rays = [p for r in tracked for p in r["rays"]]
+
+    def mx(key, sub):
+        return max(r["pose"][key][sub] for r in tracked)
+    return {
+        "config": "640x480, the reference's constants (bilateral 4 px / 0.25 m / 7x7, mu 3 voxels, ICP 10/5/3 at "
+                  "0.4 m / 40 deg, its early stop), 512^3 f32 over 3 m; %d frames of the seeded loop, the reference "
+                  "and the FP64 oracle synced to the library's volume and pose every frame" % frames,
+        "pyramid_bit_exact": all(r["meters"] and all(a and b for a, b in r.get("pyramid", [])) for r in rows),
+        "icp_mask_agreement_min": round(min(a for r in tracked for a in r["icp_masks"]), 6),
+        "tsdf_trunc_max_nonflip": max(r["tsdf"]["max_nonflip"] for r in rows),
+        "tsdf_boundary_flips": sum(r["tsdf"]["boundary_flips"] for r in rows),
+        "tsdf_voxels_touched": sum(r["tsdf"]["touched"] for r in rows),
+        "raycast_hit_agreement_min": round(min(p["hit_agreement"] for p in rays), 6),
+        "raycast_both_hit": sum(p["both"] for p in rays),
+        "raycast_lib_vs_ref_over_1mm": sum(p["lib_ref_over_1mm"] for p in rays),
+        "raycast_ref_vs_fp64_over_1mm": sum(p["ref_fp64_over_1mm"] for p in rays),
+        "raycast_lib_vs_fp64_over_1mm": sum(p["lib_fp64_over_1mm"] for p in rays),
+        "raycast_lib_vs_ref_over_1mm_unexplained": sum(p["unexplained"] for p in rays),
+        "raycast_median_mm": {"lib_vs_ref": round(max(p["lib_ref_median_mm"] for p in rays), 5),
+                              "ref_vs_fp64": round(max(p["ref_fp64_median_mm"] for p in rays), 5),
+                              "lib_vs_fp64": round(max(p["lib_fp64_median_mm"] for p in rays), 5)},
+        "pose_max": {"lib_vs_fp64": [mx("lib_fp64", 0), mx("lib_fp64", 1)],
+                     "ref_vs_fp64": [mx("ref_fp64", 0), mx("ref_fp64", 1)],
+                     "lib_vs_ref": [mx("lib_ref", 0), mx("lib_ref", 1)]},
+        "note": "the reference raycasts through hardware texture filtering (8 fractional bits in the "
+                "interpolation weights); the library interpolates in exact float arithmetic, so its "
+                "differences from the reference are the reference's own differences from the FP64 oracle",
+    }
 
 
 def run_ours(args, world, rank, local):

@@ -19,6 +19,11 @@ REPO = os.path.dirname(HERE)
 
 CU_SOURCES = ["k_preprocess.cu", "k_raycast.cu", "k_tsdf.cu", "k_icp.cu", "k_display.cu", "k_probe.cu", "api.cu"]
 CXX_SOURCES = ["dataset.cpp"]   # host-only parts of the library (zlib for 16-bit PNG)
+# The depth pyramid is computed with the float semantics of the reference's Release build
+# (FastMath, project/project.vcxproj:139): denormals flushed, division and square root to the
+# fast forms.  With the same operations in the same order, the converted, filtered and
+# down-sampled depth and the vertex maps are then bit-identical to the reference's kernels.
+FILE_FLAGS = {"k_preprocess.cu": ["-ftz=true", "-prec-div=false", "-prec-sqrt=false", "-fmad=true"]}
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",
     "-lineinfo", "-O3", "-std=c++17",
@@ -67,8 +72,8 @@ def build(verbose=False, ptxas_info=False):
         s = os.path.join(CSRC, src)
         o = os.path.join(OBJ, src.replace(".cu", ".o"))
         objs.append(o)
-        if ptxas_info or _stale(o, [s] + headers):
-            jobs.append([nvcc] + NVCC_FLAGS + extra + ["-c", s, "-o", o])
+        if ptxas_info or _stale(o, [s] + headers + [os.path.abspath(__file__)]):
+            jobs.append([nvcc] + NVCC_FLAGS + FILE_FLAGS.get(src, []) + extra + ["-c", s, "-o", o])
     for src in CXX_SOURCES:
         s = os.path.join(CSRC, src)
         o = os.path.join(OBJ, src.replace(".cpp", ".o"))

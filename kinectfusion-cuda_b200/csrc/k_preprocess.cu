@@ -9,6 +9,12 @@
 // its filter halo into shared memory once, filters from there, and produces the 16x16 and
 // 8x8 tiles of levels 1 and 2 and all vertex maps without touching HBM again.  All sessions'
 // tiles form one work list, so a single launch serves a whole batch.
+//
+// This file is compiled with the float semantics of the reference's Release build (FastMath,
+// project/project.vcxproj:139: denormals flushed, fast division and square root; see
+// build.py), and each core below performs the reference's operations in the reference's
+// order, so the converted, filtered and down-sampled depth maps and the vertex maps are
+// bit-identical to those of the reference's own kernels.
 #include "kf_host.h"
 
 namespace kf {
@@ -16,8 +22,8 @@ namespace kf {
 // ---- per-pixel cores shared by the fused kernel and the stage kernels ----
 
 // applyBilateralFilterKernel body (project/src/measurement.cu:45-65): x outer, y inner,
-// exp(-dx2/ss^2 - dr2/sr^2) with the fast exponential the reference's -use_fast_math
-// build selects, then acc / norm.  rd(x, y) returns the clamped neighbour.
+// exp(-dx2/ss^2 - dr2/sr^2) with the fast exponential the reference's fast-math build
+// selects, then acc / norm.  rd(x, y) returns the clamped neighbour.
 template <class Reader>
 __device__ __forceinline__ float bilateral_core(Reader rd, int R, float inv_ss, float inv_sr) {
     const float center = rd(0, 0);

@@ -76,12 +76,20 @@ def test_bilateral_vs_oracle(kf, orc, cuda, frames_small, ss, sr, r):
     np.testing.assert_allclose(got[valid], want[valid], rtol=2e-6)
 
 
-def test_down_sample_bit_exact(kf, orc, cuda, frames_small):
+def test_down_sample_vs_oracle(kf, orc, cuda, frames_small):
+    """The same gating and sums as the oracle; the mean divides the way the reference's
+    fast-math build does (at most 2 ulp from IEEE division, exact for 1, 2 or 4 terms), so the
+    oracle's IEEE quotient is matched within 2 ulp.  Bit-exactness is checked against the
+    reference's own kernel (test_gpu_reference_pipeline.py)."""
     cfg, imgs, _ = frames_small
     d = orc.bilateral(orc.convert(imgs[3], cfg.depth_scale), 4.5, 0.03, 2)
     out = cuda.zeros((cfg.height // 2, cfg.width // 2), dtype=cuda.float32, device="cuda")
     kf.kernel.downSample(dev(cuda, d), out, 0.03)
-    np.testing.assert_array_equal(host(out), orc.down_sample(d, 0.03))
+    got = np.ascontiguousarray(host(out), np.float32)
+    want = np.ascontiguousarray(orc.down_sample(d, 0.03), np.float32)
+    np.testing.assert_array_equal(got > 0.01, want > 0.01)
+    ulps = np.abs(got.view(np.int32).astype(np.int64) - want.view(np.int32).astype(np.int64))
+    assert int(ulps.max()) <= 2, int(ulps.max())
 
 
 def test_vertex_and_normal_maps(kf, orc, cuda, frames_small):
