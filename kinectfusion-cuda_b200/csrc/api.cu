@@ -431,9 +431,15 @@ kf_status grow(T*& ptr, int& cap, int need) {
     return KF_OK;
 }
 
-// The long-ray queue holds 1 / kLongRayShare of a step's rays (about 4 % of a frame's rays take
-// the long-ray path; more than the queue holds finish in their lane).
+// The long-ray queue holds 1 / kLongRayShare of a step's rays (about 2 % of a frame's rays take
+// the long-ray path; more than the queue holds finish in their lane, several times slower), and
+// at least a quarter of them up to kLongRayFloor entries, so that a small step (one session)
+// has room for a scene with many more grazing rays.
 constexpr int kLongRayShare = 16;
+constexpr long long kLongRayFloor = 1 << 18;
+long long long_ray_entries(long long rays) {
+    return std::max(std::max(1024LL, rays / kLongRayShare), std::min(rays / 4, kLongRayFloor));
+}
 
 // Launch shapes of a step.  Every value gives the same results bit for bit -- they only change
 // which block or lane does which part of the work -- so they can be tuned on live steps.
@@ -724,7 +730,7 @@ struct Engine {
         const long long need_it = cur_it + res_it;
         const long long need_fq = tb.fuse_total + res_fq;
         const long long need_vfq = tb.vis_fuse_total + res_vfq;
-        if (need_pre > INT32_MAX || need_ray * 32 / kLongRayShare > INT32_MAX / long_ray_bytes() ||
+        if (need_pre > INT32_MAX || long_ray_entries(need_ray * 32) > INT32_MAX / long_ray_bytes() ||
             need_it * kIcpPartialStride > INT32_MAX || need_fq > (1 << 29) || need_vfq > (1 << 29))
             return KF_ERR_CAPACITY;
         const int old_pre = cap_pre, old_ray = cap_ray, old_it = cap_it, old_part = cap_part, old_lq = cap_longq,
@@ -733,7 +739,7 @@ struct Engine {
         KF_TRY(grow(d_ray, cap_ray, int(need_ray)));
         KF_TRY(grow(d_itiles, cap_it, int(need_it)));
         KF_TRY(grow(d_partials, cap_part, 2 * int(need_it) * kIcpPartialStride));
-        KF_TRY(grow(d_longq, cap_longq, std::max<int>(1024, int(need_ray) * 32 / kLongRayShare) * long_ray_bytes()));
+        KF_TRY(grow(d_longq, cap_longq, int(long_ray_entries(need_ray * 32)) * long_ray_bytes()));
         KF_TRY(grow(d_fuseq, cap_fuseq, int(need_fq)));
         const int old_vfq = cap_vfuseq;
         if (need_vfq > 0) KF_TRY(grow(d_vfuseq, cap_vfuseq, int(need_vfq)));
@@ -831,7 +837,8 @@ struct Engine {
         KF_TRY(grow(d_ray, cap_ray, std::max<int>(1, int(ray.size()))));
         KF_TRY(grow(d_itiles, cap_it, std::max<int>(1, int(all.size()))));
         KF_TRY(grow(d_partials, cap_part, 2 * std::max<int>(1, int(all.size())) * kIcpPartialStride));
-        KF_TRY(grow(d_longq, cap_longq, std::max<int>(1024, int(ray.size()) * 32 / kLongRayShare) * long_ray_bytes()));
+        if (long_ray_entries((long long)ray.size() * 32) > INT32_MAX / long_ray_bytes()) return KF_ERR_CAPACITY;
+        KF_TRY(grow(d_longq, cap_longq, int(long_ray_entries((long long)ray.size() * 32)) * long_ray_bytes()));
         if (old_pre != cap_pre || old_ray != cap_ray || old_it != cap_it || old_part != cap_part || old_lq != cap_longq ||
             old_fq != cap_fuseq)
             graph_dirty = true;
