@@ -131,13 +131,17 @@ struct __align__(16) LongRay {
 };
 
 __device__ __forceinline__ void ray_matrix(const SessionDev* S, const LevelDev& Lv, float* m, F3& o) {
-    // R_prev * K_l^-1 (the reference forms mat3(pose) * invK per ray)
+    // R_prev * K_l^-1 (the reference forms mat3(pose) * invK per ray), each product and sum
+    // rounded on its own -- the same arithmetic as the host's for the stage raycast, so that a
+    // stage raycast of a session's volume at its pose takes the session's rays bit for bit
     const float* R = S->pose->Rpf;
 #pragma unroll
     for (int col = 0; col < 3; ++col)
 #pragma unroll
         for (int row = 0; row < 3; ++row)
-            m[col * 3 + row] = R[row] * Lv.ik[col * 3 + 0] + R[3 + row] * Lv.ik[col * 3 + 1] + R[6 + row] * Lv.ik[col * 3 + 2];
+            m[col * 3 + row] = __fadd_rn(__fadd_rn(__fmul_rn(R[row], Lv.ik[col * 3 + 0]),
+                                                   __fmul_rn(R[3 + row], Lv.ik[col * 3 + 1])),
+                                         __fmul_rn(R[6 + row], Lv.ik[col * 3 + 2]));
     o = F3{S->pose->tpf[0], S->pose->tpf[1], S->pose->tpf[2]};
 }
 
@@ -718,9 +722,14 @@ cudaError_t stage_raycast(const kf_volume* vol, const float* pose, const float* 
     S.lv[0].cw = w;
     S.lv[0].ch = h;
     RayStage rs;
+    // R * K^-1 with every product and sum rounded on its own (ray_matrix's arithmetic)
     for (int col = 0; col < 3; ++col)
-        for (int row = 0; row < 3; ++row)
-            rs.m[col * 3 + row] = pose[row] * ik[col * 3 + 0] + pose[4 + row] * ik[col * 3 + 1] + pose[8 + row] * ik[col * 3 + 2];
+        for (int row = 0; row < 3; ++row) {
+            const volatile float a = pose[row] * ik[col * 3 + 0], b = pose[4 + row] * ik[col * 3 + 1],
+                                 c = pose[8 + row] * ik[col * 3 + 2];
+            const volatile float ab = a + b;
+            rs.m[col * 3 + row] = ab + c;
+        }
     rs.o[0] = pose[12];
     rs.o[1] = pose[13];
     rs.o[2] = pose[14];

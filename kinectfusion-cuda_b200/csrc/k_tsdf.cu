@@ -190,7 +190,7 @@ __device__ __forceinline__ void fuse_block(const FuseCtx& c, int x0, int j0, int
             const float diff = d[q] - pz[q];
             if (diff >= -c.mu) {   // step 4 (the reference divides with -use_fast_math)
                 fn[q] = fminf(1.0f, __fdividef(diff, c.mu));
-                wn[q] = 1.0f / d[q];
+                wn[q] = __fdividef(1.0f, d[q]);   // its 1 / depth is the fast reciprocal too
                 upd |= 1u << q;
             }
         }

@@ -124,9 +124,10 @@ def test_raycast_maps(kf, run_small):
 
 
 def test_pipeline_raycast_equals_serial_stage(kf, cuda):
-    """The pipeline's march (cell skipping, 40-iteration lane budget, long rays marched by a
-    whole warp) takes the same samples as a plain serial march: compare with the stage
-    raycast (no skipping, no hand-off) on the same volume and pose."""
+    """The pipeline's march (cell skipping with runs of super-bricks, 40-iteration lane budget,
+    long rays marched by a whole warp) takes the same samples as a plain serial march: compare
+    with the stage raycast (no skipping, no hand-off) on the same volume and pose, with the
+    library's K^-1."""
     from kfb200 import synth
     cfg = kf.config_full(volume_n=256)
     imgs, _ = synth.sequence(cfg, 6, seed=41, kind=synth.LOOP)
@@ -135,8 +136,9 @@ def test_pipeline_raycast_equals_serial_stage(kf, cuda):
         s.process_frame(img)
     vol = s.volume()
     pose = s.pose()
-    k = kf.level_intrinsics(cfg, 0)
-    ik = np.linalg.inv(k.astype(np.float64)).astype(np.float32)
+    # the library's own K^-1 (a K^-1 one ulp apart is a different ray: it can move a sample
+    # across 0.99 or 0 near a surface)
+    ik = kf.level_inverse_intrinsics(cfg, 0)
     vt = cuda.zeros((cfg.height, cfg.width, 4), dtype=cuda.float32, device="cuda")
     nt = cuda.zeros_like(vt)
     kf.kernel.raycast(vol, pose, ik, vt, nt, cfg.min_depth, cfg.max_depth, cfg.step_large, cfg.step_small)
@@ -144,11 +146,10 @@ def test_pipeline_raycast_equals_serial_stage(kf, cuda):
     s.process_frame(imgs[5])              # its raycast runs on the same volume and pose
     gv, gn = s.raycast_maps(0)
     written = sv[..., 3] != 0
-    gh, sh = gv[..., 3] == -1, sv[..., 3] == -1
-    assert np.mean((gh == sh)[written]) >= 0.9999
-    both = gh & sh
-    assert both.mean() > 0.1
-    assert np.max(np.abs(gv[both][:, :3] - sv[both][:, :3])) < 1e-4
+    assert (sv[..., 3] == -1).mean() > 0.1
+    # the same rays, the same samples: bit for bit wherever the stage raycast wrote
+    np.testing.assert_array_equal(gv[written], sv[written])
+    np.testing.assert_array_equal(gn[written], sn[written])
     s.close()
 
 
