@@ -34,9 +34,8 @@ for p in (os.path.join(ROOT, "kinectfusion-cuda_b200"), os.path.join(ROOT, "orac
         sys.path.insert(0, p)
 
 
-# kernels one frame launches: preprocess, raycast, raycast_long, icp, fuse_cull, fuse, bricks
-# (the ncu launch list of this workload shows the same seven per frame)
-KERNELS_PER_FRAME = 7
+# kernels one frame launches: preprocess, raycast, raycast_long, icp, fuse_cull, fuse
+KERNELS_PER_FRAME = 6
 
 
 def progress(msg):

@@ -444,7 +444,7 @@ long long long_ray_entries(long long rays) {
 // Launch shapes of a step.  Every value gives the same results bit for bit -- they only change
 // which block or lane does which part of the work -- so they can be tuned on live steps.
 struct Shape {
-    int grid_pre = 0, grid_ray = 0, grid_fuse = 0, grid_brick = 0, grid_icp = 0;
+    int grid_pre = 0, grid_ray = 0, grid_fuse = 0, grid_icp = 0;
     int ray_form = 0;     // 0: by the ray-tile count (many_ray_tiles); 3 or 4: the raycast kernel's
                           // form with that many blocks per SM
     int ray_budget = 0;   // 0: by the ray-tile count (serial_budget); else march iterations a lane
@@ -453,7 +453,7 @@ struct Shape {
     int fuse_split = 0;   // 0: by the queue length (fuse_split); 1, 2, 4: entries whole, halves, quarters
     bool operator==(const Shape& o) const {
         return grid_pre == o.grid_pre && grid_ray == o.grid_ray && grid_fuse == o.grid_fuse &&
-               grid_brick == o.grid_brick && grid_icp == o.grid_icp && ray_form == o.ray_form &&
+               grid_icp == o.grid_icp && ray_form == o.ray_form &&
                ray_budget == o.ray_budget && ray_tw == o.ray_tw && fuse_split == o.fuse_split;
     }
     bool operator!=(const Shape& o) const { return !(*this == o); }
@@ -503,11 +503,7 @@ struct Engine {
     IcpTile* d_itiles = nullptr;
     IcpRange* d_iranges = nullptr;
     long long* d_fprefix = nullptr;
-    long long* d_bprefix = nullptr;
-    long long* d_sprefix = nullptr;
     long long* d_vfprefix = nullptr;   // the same three over the visualization volumes
-    long long* d_vbprefix = nullptr;
-    long long* d_vsprefix = nullptr;
     float* d_partials = nullptr;
     int4* d_icp_sched = nullptr;
     float* d_icp_mats = nullptr;
@@ -576,11 +572,7 @@ struct Engine {
         KF_CK(cudaMalloc(&d_iranges, sizeof(IcpRange) * KF_MAX_LEVELS * capacity));
         KF_CK(cudaMemset(d_iranges, 0, sizeof(IcpRange) * KF_MAX_LEVELS * capacity));
         KF_CK(cudaMalloc(&d_fprefix, sizeof(long long) * (capacity + 1)));
-        KF_CK(cudaMalloc(&d_bprefix, sizeof(long long) * (capacity + 1)));
-        KF_CK(cudaMalloc(&d_sprefix, sizeof(long long) * (capacity + 1)));
         KF_CK(cudaMalloc(&d_vfprefix, sizeof(long long) * (capacity + 1)));
-        KF_CK(cudaMalloc(&d_vbprefix, sizeof(long long) * (capacity + 1)));
-        KF_CK(cudaMalloc(&d_vsprefix, sizeof(long long) * (capacity + 1)));
         KF_CK(cudaMalloc(&d_icp_sched, sizeof(int4) * capacity));
         KF_CK(cudaMemset(d_icp_sched, 0, sizeof(int4) * capacity));
         KF_CK(cudaMalloc(&d_icp_mats, sizeof(float) * 24 * capacity));
@@ -604,7 +596,6 @@ struct Engine {
         shape.grid_pre = sms * 4;
         shape.grid_ray = sms * 6;
         shape.grid_fuse = sms * 4;
-        shape.grid_brick = sms * 4;
         shape.grid_icp = icp_max_grid(sms);
         return KF_OK;
     }
@@ -660,8 +651,8 @@ struct Engine {
         for (cudaEvent_t& e : ev)
             if (e) cudaEventDestroy(e);
         cudaFree(d_sess); cudaFree(d_step); cudaFree(d_out); cudaFree(d_tb); cudaFree(d_pre); cudaFree(d_ray);
-        cudaFree(d_itiles); cudaFree(d_iranges); cudaFree(d_fprefix); cudaFree(d_bprefix); cudaFree(d_sprefix);
-        cudaFree(d_vfprefix); cudaFree(d_vbprefix); cudaFree(d_vsprefix); cudaFree(d_vfuseq);
+        cudaFree(d_itiles); cudaFree(d_iranges); cudaFree(d_fprefix);
+        cudaFree(d_vfprefix); cudaFree(d_vfuseq);
         cudaFree(d_ray_counts);
         cudaFree(d_partials);
         cudaFree(d_icp_sched);
@@ -683,8 +674,7 @@ struct Engine {
     EngineView view() const {
         EngineView v;
         v.sess = d_sess; v.step = d_step; v.out = d_out; v.tb = d_tb; v.pre = d_pre; v.ray = d_ray;
-        v.itiles = d_itiles; v.iranges = d_iranges; v.fuse_prefix = d_fprefix; v.brick_prefix = d_bprefix;
-        v.super_prefix = d_sprefix;
+        v.itiles = d_itiles; v.iranges = d_iranges; v.fuse_prefix = d_fprefix;
         v.partials = d_partials;
         v.partials2 = d_partials ? d_partials + cap_part / 2 : nullptr;   // two equal halves
         v.icp_sched = d_icp_sched;
@@ -695,8 +685,6 @@ struct Engine {
         v.fuseq = d_fuseq;
         v.fuseq_cap = cap_fuseq;
         v.vis_fuse_prefix = d_vfprefix;
-        v.vis_brick_prefix = d_vbprefix;
-        v.vis_super_prefix = d_vsprefix;
         v.vis_fuseq = d_vfuseq;
         v.vis_fuseq_cap = cap_vfuseq;
         v.ray_counts = count_rays ? d_ray_counts : nullptr;
@@ -757,18 +745,13 @@ struct Engine {
         std::vector<RayTile> ray;
         std::vector<IcpTile> it[KF_MAX_LEVELS];
         std::vector<IcpRange> ranges(size_t(KF_MAX_LEVELS) * cap, IcpRange{0, 0});
-        std::vector<long long> fprefix(cap + 1, 0), bprefix(cap + 1, 0), sprefix(cap + 1, 0);
-        std::vector<long long> vfprefix(cap + 1, 0), vbprefix(cap + 1, 0), vsprefix(cap + 1, 0);
+        std::vector<long long> fprefix(cap + 1, 0), vfprefix(cap + 1, 0);
         std::vector<SessionDev> sess(cap);
         int max_levels = 1;
         for (int s = 0; s < cap; ++s) {
             const Slot& sl = slots[s];
             fprefix[s + 1] = fprefix[s];
-            bprefix[s + 1] = bprefix[s];
-            sprefix[s + 1] = sprefix[s];
             vfprefix[s + 1] = vfprefix[s];
-            vbprefix[s + 1] = vbprefix[s];
-            vsprefix[s + 1] = vsprefix[s];
             if (!sl.used) { std::memset(&sess[s], 0, sizeof(SessionDev)); continue; }
             sess[s] = sl.d;
             const kf_config& c = sl.cfg;
@@ -783,14 +766,7 @@ struct Engine {
                         for (int x = 0; x < Lv.cw; x += tw) ray.push_back(RayTile{s, l, x, y});
                 }
                 fprefix[s + 1] += fuse_units(c.volume_n);
-                bprefix[s + 1] += (long long)sl.d.nb * sl.d.nb * sl.d.nb;
-                sprefix[s + 1] += (long long)sl.d.ns * sl.d.ns * sl.d.ns;
-                if (sl.d.vis.n) {
-                    const VisDev& V = sl.d.vis;
-                    vfprefix[s + 1] += fuse_units(V.n);
-                    vbprefix[s + 1] += (long long)V.nb * V.nb * V.nb;
-                    vsprefix[s + 1] += (long long)V.ns * V.ns * V.ns;
-                }
+                if (sl.d.vis.n) vfprefix[s + 1] += fuse_units(sl.d.vis.n);
             }
             for (int l = 0; l < c.levels; ++l) {
                 const LevelDev& Lv = sl.d.lv[l];
@@ -847,11 +823,7 @@ struct Engine {
         if (!all.empty()) KF_CK(cudaMemcpy(d_itiles, all.data(), sizeof(IcpTile) * all.size(), cudaMemcpyHostToDevice));
         KF_CK(cudaMemcpy(d_iranges, ranges.data(), sizeof(IcpRange) * ranges.size(), cudaMemcpyHostToDevice));
         KF_CK(cudaMemcpy(d_fprefix, fprefix.data(), sizeof(long long) * fprefix.size(), cudaMemcpyHostToDevice));
-        KF_CK(cudaMemcpy(d_bprefix, bprefix.data(), sizeof(long long) * bprefix.size(), cudaMemcpyHostToDevice));
-        KF_CK(cudaMemcpy(d_sprefix, sprefix.data(), sizeof(long long) * sprefix.size(), cudaMemcpyHostToDevice));
         KF_CK(cudaMemcpy(d_vfprefix, vfprefix.data(), sizeof(long long) * vfprefix.size(), cudaMemcpyHostToDevice));
-        KF_CK(cudaMemcpy(d_vbprefix, vbprefix.data(), sizeof(long long) * vbprefix.size(), cudaMemcpyHostToDevice));
-        KF_CK(cudaMemcpy(d_vsprefix, vsprefix.data(), sizeof(long long) * vsprefix.size(), cudaMemcpyHostToDevice));
         KF_CK(cudaMemcpy(d_sess, sess.data(), sizeof(SessionDev) * cap, cudaMemcpyHostToDevice));
         tb.S = cap;
         tb.n_pre = int(pre.size());
@@ -868,11 +840,7 @@ struct Engine {
         }
         tb.max_levels = max_levels;
         tb.fuse_total = fprefix[cap];
-        tb.brick_total = bprefix[cap];
-        tb.super_total = sprefix[cap];
         tb.vis_fuse_total = vfprefix[cap];
-        tb.vis_brick_total = vbprefix[cap];
-        tb.vis_super_total = vsprefix[cap];
         KF_CK(cudaMemcpy(d_tb, &tb, sizeof(Tables), cudaMemcpyHostToDevice));
         tables_dirty = false;
         return KF_OK;
@@ -915,14 +883,12 @@ struct Engine {
         {
             NvtxRange r("kf.fusion");
             if (stages[3]) KF_CK(launch_fuse(v, shape.grid_fuse, st));
-            if (stages[3]) KF_CK(launch_bricks(v, shape.grid_brick, st));
         }
         if (has_vis && stages[3]) {
             // the visualization volumes (the reference's second grid), after the tracking fusion
             // and in the same stage time
             NvtxRange r("kf.fusion_vis");
             KF_CK(launch_fuse_vis(v, shape.grid_fuse, st));
-            KF_CK(launch_bricks_vis(v, shape.grid_brick, st));
         }
         if (profile) KF_CK(cudaEventRecordWithFlags(ev[4], st, cudaEventRecordExternal));
         KF_CK(cudaMemcpyAsync(h_out, d_out, sizeof(OutDev) * cap, cudaMemcpyDeviceToHost, st));
@@ -2008,12 +1974,11 @@ std::string mix_key(const Engine& e) {
     return key;
 }
 
-const char* const kShapeFields[] = {"grid_pre", "grid_ray", "grid_fuse", "grid_brick", "grid_icp",
+const char* const kShapeFields[] = {"grid_pre", "grid_ray", "grid_fuse", "grid_icp",
                                     "ray_form", "ray_budget", "ray_tw", "fuse_split"};
-int Shape::* const kShapeMembers[] = {&Shape::grid_pre, &Shape::grid_ray, &Shape::grid_fuse, &Shape::grid_brick,
-                                      &Shape::grid_icp, &Shape::ray_form, &Shape::ray_budget, &Shape::ray_tw,
-                                      &Shape::fuse_split};
-constexpr int kShapeFieldCount = 9;
+int Shape::* const kShapeMembers[] = {&Shape::grid_pre, &Shape::grid_ray, &Shape::grid_fuse, &Shape::grid_icp,
+                                      &Shape::ray_form, &Shape::ray_budget, &Shape::ray_tw, &Shape::fuse_split};
+constexpr int kShapeFieldCount = 8;
 
 std::string shape_json(const Shape& sh) {
     std::string j = "{";
@@ -2093,7 +2058,6 @@ std::vector<Tuner::Param> tuner_params(int sms) {
     p.push_back({"grid_icp", &Shape::grid_icp, {sms / 2, sms}});
     p.push_back({"grid_fuse", &Shape::grid_fuse, {2 * sms, 4 * sms, 6 * sms, 8 * sms}});
     p.push_back({"fuse_split", &Shape::fuse_split, {1, 2, 4}});
-    p.push_back({"grid_brick", &Shape::grid_brick, {2 * sms, 4 * sms, 8 * sms}});
     return p;
 }
 

@@ -16,8 +16,9 @@
 //     there are few, and walk the rows four at a time, each lane four consecutive voxels along
 //     x, so the warp reads and writes the volume as 16-byte vectors in 128-byte rows.
 // Each 8^3 brick keeps a lower bound of its distances (an atomic minimum of every value
-// fusion stores), and a small pass widens it to the 2 x 2 x 2 bricks a trilinear sample can
-// touch; the raycaster skips samples whose bound proves they cannot matter.
+// fusion stores), widened to the 2 x 2 x 2 bricks a trilinear sample can touch and to 32^3
+// super-bricks; fusion lowers the widened bounds itself whenever a brick's bound falls, so no
+// pass recomputes them.  The raycaster skips samples whose bound proves they cannot matter.
 #include "kf_host.h"
 
 namespace kf {
@@ -43,7 +44,36 @@ struct FuseCtx {
     const float* xs;
     const float* zs;
     int* bmin;                   // brick lower bounds (null: none kept)
+    int* bdil;                   // their widenings to the bricks and super-bricks around them
+    int* sdil;
+    int ns;
 };
+
+// A brick's lower bound fell to key k: the widened bounds of every brick and super-brick whose
+// neighbourhood holds the brick fall with it -- bdil of bricks b - {0,1}^3 (a brick's bdil
+// covers {b, b+1}^3) and sdil of super-bricks s with 4 s <= b <= 4 s + 4 per axis.  Bounds only
+// ever fall (atomic minima), so these running minima are exactly the minima over each
+// neighbourhood.  Most calls find the bound already at or below k and stop at one load.
+__device__ __forceinline__ void lower_brick_bound(const FuseCtx& c, int bx, int by, int bz, int k) {
+    const int nb = c.nb;
+    int* pb = c.bmin + (size_t(bz) * nb + by) * nb + bx;
+    if (k >= __ldcg(pb)) return;          // a stale read is never below the bound
+    if (k >= atomicMin(pb, k)) return;    // another warp lowered it as far already
+#pragma unroll
+    for (int d = 0; d < 8; ++d) {
+        const int x = bx - (d & 1), y = by - ((d >> 1) & 1), z = bz - (d >> 2);
+        if (x >= 0 && y >= 0 && z >= 0) atomicMin(c.bdil + (size_t(z) * nb + y) * nb + x, k);
+    }
+    const int ns = c.ns;
+#pragma unroll
+    for (int d = 0; d < 8; ++d) {
+        // super-brick b / 4 per axis, and b / 4 - 1 when b is the last brick of its range too
+        const int x = (bx >> 2) - (d & 1), y = (by >> 2) - ((d >> 1) & 1), z = (bz >> 2) - (d >> 2);
+        const bool ok = ((d & 1) == 0 || ((bx & 3) == 0 && bx > 0)) && (((d >> 1) & 1) == 0 || ((by & 3) == 0 && by > 0)) &&
+                        ((d >> 2) == 0 || ((bz & 3) == 0 && bz > 0));
+        if (ok && x < ns && y < ns && z < ns) atomicMin(c.sdil + (size_t(z) * ns + y) * ns + x, k);
+    }
+}
 
 // running weighted average (project/src/tsdf.cu:56-69, built with -use_fast_math: the
 // division is the approximate one); max_w > 0 clamps the weight
@@ -234,8 +264,7 @@ __device__ __forceinline__ void fuse_block(const FuseCtx& c, int x0, int j0, int
         kmin = min(kmin, __shfl_xor_sync(0xffffffffu, kmin, 1));
         kmin = min(kmin, __shfl_xor_sync(0xffffffffu, kmin, 8));
         kmin = min(kmin, __shfl_xor_sync(0xffffffffu, kmin, 16));
-        if ((lane & 0x19) == 0 && kmin != 0x7fffffff && lane_in)
-            atomicMin(c.bmin + (size_t(k0 >> 3) * c.nb + (j0 >> 3)) * c.nb + (x >> 3), kmin);
+        if ((lane & 0x19) == 0 && kmin != 0x7fffffff && lane_in) lower_brick_bound(c, x >> 3, j0 >> 3, k0 >> 3, kmin);
     }
 }
 
@@ -261,11 +290,11 @@ __device__ void load_ctx(const SessionDev* S, FuseCtx& c) {
     c.w = S->W; c.h = S->H; c.fmt = S->fmt;
     if (kVis) {
         const VisDev& V = S->vis;
-        c.mu = V.mu; c.n = V.n; c.nb = V.nb;
-        c.F = V.tf; c.W = V.tw; c.xs = V.xs; c.zs = V.zs; c.bmin = V.bmin;
+        c.mu = V.mu; c.n = V.n; c.nb = V.nb; c.ns = V.ns;
+        c.F = V.tf; c.W = V.tw; c.xs = V.xs; c.zs = V.zs; c.bmin = V.bmin; c.bdil = V.bdil; c.sdil = V.sdil;
     } else {
-        c.mu = S->mu; c.n = S->n; c.nb = S->nb;
-        c.F = S->tf; c.W = S->tw; c.xs = S->xs; c.zs = S->zs; c.bmin = S->bmin;
+        c.mu = S->mu; c.n = S->n; c.nb = S->nb; c.ns = S->ns;
+        c.F = S->tf; c.W = S->tw; c.xs = S->xs; c.zs = S->zs; c.bmin = S->bmin; c.bdil = S->bdil; c.sdil = S->sdil;
     }
 }
 
@@ -402,6 +431,8 @@ cudaError_t launch_fuse_vis(const EngineView& v, int grid, cudaStream_t st) {
 //       voxel lies in brick b can touch; the raycaster's brick-level skip test reads it.
 // sdil: the same for 32^3 super-bricks: the minimum of bmin over bricks [4s, 4s + 4] per axis.
 //       The raycaster reads the two small arrays (sdil stays in L1) to skip samples.
+// Fusion keeps bdil and sdil equal to these minima as it lowers bmin (lower_brick_bound); the
+// kernels below compute them from scratch after a volume is loaded.
 
 __device__ __forceinline__ int large_key() { return __float_as_int(0.991f); }
 
@@ -427,66 +458,6 @@ __device__ __forceinline__ int superbrick_bound(const int* bmin, int nb, int sx,
 #pragma unroll
     for (int off = 16; off >= 1; off >>= 1) k = min(k, __shfl_xor_sync(0xffffffffu, k, off));
     return k;
-}
-
-__device__ __forceinline__ int slot_of(const long long* prefix, long long g, int S_cap) {
-    int lo = 0, hi = S_cap;
-    while (hi - lo > 1) {
-        const int mid = (lo + hi) >> 1;
-        if (__ldg(prefix + mid) <= g) lo = mid; else hi = mid;
-    }
-    return lo;
-}
-
-// bdil of every brick (the first half of the grid) and sdil of every super-brick (the second
-// half, one warp each) of the stepping sessions
-// the brick bounds of a session's tracking volume, or of its visualization volume (kVis)
-struct BrickView { int* bmin; int* bdil; int* sdil; int nb, ns; };
-template <bool kVis>
-__device__ __forceinline__ BrickView brick_view(const SessionDev* S) {
-    if (kVis) return BrickView{S->vis.bmin, S->vis.bdil, S->vis.sdil, S->vis.nb, S->vis.ns};
-    return BrickView{S->bmin, S->bdil, S->sdil, S->nb, S->ns};
-}
-
-template <bool kVis>
-__global__ void __launch_bounds__(256) bricks_kernel(EngineView v) {
-    const int S_cap = v.tb->S;
-    const int half = gridDim.x / 2;
-    const long long* bprefix = kVis ? v.vis_brick_prefix : v.brick_prefix;
-    const long long* sprefix = kVis ? v.vis_super_prefix : v.super_prefix;
-    if (int(blockIdx.x) < half) {
-        const long long total = kVis ? v.tb->vis_brick_total : v.tb->brick_total;
-        for (long long g = blockIdx.x * (long long)blockDim.x + threadIdx.x; g < total; g += (long long)half * blockDim.x) {
-            const int s = slot_of(bprefix, g, S_cap);
-            if (!v.step[s].active) continue;
-            const BrickView B = brick_view<kVis>(&v.sess[s]);
-            dilate_brick(B.bmin, B.bdil, B.nb, int(g - __ldg(bprefix + s)));
-        }
-    } else {
-        const long long total = kVis ? v.tb->vis_super_total : v.tb->super_total;
-        const int lane = threadIdx.x & 31;
-        const long long warp = ((blockIdx.x - half) * (long long)blockDim.x + threadIdx.x) >> 5;
-        const long long nwarps = ((long long)(gridDim.x - half) * blockDim.x) >> 5;
-        for (long long g = warp; g < total; g += nwarps) {
-            const int s = slot_of(sprefix, g, S_cap);
-            if (!v.step[s].active) continue;
-            const BrickView B = brick_view<kVis>(&v.sess[s]);
-            const long long b = g - __ldg(sprefix + s);
-            const int ns = B.ns;
-            const int k = superbrick_bound(B.bmin, B.nb, int(b % ns), int((b / ns) % ns), int(b / ((long long)ns * ns)), lane);
-            if (lane == 0) B.sdil[b] = k;
-        }
-    }
-}
-
-cudaError_t launch_bricks(const EngineView& v, int grid, cudaStream_t st) {
-    bricks_kernel<false><<<grid, 256, 0, st>>>(v);
-    return cudaGetLastError();
-}
-
-cudaError_t launch_bricks_vis(const EngineView& v, int grid, cudaStream_t st) {
-    bricks_kernel<true><<<grid, 256, 0, st>>>(v);
-    return cudaGetLastError();
 }
 
 __global__ void fill_key_kernel(int* a, long long count, int key) {

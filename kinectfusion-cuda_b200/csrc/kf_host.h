@@ -22,11 +22,7 @@ struct Tables {
     int fuse_split;          // 0: fusion takes queue entries by the rule of fuse_split(); 1, 2, 4:
                              // whole, in halves or in quarters
     long long fuse_total;    // fusion segments over all slots
-    long long brick_total;   // bricks over all slots
-    long long super_total;   // super-bricks over all slots
-    long long vis_fuse_total;  // the same three over the slots' visualization volumes
-    long long vis_brick_total;
-    long long vis_super_total;
+    long long vis_fuse_total;  // the same over the slots' visualization volumes
 };
 
 struct LongRay;   // march state of a ray handed from a lane to a warp (k_raycast.cu)
@@ -44,11 +40,7 @@ struct EngineView {
     const IcpTile* itiles;
     const IcpRange* iranges;     // [level * S + s]
     const long long* fuse_prefix;// S + 1 entries, in segments
-    const long long* brick_prefix;// S + 1 entries, in bricks
-    const long long* super_prefix;// S + 1 entries, in super-bricks
-    const long long* vis_fuse_prefix;   // the same three for the visualization volumes
-    const long long* vis_brick_prefix;
-    const long long* vis_super_prefix;
+    const long long* vis_fuse_prefix;   // the same for the visualization volumes
     float* partials;             // ICP tile partials, kIcpPartialStride floats per tile
     float* partials2;            // a second set: a single session's odd passes (see icp_kernel)
     int4* icp_sched;             // per slot: {level of the next ICP pass or -1, first tile, tiles, 0}
@@ -92,10 +84,6 @@ cudaError_t launch_icp(const EngineView& v, int grid, cudaStream_t st, bool sing
 cudaError_t launch_fuse(const EngineView& v, int grid, cudaStream_t st);
 // the same for the sessions' visualization volumes (cull, fuse and bounds)
 cudaError_t launch_fuse_vis(const EngineView& v, int grid, cudaStream_t st);
-// widen the brick lower bounds to the 2 x 2 x 2 bricks the raycaster reads, and bound the
-// super-bricks (one launch)
-cudaError_t launch_bricks(const EngineView& v, int grid, cudaStream_t st);
-cudaError_t launch_bricks_vis(const EngineView& v, int grid, cudaStream_t st);
 // bounds = key(2), the initial distance; rebuild recomputes them exactly from a loaded volume
 cudaError_t launch_init_bricks(int* bmin, int* bdil, int* sdil, int n, cudaStream_t st);
 cudaError_t launch_rebuild_bricks(const void* f, int fmt, int n, int* bmin, int* bdil, int* sdil, cudaStream_t st);
