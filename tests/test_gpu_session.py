@@ -123,13 +123,15 @@ def test_raycast_maps(kf, run_small):
             assert p["trace_flips"] <= 1e-3 * p["rays"], (i, level, p)
 
 
-def test_pipeline_raycast_equals_serial_stage(kf, cuda):
+@pytest.mark.parametrize("volume_n,fmt", [(256, 0), (200, 0), (256, 1)], ids=["n256", "n200", "n256f16"])
+def test_pipeline_raycast_equals_serial_stage(kf, cuda, volume_n, fmt):
     """The pipeline's march (cell skipping with runs of super-bricks, 40-iteration lane budget,
     long rays marched by a whole warp) takes the same samples as a plain serial march: compare
     with the stage raycast (no skipping, no hand-off) on the same volume and pose, with the
-    library's K^-1."""
+    library's K^-1.  n = 200 is a multiple of 8 but not of 32: its last super-bricks are
+    partial, and their far faces are the volume's edges (which bound no skip)."""
     from kfb200 import synth
-    cfg = kf.config_full(volume_n=256)
+    cfg = kf.config_full(volume_n=volume_n, tsdf_format=fmt)
     imgs, _ = synth.sequence(cfg, 6, seed=41, kind=synth.LOOP)
     s = kf.KinectFusion(cfg)
     for img in imgs[:5]:
@@ -146,7 +148,7 @@ def test_pipeline_raycast_equals_serial_stage(kf, cuda):
     s.process_frame(imgs[5])              # its raycast runs on the same volume and pose
     gv, gn = s.raycast_maps(0)
     written = sv[..., 3] != 0
-    assert (sv[..., 3] == -1).mean() > 0.1
+    assert (sv[..., 3] == -1).mean() > 0.05   # enough hits to compare (8 % at n = 200)
     # the same rays, the same samples: bit for bit wherever the stage raycast wrote
     np.testing.assert_array_equal(gv[written], sv[written])
     np.testing.assert_array_equal(gn[written], sn[written])
