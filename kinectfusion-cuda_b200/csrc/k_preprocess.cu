@@ -42,6 +42,29 @@ __device__ __forceinline__ float bilateral_core(Reader rd, int R, float inv_ss, 
     return acc / norm;
 }
 
+// The same for a radius known at compile time (the configurations' 2 and the reference's 3):
+// the taps unroll with constant offsets into the tile; the arithmetic is the loop's above,
+// operation for operation.
+template <int kR, class Reader>
+__device__ __forceinline__ float bilateral_fixed(Reader rd, float inv_ss, float inv_sr) {
+    const float center = rd(0, 0);
+    float norm = 0.f, acc = 0.f;
+#pragma unroll
+    for (int x = -kR; x <= kR; ++x) {
+#pragma unroll
+        for (int y = -kR; y <= kR; ++y) {
+            const float cur = rd(x, y);
+            const float s = float(x * x + y * y);
+            float r = center - cur;
+            r *= r;
+            const float e = __expf(-s * inv_ss - r * inv_sr);
+            norm += e;
+            acc += e * cur;
+        }
+    }
+    return acc / norm;
+}
+
 // downSampleKernel body (project/src/measurement.cu:73-101)
 __device__ __forceinline__ float downsample_core(float f1, float f2, float f3, float f4, float thr) {
     float acc = f1;
@@ -113,8 +136,15 @@ __global__ void __launch_bounds__(256) preprocess_kernel(EngineView v) {
             float d = 0.f;
             if (gx < L0.cw && gy < L0.ch) {
                 const float* c = reg + (ly + R) * pitch + (lx + R);
-                d = bilateral_core([c, pitch](int x, int y) { return c[y * pitch + x]; }, R, S->bil_inv_ss,
-                                   S->bil_inv_sr);
+                if (R == 2)
+                    d = bilateral_fixed<2>([c](int x, int y) { return c[y * (kPreTileSize + 4) + x]; },
+                                           S->bil_inv_ss, S->bil_inv_sr);
+                else if (R == 3)
+                    d = bilateral_fixed<3>([c](int x, int y) { return c[y * (kPreTileSize + 6) + x]; },
+                                           S->bil_inv_ss, S->bil_inv_sr);
+                else
+                    d = bilateral_core([c, pitch](int x, int y) { return c[y * pitch + x]; }, R, S->bil_inv_ss,
+                                       S->bil_inv_sr);
                 S->depth[0][size_t(gy) * W + gx] = d;
                 S->vmap[0][size_t(gy) * W + gx] = vertex_core(d, gx, gy, L0.ik);
             }
