@@ -87,16 +87,14 @@ __device__ __forceinline__ float4 vertex_core(float d, int i, int j, const float
 
 // ---- fused, batched kernel ----
 
-__global__ void __launch_bounds__(256) preprocess_kernel(EngineView v) {
-    extern __shared__ float smem[];
-    __shared__ unsigned int qmax[4];   // largest valid depth of each 16x16 quadrant (float bits)
+// One tile.  kR: the bilateral radius when it is known at compile time (2 or 3: the halo's
+// pitch and the filter's offsets are constants), 0 for any other radius.
+template <int kR>
+__device__ __forceinline__ void preprocess_tile(const EngineView& v, const PreTile T, float* smem, unsigned int* qmax) {
     const int tid = threadIdx.x;
-    const int ntiles = v.tb->n_pre;
-    for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
-        const PreTile T = v.pre[t];
-        if (!v.step[T.s].active) continue;   // block-uniform
+    {
         const SessionDev* S = &v.sess[T.s];
-        const int W = S->W, H = S->H, R = S->bil_r, L = S->L;
+        const int W = S->W, H = S->H, R = kR ? kR : S->bil_r, L = S->L;
         const int pitch = kPreTileSize + 2 * R;
         float* reg = smem;                           // converted metres, tile + halo
         float* l0 = smem + pitch * pitch;            // filtered level 0, 32 x 32
@@ -136,12 +134,9 @@ __global__ void __launch_bounds__(256) preprocess_kernel(EngineView v) {
             float d = 0.f;
             if (gx < L0.cw && gy < L0.ch) {
                 const float* c = reg + (ly + R) * pitch + (lx + R);
-                if (R == 2)
-                    d = bilateral_fixed<2>([c](int x, int y) { return c[y * (kPreTileSize + 4) + x]; },
-                                           S->bil_inv_ss, S->bil_inv_sr);
-                else if (R == 3)
-                    d = bilateral_fixed<3>([c](int x, int y) { return c[y * (kPreTileSize + 6) + x]; },
-                                           S->bil_inv_ss, S->bil_inv_sr);
+                if constexpr (kR > 0)
+                    d = bilateral_fixed<kR>([c](int x, int y) { return c[y * (kPreTileSize + 2 * kR) + x]; },
+                                            S->bil_inv_ss, S->bil_inv_sr);
                 else
                     d = bilateral_core([c, pitch](int x, int y) { return c[y * pitch + x]; }, R, S->bil_inv_ss,
                                        S->bil_inv_sr);
@@ -183,6 +178,23 @@ __global__ void __launch_bounds__(256) preprocess_kernel(EngineView v) {
             }
         }
         __syncthreads();
+    }
+}
+
+__global__ void __launch_bounds__(256) preprocess_kernel(EngineView v) {
+    extern __shared__ float smem[];
+    __shared__ unsigned int qmax[4];   // largest valid depth of each 16x16 quadrant (float bits)
+    const int ntiles = v.tb->n_pre;
+    for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
+        const PreTile T = v.pre[t];
+        if (!v.step[T.s].active) continue;   // block-uniform
+        const int R = v.sess[T.s].bil_r;
+        if (R == 2)
+            preprocess_tile<2>(v, T, smem, qmax);
+        else if (R == 3)
+            preprocess_tile<3>(v, T, smem, qmax);
+        else
+            preprocess_tile<0>(v, T, smem, qmax);
     }
 }
 
