@@ -154,7 +154,9 @@ __device__ __forceinline__ void make_geo(const SessionDev* S, const float* m, F3
     g.off = 0.5f * float(S->n) - 0.5f;
     g.tox = o.x * g.sc + g.off; g.toy = o.y * g.sc + g.off; g.toz = o.z * g.sc + g.off;
     g.tdx = g.dir.x * g.sc; g.tdy = g.dir.y * g.sc; g.tdz = g.dir.z * g.sc;
-    g.itdx = 1.0f / g.tdx; g.itdy = 1.0f / g.tdy; g.itdz = 1.0f / g.tdz;
+    // only the skips' cell exits use these, 0.01 texel inside the faces: the fast reciprocal's
+    // 2 ulp cannot move a skip across a sample
+    g.itdx = __fdividef(1.0f, g.tdx); g.itdy = __fdividef(1.0f, g.tdy); g.itdz = __fdividef(1.0f, g.tdz);
 }
 
 // texel coordinate of the sample at t, (o + dir t) * sc + off, with its roundings spelled out
