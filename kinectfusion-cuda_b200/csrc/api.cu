@@ -2055,7 +2055,7 @@ std::vector<Tuner::Param> tuner_params(int sms) {
     p.push_back({"ray_budget", &Shape::ray_budget, {24, 32, 40, 48, 64, 96}});
     p.push_back({"ray_tw", &Shape::ray_tw, {8, 16, 4}});
     p.push_back({"grid_pre", &Shape::grid_pre, {1 * sms, 2 * sms, 4 * sms, 8 * sms}});
-    p.push_back({"grid_icp", &Shape::grid_icp, {sms / 2, sms}});
+    p.push_back({"grid_icp", &Shape::grid_icp, {sms, 2 * sms}});
     p.push_back({"grid_fuse", &Shape::grid_fuse, {2 * sms, 4 * sms, 6 * sms, 8 * sms}});
     p.push_back({"fuse_split", &Shape::fuse_split, {1, 2, 4}});
     return p;

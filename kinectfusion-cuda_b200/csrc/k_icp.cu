@@ -634,8 +634,11 @@ __device__ void store_local_state(PoseDev* P, const IcpLocal& L, bool first) {
     P->status = L.status;
 }
 
+// A batch's launch holds two blocks per SM (128 registers; the solve, run once per session
+// and pass, spills a little): twice the warps to hide phase A's gathers.  A single session's
+// keeps one block per SM, the solve in registers: every block runs it on every pass.
 template <bool local>
-__global__ void __launch_bounds__(kIcpThreads, 1) icp_kernel(EngineView v) {
+__global__ void __launch_bounds__(kIcpThreads, local ? 1 : 2) icp_kernel(EngineView v) {
     __shared__ float red[8 * 32 * 2];
     __shared__ double dsm[(kIcpThreads / 14 + 1) * 28];
     __shared__ float mats[24];
@@ -731,7 +734,7 @@ __global__ void __launch_bounds__(kIcpThreads, 1) icp_kernel(EngineView v) {
     }
 }
 
-int icp_max_grid(int num_sms) { return num_sms; }
+int icp_max_grid(int num_sms) { return 2 * num_sms; }
 
 // Bounded-wait self test: a two-block cooperative launch in which block 1 never arrives at
 // the barrier block 0 waits on.  The wait gives up after timeout_ns, sets the abort flag and
@@ -752,6 +755,10 @@ cudaError_t launch_barrier_selftest(GridSync* g, unsigned long long timeout_ns, 
 cudaError_t launch_icp(const EngineView& v, int grid, cudaStream_t st, bool single) {
     void* args[] = {const_cast<EngineView*>(&v)};
     const void* k = single ? (const void*)icp_kernel<true> : (const void*)icp_kernel<false>;
+    int dev = 0, sms = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (single) grid = std::min(grid, sms);   // one co-resident block per SM
     return cudaLaunchCooperativeKernel(k, dim3(grid), dim3(kIcpThreads), args, 0, st);
 }
 
