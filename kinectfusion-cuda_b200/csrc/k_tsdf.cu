@@ -328,7 +328,7 @@ __device__ __forceinline__ int unit_session(const long long* prefix, long long g
 // one thread per block of every stepping session: append the blocks that can update to the
 // queue (counters[4] = entries; [8] for the visualization volumes), one atomic per warp
 template <bool kVis>
-__global__ void __launch_bounds__(256) fuse_cull_kernel(EngineView v) {
+__global__ void __launch_bounds__(256, 4) fuse_cull_kernel(EngineView v) {
     using Lists = FuseLists<kVis>;
     const long long total = Lists::total(v);
     const long long* prefix = Lists::prefix(v);
