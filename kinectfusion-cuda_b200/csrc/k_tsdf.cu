@@ -78,8 +78,8 @@ __device__ __forceinline__ void lower_brick_bound(const FuseCtx& c, int bx, int 
 // running weighted average (project/src/tsdf.cu:56-69, built with -use_fast_math: the
 // division is the approximate one); max_w > 0 clamps the weight
 __device__ __forceinline__ void fuse_update(float& F, float& Wt, float fn, float wn, float max_w) {
-    F = __fdividef(F * Wt + fn * wn, Wt + wn);
-    float w1 = Wt + wn;
+    F = __fdividef(__fmaf_rn(F, Wt, __fmul_rn(fn, wn)), __fadd_rn(Wt, wn));
+    float w1 = __fadd_rn(Wt, wn);
     if (max_w > 0.0f) w1 = fminf(w1, max_w);
     Wt = w1;
 }
@@ -150,14 +150,6 @@ __device__ __forceinline__ void st4(__half* p, uint2 v) { *reinterpret_cast<uint
 __device__ __forceinline__ void st4(uint16_t* p, uint2 v) { *reinterpret_cast<uint2*>(p) = v; }
 // component q of a 4-vector (q a compile-time constant after unrolling)
 __device__ __forceinline__ float& comp(float4& v, int q) { return q == 0 ? v.x : q == 1 ? v.y : q == 2 ? v.z : v.w; }
-__device__ __forceinline__ uint16_t get16(uint2 v, int q) {
-    const unsigned int w = q < 2 ? v.x : v.y;
-    return uint16_t((q & 1) ? (w >> 16) : (w & 0xffffu));
-}
-__device__ __forceinline__ void set16(uint2& v, int q, uint16_t b) {
-    unsigned int& w = q < 2 ? v.x : v.y;
-    w = (q & 1) ? ((w & 0xffffu) | (unsigned(b) << 16)) : ((w & 0xffff0000u) | b);
-}
 
 // fuseKernel (project/src/tsdf.cu:28-74) for rows [r_begin, r_end) of one block (row r is
 // y = j0 + r % 8, z = k0 + r / 8; n is a multiple of 8, so every block has 64 rows).  A warp
@@ -243,17 +235,36 @@ __device__ __forceinline__ void fuse_block(const FuseCtx& c, int x0, int j0, int
             st4(Wa + idx, wv);
         } else {
             uint2 fv = ld4(F + idx), wv = ld4(Wa + idx);
+            // All four voxels are decoded and encoded again, the unchanged ones exactly: an fp16
+            // value survives float and back, and a weight u / 1024 survives the scaling by a
+            // power of two.  The weight steps u < 2^16 become floats as the float 2^23 + u
+            // (bits 0x4B000000 | u) less 2^23, and return as the low bits of x + 2^23, whose
+            // round-to-nearest-even addition is rintf(x) for 0 <= x < 2^22: exact, without
+            // conversion instructions.
+            static_assert(KF_WEIGHT_SCALE == 1024.0f, "weights are steps of 1 / 1024");
+            const float2 f01 = __half22float2(*reinterpret_cast<const __half2*>(&fv.x));
+            const float2 f23 = __half22float2(*reinterpret_cast<const __half2*>(&fv.y));
+            float f[4] = {f01.x, f01.y, f23.x, f23.y}, w[4];
 #pragma unroll
             for (int q = 0; q < 4; ++q) {
-                if (!(upd & (1u << q))) continue;
-                float f0 = __half2float(__ushort_as_half(get16(fv, q)));
-                float w0 = float(get16(wv, q)) * (1.0f / KF_WEIGHT_SCALE);
-                fuse_update(f0, w0, fn[q], wn[q], c.max_w);
-                const __half hf = __float2half_rn(f0);
-                set16(fv, q, __half_as_ushort(hf));
-                set16(wv, q, uint16_t(fminf(rintf(w0 * KF_WEIGHT_SCALE), 65535.0f)));
-                kmin = min(kmin, fkey(__half2float(hf)));
+                const unsigned int bits = __byte_perm(q < 2 ? wv.x : wv.y, 0x4B000000u, (q & 1) ? 0x7632 : 0x7610);
+                w[q] = __fmul_rn(__fsub_rn(__uint_as_float(bits), 8388608.0f), 1.0f / KF_WEIGHT_SCALE);
+                if (upd & (1u << q)) fuse_update(f[q], w[q], fn[q], wn[q], c.max_w);
             }
+            const __half2 h01 = __floats2half2_rn(f[0], f[1]), h23 = __floats2half2_rn(f[2], f[3]);
+            fv.x = *reinterpret_cast<const unsigned int*>(&h01);
+            fv.y = *reinterpret_cast<const unsigned int*>(&h23);
+            unsigned int wb[4];
+#pragma unroll
+            for (int q = 0; q < 4; ++q)
+                wb[q] = __float_as_uint(__fadd_rn(fminf(__fmul_rn(w[q], KF_WEIGHT_SCALE), 65535.0f), 8388608.0f));
+            wv.x = __byte_perm(wb[0], wb[1], 0x5410);
+            wv.y = __byte_perm(wb[2], wb[3], 0x5410);
+            const float2 r01 = __half22float2(h01), r23 = __half22float2(h23);
+            const float r[4] = {r01.x, r01.y, r23.x, r23.y};
+#pragma unroll
+            for (int q = 0; q < 4; ++q)
+                if (upd & (1u << q)) kmin = min(kmin, fkey(r[q]));
             st4(F + idx, fv);
             st4(Wa + idx, wv);
         }
