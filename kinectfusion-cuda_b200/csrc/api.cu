@@ -507,9 +507,12 @@ struct Engine {
     float* d_partials = nullptr;
     int4* d_icp_sched = nullptr;
     float* d_icp_mats = nullptr;
+    // one block [OutDev x cap | GridSync | counters]: a step clears the wait record and the
+    // counters with one memset, and a caller that reads the results copies them with one copy
     GridSync* d_sync = nullptr;
     unsigned int* d_ctr = nullptr;
     static constexpr int kCounters = 12;
+    size_t out_bytes() const { return sizeof(OutDev) * cap + sizeof(GridSync); }
     int cap_pre = 0, cap_ray = 0, cap_it = 0, cap_part = 0;
     // long-ray queue of the raycaster (bytes; entries = bytes / long_ray_bytes())
     char* d_longq = nullptr;
@@ -566,8 +569,11 @@ struct Engine {
         KF_CK(cudaMemset(d_sess, 0, sizeof(SessionDev) * capacity));
         KF_CK(cudaMalloc(&d_step, sizeof(StepDev) * capacity));
         KF_CK(cudaMemset(d_step, 0, sizeof(StepDev) * capacity));
-        KF_CK(cudaMalloc(&d_out, sizeof(OutDev) * capacity));
-        KF_CK(cudaMemset(d_out, 0, sizeof(OutDev) * capacity));
+        static_assert(sizeof(OutDev) % 16 == 0 && sizeof(GridSync) % 16 == 0, "result block layout");
+        KF_CK(cudaMalloc(&d_out, out_bytes() + sizeof(unsigned int) * kCounters));
+        KF_CK(cudaMemset(d_out, 0, out_bytes() + sizeof(unsigned int) * kCounters));
+        d_sync = reinterpret_cast<GridSync*>(d_out + capacity);
+        d_ctr = reinterpret_cast<unsigned int*>(d_sync + 1);
         KF_CK(cudaMalloc(&d_tb, sizeof(Tables)));
         KF_CK(cudaMalloc(&d_iranges, sizeof(IcpRange) * KF_MAX_LEVELS * capacity));
         KF_CK(cudaMemset(d_iranges, 0, sizeof(IcpRange) * KF_MAX_LEVELS * capacity));
@@ -577,14 +583,11 @@ struct Engine {
         KF_CK(cudaMemset(d_icp_sched, 0, sizeof(int4) * capacity));
         KF_CK(cudaMalloc(&d_icp_mats, sizeof(float) * 24 * capacity));
         KF_CK(cudaMemset(d_icp_mats, 0, sizeof(float) * 24 * capacity));
-        KF_CK(cudaMalloc(&d_sync, sizeof(GridSync)));
-        KF_CK(cudaMalloc(&d_ctr, sizeof(unsigned int) * kCounters));
         KF_CK(cudaMallocHost(&h_step, sizeof(StepDev) * capacity));
-        KF_CK(cudaMallocHost(&h_out, sizeof(OutDev) * capacity));
-        KF_CK(cudaMallocHost(&h_sync, sizeof(GridSync)));
+        KF_CK(cudaMallocHost(&h_out, out_bytes()));
+        h_sync = reinterpret_cast<GridSync*>(h_out + capacity);
         std::memset(h_step, 0, sizeof(StepDev) * capacity);
-        std::memset(h_out, 0, sizeof(OutDev) * capacity);
-        std::memset(h_sync, 0, sizeof(GridSync));
+        std::memset(h_out, 0, out_bytes());
         KF_CK(cudaStreamCreateWithFlags(&cap_stream, cudaStreamNonBlocking));
         KF_CK(cudaStreamCreateWithFlags(&aux_stream, cudaStreamNonBlocking));
         KF_CK(cudaEventCreateWithFlags(&ev_fork, cudaEventDisableTiming));
@@ -600,10 +603,12 @@ struct Engine {
         return KF_OK;
     }
 
-    // the stream a step's frame copies go on: h2d_stream for host frames, after the work already
-    // queued on st (earlier steps read the same input buffers); st itself for device frames
-    kf_status begin_inputs(bool host, cudaStream_t st, cudaStream_t* cs) {
-        if (!host) { *cs = st; return KF_OK; }
+    // the stream a step's frame copies go on: h2d_stream, after the work already queued on st
+    // (earlier steps read the same input buffers; a device frame may come from work on st).  The
+    // step's raycast needs only earlier frames and starts at once; its preprocess branch waits
+    // for ev_input, and the step ends after that branch, so later work on st (a caller
+    // refilling its frame buffer) stays ordered after the copy.
+    kf_status begin_inputs(cudaStream_t st, cudaStream_t* cs) {
         KF_CK(cudaEventRecord(ev_prev, st));
         KF_CK(cudaStreamWaitEvent(h2d_stream, ev_prev, 0));
         *cs = h2d_stream;
@@ -659,9 +664,7 @@ struct Engine {
         cudaFree(d_icp_mats);
         cudaFree(d_longq);
         cudaFree(d_fuseq);
-        cudaFree(d_sync);
-        cudaFree(d_ctr);
-        cudaFreeHost(h_step); cudaFreeHost(h_out); cudaFreeHost(h_sync);
+        cudaFreeHost(h_step); cudaFreeHost(h_out);
         if (cap_stream) cudaStreamDestroy(cap_stream);
         if (aux_stream) cudaStreamDestroy(aux_stream);
         if (ev_fork) cudaEventDestroy(ev_fork);
@@ -849,8 +852,7 @@ struct Engine {
     // the per-step sequence
     kf_status record(cudaStream_t st) {
         const EngineView v = view();
-        KF_CK(cudaMemsetAsync(d_ctr, 0, sizeof(unsigned int) * kCounters, st));
-        KF_CK(cudaMemsetAsync(d_sync, 0, sizeof(GridSync), st));
+        KF_CK(cudaMemsetAsync(d_sync, 0, sizeof(GridSync) + sizeof(unsigned int) * kCounters, st));
         if (count_rays) KF_CK(cudaMemsetAsync(d_ray_counts, 0, sizeof(unsigned long long) * ray_count_slots(), st));
         if (profile) KF_CK(cudaEventRecordWithFlags(ev[0], st, cudaEventRecordExternal));
         const bool fork = stages[0] && stages[1];
@@ -891,8 +893,13 @@ struct Engine {
             KF_CK(launch_fuse_vis(v, shape.grid_fuse, st));
         }
         if (profile) KF_CK(cudaEventRecordWithFlags(ev[4], st, cudaEventRecordExternal));
-        KF_CK(cudaMemcpyAsync(h_out, d_out, sizeof(OutDev) * cap, cudaMemcpyDeviceToHost, st));
-        KF_CK(cudaMemcpyAsync(h_sync, d_sync, sizeof(GridSync), cudaMemcpyDeviceToHost, st));
+        return KF_OK;
+    }
+
+    // the step's results (every slot's OutDev and the wait record) into pinned memory, for
+    // collect() once the stream is idle; steps whose results stay on the device skip it
+    kf_status fetch(cudaStream_t st) {
+        KF_CK(cudaMemcpyAsync(h_out, d_out, out_bytes(), cudaMemcpyDeviceToHost, st));
         return KF_OK;
     }
 
@@ -1054,21 +1061,20 @@ void level_intrinsics(const kf_config& c, int level, float k[9], float ik[9]) {
 // kf_process_frame_wait: each has its own pinned copy of the step's result and an event
 struct FrameRing {
     static constexpr int kDepth = KF_MAX_FRAMES_IN_FLIGHT;
-    OutDev* out = nullptr;                 // kDepth pinned result blocks
-    GridSync* sync = nullptr;              // kDepth pinned copies of the step's wait record
+    // a frame's result block and the step's wait record, laid out as on the device when the
+    // session is its engine's last slot (one copy)
+    struct Entry { OutDev out; GridSync sync; };
+    Entry* res = nullptr;                  // kDepth pinned entries
     cudaEvent_t done[kDepth] = {};
     int head = 0, count = 0;               // oldest in-flight entry, entries in flight
     kf_status init() {
-        KF_CK(cudaMallocHost(&out, sizeof(OutDev) * kDepth));
-        KF_CK(cudaMallocHost(&sync, sizeof(GridSync) * kDepth));
+        KF_CK(cudaMallocHost(&res, sizeof(Entry) * kDepth));
         for (cudaEvent_t& e : done) KF_CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
         return KF_OK;
     }
     void destroy() {
-        if (out) cudaFreeHost(out);
-        if (sync) cudaFreeHost(sync);
-        out = nullptr;
-        sync = nullptr;
+        if (res) cudaFreeHost(res);
+        res = nullptr;
         for (cudaEvent_t& e : done)
             if (e) cudaEventDestroy(e);
     }
@@ -1202,7 +1208,7 @@ static kf_status session_enqueue(kf_session* s, const uint16_t* depth, int is_de
     KF_TRY(s->eng->set_step(want, st));
     Engine& e = *s->eng;
     cudaStream_t cs = st;
-    KF_TRY(e.begin_inputs(!is_dev, st, &cs));
+    KF_TRY(e.begin_inputs(st, &cs));
     KF_CK(cudaMemcpyAsync(const_cast<uint16_t*>(sl.d.raw), depth, bytes,
                           is_dev ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, cs));
     KF_TRY(e.end_inputs(cs));
@@ -1215,6 +1221,7 @@ kf_status kf_process_frame(kf_session* s, const uint16_t* depth, int is_device_p
     if (s->ring && s->ring->count) return KF_ERR_STATE;   // collect submitted frames first
     cudaStream_t st = as_stream(stream);
     KF_TRY(session_enqueue(s, depth, is_device_ptr, st));
+    KF_TRY(s->eng->fetch(st));
     KF_CK(cudaStreamSynchronize(st));
     std::vector<StepDev> want(s->eng->cap, StepDev{0, 0});
     want[s->slot] = StepDev{1, 0};
@@ -1241,8 +1248,13 @@ kf_status kf_process_frame_submit(kf_session* s, const uint16_t* depth, int is_d
     KF_TRY(session_enqueue(s, depth, is_device_ptr, st));
     // this frame's result, read back before a later frame's step overwrites it on the device
     const int k = (r.head + r.count) % FrameRing::kDepth;
-    KF_CK(cudaMemcpyAsync(&r.out[k], s->eng->d_out + s->slot, sizeof(OutDev), cudaMemcpyDeviceToHost, st));
-    KF_CK(cudaMemcpyAsync(&r.sync[k], s->eng->d_sync, sizeof(GridSync), cudaMemcpyDeviceToHost, st));
+    static_assert(sizeof(FrameRing::Entry) == sizeof(OutDev) + sizeof(GridSync), "ring entry layout");
+    if (s->slot == s->eng->cap - 1) {
+        KF_CK(cudaMemcpyAsync(&r.res[k], s->eng->d_out + s->slot, sizeof(FrameRing::Entry), cudaMemcpyDeviceToHost, st));
+    } else {
+        KF_CK(cudaMemcpyAsync(&r.res[k].out, s->eng->d_out + s->slot, sizeof(OutDev), cudaMemcpyDeviceToHost, st));
+        KF_CK(cudaMemcpyAsync(&r.res[k].sync, s->eng->d_sync, sizeof(GridSync), cudaMemcpyDeviceToHost, st));
+    }
     KF_CK(cudaEventRecord(r.done[k], st));
     r.count += 1;
     s->sl().frames = frame_no + 1;
@@ -1256,11 +1268,11 @@ kf_status kf_process_frame_wait(kf_session* s, float pose_out[16], kf_frame_stat
     FrameRing& r = *s->ring;
     const int k = r.head;
     KF_CK(cudaEventSynchronize(r.done[k]));
-    const OutDev& o = r.out[k];
+    const OutDev& o = r.res[k].out;
     Slot& sl = s->sl();
     kf_frame_stats fs{};
     fs.frame = o.frame - 1;
-    fs.status = r.sync[k].abort != 0 ? KF_ERR_TIMEOUT : o.status;
+    fs.status = r.res[k].sync.abort != 0 ? KF_ERR_TIMEOUT : o.status;
     for (int l = 0; l < KF_MAX_LEVELS; ++l) fs.icp_iters[l] = o.iters[l];
     r.head = (r.head + 1) % FrameRing::kDepth;
     r.count -= 1;
@@ -1843,8 +1855,7 @@ kf_status kf_compute_pose(const float* const* vertex, const float* const* target
     e = cudaMemcpy(eng.d_step, &step, sizeof(step), cudaMemcpyHostToDevice);
     if (e == cudaSuccess) e = cudaMemsetAsync(eng.d_sync, 0, sizeof(GridSync), s);
     if (e == cudaSuccess) e = launch_icp(eng.view(), eng.shape.grid_icp, s, eng.cap == 1);
-    if (e == cudaSuccess) e = cudaMemcpyAsync(eng.h_out, eng.d_out, sizeof(OutDev), cudaMemcpyDeviceToHost, s);
-    if (e == cudaSuccess) e = cudaMemcpyAsync(eng.h_sync, eng.d_sync, sizeof(GridSync), cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(eng.h_out, eng.d_out, eng.out_bytes(), cudaMemcpyDeviceToHost, s);
     if (e == cudaSuccess) e = cudaStreamSynchronize(s);
     if (e != cudaSuccess) return fail(e);
     std::memcpy(pose_out, eng.h_out[0].pose, sizeof(float) * 16);
@@ -1909,7 +1920,7 @@ kf_status kf_batch_step(kf_batch* b, const uint16_t* const* depth, int is_device
     KF_TRY(b->eng.set_step(want, st));
     KF_TRY(tuner_before_step(b->eng));
     cudaStream_t cs = st;
-    KF_TRY(b->eng.begin_inputs(!is_device_ptr, st, &cs));
+    KF_TRY(b->eng.begin_inputs(st, &cs));
     for (int i = 0; i < b->n; ++i) {
         if (!depth[i]) continue;
         Slot& sl = b->eng.slots[i];
@@ -1918,6 +1929,7 @@ kf_status kf_batch_step(kf_batch* b, const uint16_t* const* depth, int is_device
     }
     KF_TRY(b->eng.end_inputs(cs));
     KF_TRY(b->eng.enqueue(st));
+    KF_TRY(b->eng.fetch(st));
     KF_CK(cudaStreamSynchronize(st));
     kf_status r = b->eng.collect(want);
     KF_TRY(tuner_after_step(b->eng));
@@ -2436,7 +2448,7 @@ kf_status kf_server_step(kf_server* s, int* served) {
     cudaStream_t st = s->stream;
     KF_TRY(s->eng.set_step(want, st));
     cudaStream_t cs = st;
-    KF_TRY(s->eng.begin_inputs(true, st, &cs));
+    KF_TRY(s->eng.begin_inputs(st, &cs));
     for (int i = 0; i < cap; ++i) {
         if (!want[i].active) continue;
         const ServerSlot& h = s->hs[i];
@@ -2445,6 +2457,7 @@ kf_status kf_server_step(kf_server* s, int* served) {
     }
     KF_TRY(s->eng.end_inputs(cs));
     KF_TRY(s->eng.enqueue(st));
+    KF_TRY(s->eng.fetch(st));
     KF_CK(cudaStreamSynchronize(st));
     kf_status r = s->eng.collect(want);
     const double t = now_ms();
