@@ -278,12 +278,24 @@ __device__ __forceinline__ float superbrick_run_exit(const SessionDev* S, const 
     return fminf(fminf(tmx, tmy), tmz);
 }
 
+// a read-only load the compiler keeps where it is written (not sunk into a branch)
+__device__ __forceinline__ int ld_keep(const int* p) {
+    int v;
+    asm volatile("ld.global.nc.s32 %0, [%1];" : "=r"(v) : "l"(p));
+    return v;
+}
+
 // Samples whose base voxel lies in a cell whose distance lower bound is at or above the
 // current threshold (0.991 during large steps, 0.001 during small steps) cannot change the
 // march.  If the sample at st.t, with base voxel (vx, vy, vz), is such a sample, advance st past
 // every following sample in the same cell -- the run of skippable 32^3 super-bricks along the
 // ray when its super-brick qualifies, else its 8^3 brick -- to the first sample index whose
-// position is at or past the cell's (run's) exit, and return true.
+// position is at or past the cell's (run's) exit, and return true.  kEager issues the brick
+// bound's load beside the super-brick bound's (an evaluated sample needs both): one L1/L2 round
+// trip instead of two where latency bounds the march (a single session's raycast, the long
+// rays: +0.9 % for one session); where instruction issue bounds it (the 64-register form for
+// many ray tiles) the load after a failed super-brick test only is cheaper (0.8 %).
+template <bool kEager>
 __device__ __forceinline__ bool skip_cell(const SessionDev* S, const RayGeo& g, RayState& st, int vx, int vy, int vz,
                                           float inc) {
     const int n = S->n;
@@ -292,12 +304,24 @@ __device__ __forceinline__ bool skip_cell(const SessionDev* S, const RayGeo& g, 
     const int sx = vx >> 5, sy = vy >> 5, sz = vz >> 5;
     const int ns = S->ns, nb = S->nb;   // (n / 8)^3 bricks: 32-bit indices
     float exit_t;
-    if (__ldg(S->sdil + (sz * ns + sy) * ns + sx) >= thr) {
-        exit_t = superbrick_run_exit(S, g, thr, sx, sy, sz, st.far_d);
-    } else {
+    if constexpr (kEager) {
         const int bx = vx >> 3, by = vy >> 3, bz = vz >> 3;
-        if (__ldg(S->bdil + (bz * nb + by) * nb + bx) < thr) return false;
-        exit_t = box_exit(g, n, bx * 8, bx * 8 + 8, by * 8, by * 8 + 8, bz * 8, bz * 8 + 8, st.far_d);
+        const int skey = ld_keep(S->sdil + (sz * ns + sy) * ns + sx);
+        const int bkey = ld_keep(S->bdil + (bz * nb + by) * nb + bx);
+        if (skey >= thr) {
+            exit_t = superbrick_run_exit(S, g, thr, sx, sy, sz, st.far_d);
+        } else {
+            if (bkey < thr) return false;
+            exit_t = box_exit(g, n, bx * 8, bx * 8 + 8, by * 8, by * 8 + 8, bz * 8, bz * 8 + 8, st.far_d);
+        }
+    } else {
+        if (__ldg(S->sdil + (sz * ns + sy) * ns + sx) >= thr) {
+            exit_t = superbrick_run_exit(S, g, thr, sx, sy, sz, st.far_d);
+        } else {
+            const int bx = vx >> 3, by = vy >> 3, bz = vz >> 3;
+            if (__ldg(S->bdil + (bz * nb + by) * nb + bx) < thr) return false;
+            exit_t = box_exit(g, n, bx * 8, bx * 8 + 8, by * 8, by * 8 + 8, bz * 8, bz * 8 + 8, st.far_d);
+        }
     }
     // skip this sample and every later one whose base voxel stays in the box: the next sample
     // is the first index k > idx with base + k inc >= lim (positions increase with k), or the
@@ -320,7 +344,7 @@ __device__ __forceinline__ bool skip_cell(const SessionDev* S, const RayGeo& g, 
 // The reference's march loop for one lane (project/src/raycast.cu:75-117).  Returns 1 when
 // the ray is finished (precise = refined hit distance, 0 for none) and 0 when `budget`
 // iterations ran out with the ray still marching (state kept in st).
-template <class TF, class Cnt>
+template <class TF, class Cnt, bool kEager>
 __device__ int march_serial(const SessionDev* S, const RayGeo& g, const TF* f, RayState& st, int budget,
                             float& precise, Cnt& cnt) {
     const int n = S->n;
@@ -334,7 +358,7 @@ __device__ int march_serial(const SessionDev* S, const RayGeo& g, const TF* f, R
         texel(g, st.t, x, y, z);
         const TexelBase tb = texel_base(n, x, y, z);
         const int g0 = st.guard;
-        if (bdil && skip_cell(S, g, st, tb.x0, tb.y0, tb.z0, inc)) {
+        if (bdil && skip_cell<kEager>(S, g, st, tb.x0, tb.y0, tb.z0, inc)) {
             cnt.add(kCntSkips, 1u);
             cnt.add(kCntSkipped, unsigned(st.guard - g0));
             continue;
@@ -391,7 +415,7 @@ __device__ void march_coop(const SessionDev* S, const RayGeo& g, const TF* f, Ra
             texel(g, st.t, x, y, z);
             const TexelBase tb = texel_base(S->n, x, y, z);
             const int g0 = st.guard;
-            if (skip_cell(S, g, st, tb.x0, tb.y0, tb.z0, inc)) {   // every lane takes the same steps
+            if (skip_cell<true>(S, g, st, tb.x0, tb.y0, tb.z0, inc)) {   // every lane takes the same steps
                 if (lane == 0) {
                     cnt.add(kCntSkips, 1u);
                     cnt.add(kCntSkipped, unsigned(st.guard - g0));
@@ -561,7 +585,7 @@ __device__ __forceinline__ void write_miss(const SessionDev* S, int level, int i
     S->pn[level][size_t(j) * w + i] = make_float4(0.f, 0.f, 0.f, kInvalid);
 }
 
-template <class TF, class Cnt>
+template <class TF, class Cnt, bool kEager>
 __device__ void serial_ray(const EngineView& v, const SessionDev* S, int s, const float* m, F3 o, int level, int i,
                            int j, int budget, Cnt& cnt) {
     const TF* f = static_cast<const TF*>(S->tf);
@@ -574,14 +598,14 @@ __device__ void serial_ray(const EngineView& v, const SessionDev* S, int s, cons
     }
     cnt.add(kCntRays, 1u);
     float precise = 0.0f;
-    if (!march_serial(S, g, f, st, budget, precise, cnt)) {
+    if (!march_serial<TF, Cnt, kEager>(S, g, f, st, budget, precise, cnt)) {
         const unsigned int slot = atomicAdd(&v.counters[6], 1u);
         if (slot < unsigned(v.longq_cap)) {
             v.longq[slot] = LongRay{s, level, i, j, st, g};
             cnt.add(kCntQueued, 1u);
             return;
         }
-        march_serial(S, g, f, st, 0x7fffffff, precise, cnt);   // queue full: finish here
+        march_serial<TF, Cnt, kEager>(S, g, f, st, 0x7fffffff, precise, cnt);   // queue full: finish here
     }
     finish_ray(S, g, f, level, i, j, precise, st, cnt);
 }
@@ -613,9 +637,9 @@ __global__ void __launch_bounds__(256, kBlocksPerSm) raycast_kernel(EngineView v
         F3 o;
         ray_matrix(S, Lv, m, o);
         if (S->fmt == KF_TSDF_F16U16)
-            serial_ray<__half>(v, S, T.s, m, o, T.level, i, j, budget, cnt);
+            serial_ray<__half, MarchCount<kCount>, kBlocksPerSm == 3>(v, S, T.s, m, o, T.level, i, j, budget, cnt);
         else
-            serial_ray<float>(v, S, T.s, m, o, T.level, i, j, budget, cnt);
+            serial_ray<float, MarchCount<kCount>, kBlocksPerSm == 3>(v, S, T.s, m, o, T.level, i, j, budget, cnt);
     }
     cnt.flush(v.ray_counts);
 }
@@ -692,7 +716,7 @@ __global__ void raycast_stage_kernel(SessionDev S, RayStage rs, int w, int h) {
     }
     float precise = 0.0f;
     MarchCount<false> cnt;
-    march_serial(&S, g, f, st, 0x7fffffff, precise, cnt);
+    march_serial<TF, MarchCount<false>, false>(&S, g, f, st, 0x7fffffff, precise, cnt);
     finish_ray(&S, g, f, 0, i, j, precise, st, cnt);
 }
 
