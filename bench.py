@@ -64,6 +64,36 @@ def ncu_traffic():
         return {}
 
 
+def ncu_issue():
+    """Warp and thread instructions per frame of each stage's kernels from the committed ncu
+    summary (one single-session 640x480 frame), if present."""
+    try:
+        with open(os.path.join(ROOT, "profiles", "ncu_issue.json")) as f:
+            return {k: v for k, v in json.load(f).items() if isinstance(v, dict)}
+    except Exception:
+        return {}
+
+
+WARP_ISSUE_PER_SM_CLOCK = 4   # four schedulers per SM, each issuing one warp instruction a cycle
+
+
+def issue_rooflines(issue, stage_ms, sms, clock_mhz):
+    """The bound of the issue-bound stages: each stage's warp instructions per frame (ncu) over
+    its event time, against the GPU's issue peak (SMs x 4 schedulers x SM clock)."""
+    peak = sms * WARP_ISSUE_PER_SM_CLOCK * clock_mhz * 1e6
+    out = {}
+    for k, ms in zip(["preprocess", "raycast", "icp", "fuse"], stage_ms):
+        n = (issue.get(k) or {}).get("warp_instructions")
+        if not n or not ms or ms <= 0:
+            continue
+        rate = n / (float(ms) / 1000.0)
+        out[k] = {"warp_instructions_per_frame": int(n), "achieved_per_s": round(rate, 1),
+                  "peak_per_s": round(peak, 1), "frac": round(rate / peak, 4),
+                  "peak_note": "%d SMs x %d warp instructions per cycle x %.0f MHz" %
+                               (sms, WARP_ISSUE_PER_SM_CLOCK, clock_mhz)}
+    return out
+
+
 class ClockSampler:
     """SM clocks and throttle reasons sampled during the timed region (NVML every 10 ms; the
     nvidia-smi query of the same fields when NVML is not importable)."""
@@ -1122,6 +1152,19 @@ def run_ours(args, world, rank, local):
         stages["raycast"]["evaluated_gather_gbs"] = round(own / rs / 1e9, 1) if rs > 0 else None
         stages["raycast"]["evaluated_gather_frac_of_l2_read"] = (round(own / rs / 1e9 / l2, 4) if rs > 0 and l2
                                                                  else None)
+        # the instruction-issue view: every stage is bound by issue or latency, not by bytes
+        props = torch.cuda.get_device_properties(torch.cuda.current_device())
+        clock_mhz = (clocks or {}).get("sm_max_mhz") or (clocks or {}).get("sm_mhz") or 1965.0
+        issue_counts = ncu_issue()
+        for k, v in issue_rooflines(issue_counts, stage_ms, props.multi_processor_count, clock_mhz).items():
+            stages[k]["issue"] = v
+        roofline["issue"] = stages[names[dom]].get("issue")
+        ray_threads = (issue_counts.get("raycast") or {}).get("thread_instructions")
+        if ray_threads and evaluated:
+            stages["raycast"]["thread_instructions_per_evaluated_sample"] = round(ray_threads / evaluated, 1)
+            iters = work["eval_large"] + work["eval_small"] + work["skips"]
+            if iters:
+                stages["raycast"]["thread_instructions_per_march_iteration"] = round(ray_threads / iters, 1)
         roofline["stages"] = stages
         progress("plain: roofline sample done")
         cpu = None

@@ -5,6 +5,7 @@ import re
 import sys
 from types import SimpleNamespace
 
+import numpy as np
 import pytest
 
 from conftest import ROOT
@@ -22,6 +23,22 @@ def test_kernels_per_frame_matches_the_launch_list():
     frames = max(int(n) for _, n in rows)
     per_frame = [k for k, n in rows if int(n) == frames and "set-up" not in k]
     assert len(per_frame) == bench.KERNELS_PER_FRAME, per_frame
+
+
+def test_ncu_issue_and_issue_rooflines():
+    """The instruction-issue view of the stages: ncu warp instructions per frame over the stage
+    time, against SMs x 4 schedulers x clock."""
+    issue = bench.ncu_issue()
+    for k in ("preprocess", "raycast", "icp", "fuse"):
+        assert issue[k]["warp_instructions"] > 0 and issue[k]["thread_instructions"] > issue[k]["warp_instructions"]
+    r = bench.issue_rooflines(issue, np.array([0.02, 0.15, 0.05, 0.06]), 148, 1965.0)
+    peak = 148 * 4 * 1965e6
+    assert set(r) == {"preprocess", "raycast", "icp", "fuse"}
+    assert r["raycast"]["peak_per_s"] == round(peak, 1)
+    assert abs(r["raycast"]["frac"] - issue["raycast"]["warp_instructions"] / 0.15e-3 / peak) < 1e-4
+    # a stage without a count or without a time is left out
+    assert "icp" not in bench.issue_rooflines({"raycast": issue["raycast"]}, [0.02, 0.15, 0.05, 0.06], 148, 1965.0)
+    assert "raycast" not in bench.issue_rooflines(issue, [0.02, 0.0, 0.05, 0.06], 148, 1965.0)
 
 
 def test_ncu_traffic_has_every_stage():
