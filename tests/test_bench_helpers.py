@@ -1,5 +1,6 @@
 """bench.py's bookkeeping on the CPU: the per-frame launch count against the committed launch
 list, the algorithmic-bytes formulas and the per-stage roofline arithmetic."""
+import json
 import os
 import re
 import sys
@@ -80,3 +81,24 @@ def test_stage_rooflines_arithmetic():
     assert out["icp"]["algorithmic_bytes"] == (px[0] * 2 + px[1] * 1 + px[2] * 2) * 48
     assert out["fuse"]["voxels_per_s_dense"] == pytest.approx(512 ** 3 / 0.064e-3, rel=1e-6)
     assert out["frame"]["voxels_per_s"] == pytest.approx(512 ** 3 * 3500.0, rel=1e-6)
+
+
+def test_drift_report(tmp_path, capsys):
+    """tests/drift_300.py's report on small stand-in pose sequences: errors against the truth
+    and the FP64 oracle's poses, and the share of frames with equal ICP iteration counts."""
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import drift_300
+    eye = np.eye(4, dtype=np.float32)
+    truth = np.stack([eye] * 3)
+    moved = truth.copy()
+    moved[:, 0, 3] = 0.01   # 1 cm off in x
+    iters = np.array([[1, 1, 2]] * 3)
+    np.savez(tmp_path / "g.npz", truth=truth, lib_f32=truth, lib_f32_iters=iters, lib_f16u16=moved,
+             lib_f16u16_iters=iters[::-1] * np.array([[1, 1, 1], [1, 2, 1], [1, 1, 1]]))
+    np.savez(tmp_path / "o.npz", truth=truth, poses=truth, iters=iters)
+    drift_300.report(str(tmp_path / "g.npz"), str(tmp_path / "o.npz"))
+    r = json.loads(capsys.readouterr().out)
+    assert r["lib_f32"]["vs_oracle_fp64"]["m"] == 0.0 and r["lib_f32"]["frames_icp_iterations_equal"] == 1.0
+    assert abs(r["lib_f16u16"]["vs_truth"]["m"] - 0.01) < 1e-6
+    assert abs(r["lib_f16u16"]["frames_icp_iterations_equal"] - 2 / 3) < 1e-9
+    assert "ref" not in r
