@@ -146,6 +146,34 @@ def test_down_sample_rules(orc):
     assert out[0, 1] == np.float32(3.0)
 
 
+def test_trunc8_covers_the_reference_launch_grids(orc):
+    """compat_trunc8 processes only the pixels the reference's launches reach: blocks =
+    dims / 8 of 8 x 8 threads (project/src/measurement.cu:150-151, 171-172, 192-193, 213-214),
+    so at 80 x 60 (level 2 of 320 x 240) rows 56-59 keep the output's initial contents; 640 x
+    480 and 320 x 240 divide by 8 and are covered whole."""
+    rng = np.random.default_rng(5)
+    raw = rng.integers(500, 4000, size=(60, 80)).astype(np.uint16)
+    full = orc.convert(raw, 1e-3)
+    part = orc.convert(raw, 1e-3, trunc8=True)
+    assert np.all(full > 0)
+    np.testing.assert_array_equal(part[:56], full[:56])
+    assert np.all(part[56:] == 0)           # never written: the initial zeros stay
+    # the same for the 2x2 downsample into 80 x 60 and for the vertex map of that level
+    d = rng.uniform(0.5, 4.0, size=(120, 160)).astype(np.float32)
+    ds_full = orc.down_sample(d, 0.03)
+    ds_part = orc.down_sample(d, 0.03, trunc8=True)
+    np.testing.assert_array_equal(ds_part[:56], ds_full[:56])
+    assert np.all(ds_part[56:] == 0) and np.all(ds_full[56:] > 0)
+    inv_k = np.linalg.inv(np.array([[131.25, 0, 39.5], [0, 131.25, 29.5], [0, 0, 1]], np.float32))
+    vm_full = orc.vertex_map(ds_full, inv_k)
+    vm_part = orc.vertex_map(ds_full, inv_k, trunc8=True)
+    np.testing.assert_array_equal(vm_part[:56], vm_full[:56])
+    assert np.all(vm_part[56:] == 0) and np.all(vm_full[56:, :, 3] == -1.0)
+    # sizes that divide by 8 are unaffected
+    raw2 = rng.integers(500, 4000, size=(240, 320)).astype(np.uint16)
+    np.testing.assert_array_equal(orc.convert(raw2, 1e-3, trunc8=True), orc.convert(raw2, 1e-3))
+
+
 def test_vertex_map_constant_depth(orc, kf):
     cfg = kf.default_config(width=8, height=4, fx=2.0, fy=2.0, cx=3.5, cy=1.5, levels=1)
     k = kf.level_intrinsics(cfg, 0)
