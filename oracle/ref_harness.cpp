@@ -27,6 +27,7 @@
 
 #include "cuda_grid_map.h"
 #include "depth_map.h"
+#include "general_helper.h"
 #include "grid_map_pyramid.h"
 #include "icp.h"
 #include "sensor.h"
@@ -381,6 +382,17 @@ int kfref_icp_residuals(void* p, int level, const float* prev_cm, const float* c
     cudaFree(dA);
     cudaFree(db);
     return ok ? cuda_status() : 2;
+}
+
+// poseError (project/src/general_helper.cpp:11-21), the reference's own host function: the
+// chord between the two rotations' images of normalize(1, 1, 1) and the distance between the
+// translations of two column-major poses.  Host only: it needs no device.
+int kfref_pose_error(const float* pose1_cm, const float* pose2_cm, float* out2) {
+    if (!pose1_cm || !pose2_cm || !out2) return 3;
+    const std::pair<float, float> e = poseError(to_mat4(pose1_cm), to_mat4(pose2_cm));
+    out2[0] = e.first;
+    out2[1] = e.second;
+    return 0;
 }
 
 }  // extern "C"

@@ -49,6 +49,7 @@ _SIG = {
     "kfref_get_tsdf": (_I, [_P, _I, _P]),
     "kfref_set_tsdf": (_I, [_P, _I, _P]),
     "kfref_icp_residuals": (_I, [_P, _I, _P, _P, _F, _F, _P, _P]),
+    "kfref_pose_error": (_I, [_P, _P, _P]),
 }
 OK, NONFINITE, CUDA_ERROR, BAD_ARG = 0, 1, 2, 3
 
@@ -79,6 +80,16 @@ def _p(a):
 def _cm(pose):
     """4 x 4 matrix -> 16 column-major float32."""
     return np.ascontiguousarray(np.asarray(pose, np.float32).T).ravel()
+
+
+def pose_error(pose1, pose2):
+    """The reference's own poseError (project/src/general_helper.cpp:11-21) on two 4 x 4 poses:
+    (rotation chord, translation distance).  Host only."""
+    out = np.zeros(2, np.float32)
+    st = lib().kfref_pose_error(_p(_cm(pose1)), _p(_cm(pose2)), _p(out))
+    if st != OK:
+        raise RuntimeError("kfref_pose_error: status %d" % st)
+    return float(out[0]), float(out[1])
 
 
 def mue_scale_for(cfg):

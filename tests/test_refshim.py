@@ -140,3 +140,32 @@ def test_matching_config_has_the_reference_constants(kf):
     assert (c.bilateral_sigma_s, c.bilateral_sigma_r, c.bilateral_radius) == (4.0, 0.25, 3)
     assert list(c.iters)[:3] == [10, 5, 3]
     assert (c.min_depth, c.max_depth) == (np.float32(0.4), np.float32(6.0))
+
+
+def test_pose_error_equals_the_reference_function(kf, orc):
+    """kf_pose_error (library, host) and the oracle's pose error against the reference's own
+    poseError (project/src/general_helper.cpp:11-21, compiled from its sources over the glm
+    subset), bit for bit on random poses: rotations about random axes up to 0.5 rad and
+    translations up to 2 m, identity and equal poses included."""
+    if not refpipe.available():
+        pytest.skip("the reference harness is built only where a reference checkout exists")
+    rng = np.random.default_rng(17)
+
+    def pose():
+        ax = rng.normal(size=3)
+        ax /= np.linalg.norm(ax)
+        ang = rng.uniform(0.0, 0.5)
+        k = np.array([[0, -ax[2], ax[1]], [ax[2], 0, -ax[0]], [-ax[1], ax[0], 0]])
+        m = np.eye(4)
+        m[:3, :3] = np.eye(3) + np.sin(ang) * k + (1 - np.cos(ang)) * k @ k
+        m[:3, 3] = rng.uniform(-2.0, 2.0, size=3)
+        return m.astype(np.float32)
+
+    pairs = [(np.eye(4, dtype=np.float32), np.eye(4, dtype=np.float32))]
+    p = pose()
+    pairs.append((p, p.copy()))
+    pairs += [(pose(), pose()) for _ in range(200)]
+    for a, b in pairs:
+        want = refpipe.pose_error(a, b)
+        assert tuple(np.float32(kf.poseError(a, b))) == tuple(np.float32(want))
+        assert tuple(np.float32(orc.pose_error(a, b))) == tuple(np.float32(want))
