@@ -4,7 +4,9 @@
 // it; nothing in the CUDA library links it.
 //
 // The reference's frame loop is KinectFusion::startTracking (project/src/kinect_fusion.cpp:
-// 44-73), which also runs an SDL/OpenGL window and a dataset reader that cannot be built here.
+// 44-73), which also runs an SDL/OpenGL window (not built here) and reads depth PNGs through
+// stb_image (an empty submodule of the reference).  Its TUM sequence reader, RgbdDataset, is
+// built and exported below on its own (host only).
 // This file restates that loop's compute calls in the same order with the reference's own
 // classes and kernel wrappers:
 //   first frame  initializeTracking   (kinect_fusion.cpp:75-95): convert, fuse
@@ -19,8 +21,10 @@
 #include <chrono>
 #include <cstdint>
 #include <cstring>
+#include <fstream>
 #include <memory>
 #include <stdexcept>
+#include <string>
 #include <vector>
 
 #include <cuda_runtime.h>
@@ -30,6 +34,7 @@
 #include "general_helper.h"
 #include "grid_map_pyramid.h"
 #include "icp.h"
+#include "rgbd_dataset.h"
 #include "sensor.h"
 #include "voxel_grid.h"
 
@@ -392,6 +397,47 @@ int kfref_pose_error(const float* pose1_cm, const float* pose2_cm, float* out2) 
     const std::pair<float, float> e = poseError(to_mat4(pose1_cm), to_mat4(pose2_cm));
     out2[0] = e.first;
     out2[1] = e.second;
+    return 0;
+}
+
+// RgbdDataset (project/src/rgbd_dataset.cpp:6-96), the reference's own TUM RGB-D reader: load
+// a sequence directory (groundtruth.txt, depth.txt), then walk its frames in order, each the
+// depth image's path and the ground-truth pose of the nearest timestamp found by the
+// reference's forward search.  Host only.  The reference indexes the first frame without a
+// check, so a directory without both files or without frames is refused here first.
+void* kfref_tum_open(const char* dir) {
+    if (!dir) return nullptr;
+    const std::string root(dir);
+    std::ifstream gt(root + "/groundtruth.txt"), dl(root + "/depth.txt");
+    if (!gt || !dl) return nullptr;
+    std::string line;
+    int depth_lines = 0;
+    while (std::getline(dl, line)) ++depth_lines;
+    if (depth_lines <= 3) return nullptr;
+    auto* d = new RgbdDataset;
+    d->load(root);
+    return d;
+}
+
+void kfref_tum_close(void* d) { delete static_cast<RgbdDataset*>(d); }
+
+// the next frame: its pose (getCurrentPose) and its path (getNextDepthImagePath); 1 while
+// frames remain, 0 once the sequence is finished, 3 when the path does not fit path_len
+int kfref_tum_next(void* p, char* path, int path_len, float* pose_cm) {
+    auto* d = static_cast<RgbdDataset*>(p);
+    if (!d || !path || path_len <= 0 || !pose_cm) return 3;
+    if (d->isFinished()) return 0;
+    from_mat4(d->getCurrentPose(), pose_cm);
+    const std::string s = d->getNextDepthImagePath();
+    if (int(s.size()) >= path_len) return 3;
+    std::memcpy(path, s.c_str(), s.size() + 1);
+    return 1;
+}
+
+int kfref_tum_initial_pose_inverse(void* p, float* out_cm) {
+    auto* d = static_cast<RgbdDataset*>(p);
+    if (!d || !out_cm) return 3;
+    from_mat4(d->getInitialPoseInverse(), out_cm);
     return 0;
 }
 

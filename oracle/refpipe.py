@@ -50,6 +50,10 @@ _SIG = {
     "kfref_set_tsdf": (_I, [_P, _I, _P]),
     "kfref_icp_residuals": (_I, [_P, _I, _P, _P, _F, _F, _P, _P]),
     "kfref_pose_error": (_I, [_P, _P, _P]),
+    "kfref_tum_open": (_P, [ctypes.c_char_p]),
+    "kfref_tum_close": (None, [_P]),
+    "kfref_tum_next": (_I, [_P, ctypes.c_char_p, _I, _P]),
+    "kfref_tum_initial_pose_inverse": (_I, [_P, _P]),
 }
 OK, NONFINITE, CUDA_ERROR, BAD_ARG = 0, 1, 2, 3
 
@@ -90,6 +94,33 @@ def pose_error(pose1, pose2):
     if st != OK:
         raise RuntimeError("kfref_pose_error: status %d" % st)
     return float(out[0]), float(out[1])
+
+
+def tum_sequence(path):
+    """The reference's own RgbdDataset (project/src/rgbd_dataset.cpp:6-96) on a TUM sequence
+    directory: ([(depth image path, 4 x 4 ground-truth pose)], initial pose inverse).  Host
+    only."""
+    L = lib()
+    d = L.kfref_tum_open(os.fsencode(path))
+    if not d:
+        raise RuntimeError("kfref_tum_open: no sequence at %s" % path)
+    try:
+        frames = []
+        buf = ctypes.create_string_buffer(4096)
+        pose = np.zeros(16, np.float32)
+        while True:
+            st = L.kfref_tum_next(d, buf, len(buf), _p(pose))
+            if st == 0:
+                break
+            if st != 1:
+                raise RuntimeError("kfref_tum_next: status %d" % st)
+            frames.append((buf.value.decode(), pose.reshape(4, 4).T.copy()))
+        inv = np.zeros(16, np.float32)
+        if L.kfref_tum_initial_pose_inverse(d, _p(inv)) != OK:
+            raise RuntimeError("kfref_tum_initial_pose_inverse failed")
+        return frames, inv.reshape(4, 4).T.copy()
+    finally:
+        L.kfref_tum_close(d)
 
 
 def mue_scale_for(cfg):

@@ -9,8 +9,9 @@
 //   vec2, vec3, vec4, ivec2, mat3, mat4; + - * / on vectors and scalars; matrix * vector and
 //   matrix * matrix; dot, cross, length, distance, normalize (v * 1 / sqrt(dot(v, v))),
 //   transpose, inverse (adjugate / determinant), floor, min, max, abs, acos, radians,
-//   degrees, and orientate3 / yawPitchRoll (R = Ry(yaw) Rx(pitch) Rz(roll); orientate3(a)
-//   = yawPitchRoll(a.z, a.x, a.y)).
+//   degrees, orientate3 / yawPitchRoll (R = Ry(yaw) Rx(pitch) Rz(roll); orientate3(a)
+//   = yawPitchRoll(a.z, a.x, a.y)), and tquat with mat3_cast / mat4_cast (the rotation
+//   matrix of a unit quaternion).
 // The order in which the sums are written follows those definitions; where the absent
 // library wrote a sum in another order, results differ from a build with it in the last
 // bit only.  Nothing in the CUDA library includes this header.
@@ -270,5 +271,34 @@ KFG_HD mat4 yawPitchRoll(float yaw, float pitch, float roll) {
 
 // orientate3(angles): yawPitchRoll(angles.z, angles.x, angles.y) as a 3 x 3
 KFG_HD mat3 orientate3(const vec3& angles) { return mat3(yawPitchRoll(angles.z, angles.x, angles.y)); }
+
+// ---- quaternions (the reference's TUM reader, project/src/rgbd_dataset.cpp:28-70) ----
+// tquat<T>: components x, y, z (vector part) and w (scalar part), default identity
+template <class T>
+struct tquat {
+    T x, y, z, w;
+    KFG_HD tquat() : x(T(0)), y(T(0)), z(T(0)), w(T(1)) {}
+};
+using quat = tquat<float>;
+
+// mat3_cast: the rotation of a unit quaternion, 1 - 2(y^2 + z^2) ... by its nine products,
+// column by column (m[c][r]); mat4_cast puts it in the upper left of the identity
+KFG_HD mat3 mat3_cast(const tquat<float>& q) {
+    const float xx = q.x * q.x, yy = q.y * q.y, zz = q.z * q.z;
+    const float xz = q.x * q.z, xy = q.x * q.y, yz = q.y * q.z;
+    const float wx = q.w * q.x, wy = q.w * q.y, wz = q.w * q.z;
+    mat3 m;
+    m[0][0] = 1.f - 2.f * (yy + zz);
+    m[0][1] = 2.f * (xy + wz);
+    m[0][2] = 2.f * (xz - wy);
+    m[1][0] = 2.f * (xy - wz);
+    m[1][1] = 1.f - 2.f * (xx + zz);
+    m[1][2] = 2.f * (yz + wx);
+    m[2][0] = 2.f * (xz + wy);
+    m[2][1] = 2.f * (yz - wx);
+    m[2][2] = 1.f - 2.f * (xx + yy);
+    return m;
+}
+KFG_HD mat4 mat4_cast(const tquat<float>& q) { return mat4(mat3_cast(q)); }
 
 }  // namespace glm

@@ -4,6 +4,8 @@ oracle/ref_harness.cpp, oracle/refpipe.py), no GPU:
     functions compute (inverse, transpose, orientate3 = Ry(yaw) Rx(pitch) Rz(roll), normalize,
     cross, column-major products), checked against numpy;
   - the harness library, where it is built, exports every entry point refpipe binds;
+  - its host-only entries pin the library's host code to the reference's own functions:
+    kf_pose_error to poseError, and the TUM reader (kf_tum_*) to RgbdDataset;
   - refpipe.matching_config gives the reference's hard-coded constants."""
 import ctypes
 import os
@@ -169,3 +171,63 @@ def test_pose_error_equals_the_reference_function(kf, orc):
         want = refpipe.pose_error(a, b)
         assert tuple(np.float32(kf.poseError(a, b))) == tuple(np.float32(want))
         assert tuple(np.float32(orc.pose_error(a, b))) == tuple(np.float32(want))
+
+
+def _write_tum(d, gt_t, trans, quats, depth_t):
+    with open(os.path.join(d, "groundtruth.txt"), "w") as f:
+        f.write("# ground truth trajectory\n# file: 'x.bag'\n# timestamp tx ty tz qx qy qz qw\n")
+        for t, tr, q in zip(gt_t, trans, quats):
+            f.write("%.4f %.4f %.4f %.4f %.4f %.4f %.4f %.4f\n" % (t, *tr, *q))
+    with open(os.path.join(d, "depth.txt"), "w") as f:
+        f.write("# depth maps\n# file: 'x.bag'\n# timestamp filename\n")
+        for t in depth_t:
+            f.write("%.6f depth/%.6f.png\n" % (t, t))
+
+
+@pytest.mark.parametrize("case", ["regular", "edges_and_ties", "out_of_order"])
+def test_tum_reader_equals_the_reference_reader(kf, case):
+    """The library's TUM reader (kf_tum_*) against the reference's own RgbdDataset
+    (project/src/rgbd_dataset.cpp:6-96, compiled from its sources): the same frame count, the
+    same ground-truth pose for every depth frame, bit for bit (the nearest-timestamp search
+    forward from the last match and the quaternion-to-matrix conversion), and the same initial
+    pose inverse to float rounding (the reference inverts in float, the library in double).
+    Cases: a regular 100 Hz trajectory; depth stamps before the first and after the last pose,
+    repeated stamps and exact ties between two poses; depth stamps out of order, where the
+    forward search keeps a later pose.  Quaternions are written with 4 decimals, so they are
+    not exactly of unit length."""
+    import tempfile
+    if not refpipe.available():
+        pytest.skip("the reference harness is built only where a reference checkout exists")
+    rng = np.random.default_rng({"regular": 21, "edges_and_ties": 22, "out_of_order": 23}[case])
+    gt_t = np.round(np.arange(0.0, 2.0, 0.01) + 1305031102.0, 4)
+    trans = rng.normal(size=(gt_t.size, 3))
+    quats = rng.normal(size=(gt_t.size, 4))
+    quats /= np.linalg.norm(quats, axis=1, keepdims=True)
+    if case == "regular":
+        depth_t = gt_t[3::7][:25] + 0.0031
+    elif case == "edges_and_ties":
+        depth_t = np.concatenate([[gt_t[0] - 0.5, gt_t[0]], gt_t[10:14] + 0.005,   # midway: ties
+                                  [gt_t[20], gt_t[20], gt_t[57] + 0.004],
+                                  [gt_t[-1], gt_t[-1] + 0.3, gt_t[-1] + 7.0]])
+    else:
+        depth_t = np.concatenate([gt_t[[40, 80, 60, 20, 90, 89, 150, 5, 199]] + 0.002])
+    with tempfile.TemporaryDirectory() as d:
+        os.makedirs(os.path.join(d, "depth"))
+        _write_tum(d, gt_t, trans, quats, depth_t)
+        ref_frames, ref_inv = refpipe.tum_sequence(d)
+        ds = kf.RgbdDataset(d)
+        try:
+            assert len(ds) == len(ref_frames) == len(depth_t)
+            for k, (path, ref_pose) in enumerate(ref_frames):
+                assert path == os.path.join(d, "depth/%.6f.png" % depth_t[k])
+                pose = np.asarray(ds.getCurrentPose(), np.float32)
+                np.testing.assert_array_equal(pose, ref_pose.astype(np.float32), err_msg="frame %d" % k)
+                ds.m_current_index += 1
+            if case == "out_of_order":
+                # the stamp near pose 60 after the one near pose 80: the forward search stops at
+                # pose 80 again (a global nearest search would take pose 60)
+                np.testing.assert_array_equal(ref_frames[2][1], ref_frames[1][1])
+            np.testing.assert_allclose(np.asarray(ds.getInitialPoseInverse(), np.float32), ref_inv,
+                                       rtol=1e-6, atol=2e-6)
+        finally:
+            ds.close()
