@@ -441,4 +441,19 @@ int kfref_tum_initial_pose_inverse(void* p, float* out_cm) {
     return 0;
 }
 
+// Sensor (project/src/sensor.h:10-52), the reference's own camera: the level's intrinsics
+// (fov on the diagonal, its fixed principal points 319.5 / 159.5 / 79.5 and 239.5 / 119.5 /
+// 59.5) and their glm::inverse, both column-major 3 x 3.  Host only.
+int kfref_sensor_intrinsics(float fov, int level, float* k_cm, float* inv_k_cm) {
+    if (level < 0 || level >= kLevels || !k_cm || !inv_k_cm) return 3;
+    const Sensor sensor(fov);
+    const glm::mat3 k = sensor.getIntr(level), ik = sensor.getInverseIntr(level);
+    for (int c = 0; c < 3; ++c)
+        for (int r = 0; r < 3; ++r) {
+            k_cm[c * 3 + r] = k[c][r];
+            inv_k_cm[c * 3 + r] = ik[c][r];
+        }
+    return 0;
+}
+
 }  // extern "C"

@@ -54,6 +54,7 @@ _SIG = {
     "kfref_tum_close": (None, [_P]),
     "kfref_tum_next": (_I, [_P, ctypes.c_char_p, _I, _P]),
     "kfref_tum_initial_pose_inverse": (_I, [_P, _P]),
+    "kfref_sensor_intrinsics": (_I, [_F, _I, _P, _P]),
 }
 OK, NONFINITE, CUDA_ERROR, BAD_ARG = 0, 1, 2, 3
 
@@ -121,6 +122,17 @@ def tum_sequence(path):
         return frames, inv.reshape(4, 4).T.copy()
     finally:
         L.kfref_tum_close(d)
+
+
+def sensor_intrinsics(fov, level):
+    """The reference's own Sensor (project/src/sensor.h:10-52) at one level: (K, K^-1) as 3 x 3
+    float32 arrays, its principal points fixed for 640 x 480.  Host only."""
+    k = np.zeros(9, np.float32)
+    ik = np.zeros(9, np.float32)
+    st = lib().kfref_sensor_intrinsics(float(fov), int(level), _p(k), _p(ik))
+    if st != OK:
+        raise RuntimeError("kfref_sensor_intrinsics: status %d" % st)
+    return k.reshape(3, 3).T.copy(), ik.reshape(3, 3).T.copy()
 
 
 def mue_scale_for(cfg):

@@ -5,7 +5,8 @@ oracle/ref_harness.cpp, oracle/refpipe.py), no GPU:
     cross, column-major products), checked against numpy;
   - the harness library, where it is built, exports every entry point refpipe binds;
   - its host-only entries pin the library's host code to the reference's own functions:
-    kf_pose_error to poseError, and the TUM reader (kf_tum_*) to RgbdDataset;
+    the level intrinsics and their inverse to Sensor, kf_pose_error to poseError, and the
+    TUM reader (kf_tum_*) to RgbdDataset;
   - refpipe.matching_config gives the reference's hard-coded constants."""
 import ctypes
 import os
@@ -231,3 +232,18 @@ def test_tum_reader_equals_the_reference_reader(kf, case):
                                        rtol=1e-6, atol=2e-6)
         finally:
             ds.close()
+
+
+@pytest.mark.parametrize("fov", [525.0, 517.3, 481.2])
+def test_level_intrinsics_equal_the_reference_sensor(kf, fov):
+    """The library's level intrinsics and the K^-1 it forms for its rays (kfb200's mirror of
+    it) against the reference's own Sensor (project/src/sensor.h:10-52, compiled from its
+    sources): bit for bit at every level, for a 640 x 480 frame with fx = fy = fov, the only
+    frame the reference's fixed principal points describe."""
+    if not refpipe.available():
+        pytest.skip("the reference harness is built only where a reference checkout exists")
+    cfg = kf.default_config(width=640, height=480, fx=fov, fy=fov, cx=319.5, cy=239.5, levels=3)
+    for level in range(3):
+        ref_k, ref_ik = refpipe.sensor_intrinsics(fov, level)
+        np.testing.assert_array_equal(kf.level_intrinsics(cfg, level).astype(np.float32), ref_k)
+        np.testing.assert_array_equal(kf.level_inverse_intrinsics(cfg, level), ref_ik)
